@@ -1,0 +1,318 @@
+"""Benchmark of the RK2 projection step (PowerLLEL_Channel hot path) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload: 512x384x256 channel (Lx=2pi, Ly=pi, Lz=2; tanh stretching 2.0;
+Re_tau=1000 -> re=(Re_tau/0.09)^(1/0.88); dt=1e-4; Thomas), initial field =
+Poiseuille + uniform noise 0.1 from seed 11 (seeded synthetic input, no
+dataset).  One step = main.f90:137-208 (RK1, RK2, calcRHS, PPE, correctVel,
+forceVel with boundary fills).  Each FP64 field is 403 MB > L2 (126 MB), so
+no L2 flush is needed between steps.
+
+Arms: --impl b200 (default) times this library; --impl reference times the
+reference's own C PPE (src/src_c built unmodified in oracle/_ref) inside the C
+restatement of the Fortran stencils on the host cores.  N > 1: independent
+replicas, one per GPU (the 1-GPU path does not shard), max time over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX, NY, NZ = 512, 384, 256
+RE_TAU, STRETCH, SEED, NOISE, DT = 1000.0, 2.0, 11, 0.1, 1e-4
+METRIC = "RK2 steps/s @512x384x256: mixed vs FP64 on same GPU at rel err<=1e-5"
+WORKLOAD = "channel 512x384x256, Re_tau 1000, tanh stretch 2.0, Thomas, dt 1e-4, seed 11, noise 0.1"
+
+# algorithmic bytes per grid point per launch (FP64 path), by kernel; see
+# DESIGN.md "kernels and rooflines" (SURVEY's per-pass table with the Mean_h
+# read fused into correctVel)
+ALG_BYTES_FP64 = {
+    "rk1": 48, "rk2": 72, "calc_rhs": 32,
+    "ppe_xfft_fwd": 16, "ppe_yfft_fwd": 16, "ppe_thomas": 24, "ppe_pdd": 40,
+    "ppe_yfft_bwd": 16, "ppe_xfft_bwd": 16, "correct": 56, "force": 16,
+}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_from_profiles(kernel):
+    """dram read+write bytes per launch of `kernel` from the committed ncu
+    summary (profiles/dram_traffic_512x384x256.txt), else None."""
+    p = os.path.join(ROOT, "profiles", "dram_traffic_512x384x256.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        parts = line.split()
+        if len(parts) >= 2 and parts[0] == kernel:
+            try:
+                return float(parts[1])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_reference_steps(nsteps_max, warmup, budget_s=150.0):
+    """The reference's C PPE (oracle/_ref) inside the restated Fortran step on
+    all host threads; returns (steps_per_s, threads, sample description)."""
+    from oracle import oracle as O
+    threads = cpu_threads()
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    g = O.Grid(NX, NY, NZ, stretch=STRETCH, re_tau=RE_TAU, dt=DT)
+    u, v, w, p = g.init_flow(SEED, NOISE)
+    u1, v1, w1 = g.zeros(), g.zeros(), g.zeros()
+    if O.ref_available():
+        ppe = O.RefPPE(NX, NY, NZ, g.g.dx, g.g.dy, g.dzf_global)
+        what = "reference C PPE (src/src_c built unmodified) + C restatement of the Fortran stencils"
+    else:
+        ppe = O.PPE(NX, NY, NZ, g.g.dx, g.g.dy, g.dzf_global)
+        what = "C restatement of the PPE and of the Fortran stencils"
+    t0 = time.perf_counter()
+    for _ in range(max(1, warmup)):
+        g.step(ppe, u, v, w, u1, v1, w1, p)
+    t_first = (time.perf_counter() - t0) / max(1, warmup)
+    n = max(1, min(nsteps_max, int(budget_s / max(t_first, 1e-3))))
+    t0 = time.perf_counter()
+    for _ in range(n):
+        g.step(ppe, u, v, w, u1, v1, w1, p)
+    dt = time.perf_counter() - t0
+    if hasattr(ppe, "close"):
+        ppe.close()
+    sample = f"{n} full {NX}x{NY}x{NZ} step(s) after {max(1, warmup)} warm-up, {threads} OpenMP threads: {what}"
+    return n / dt, threads, sample
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group(backend="nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup(args.gpus)
+    if rank != 0:
+        return
+    sps, threads, sample = cpu_reference_steps(args.steps, args.warmup)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": sps, "unit": "steps/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / sps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "precision": "fp64 (reference path)", "parallelism": "host cores"},
+        "cpu_baseline": {"value": sps, "unit": "steps/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": sps, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args):
+    world, rank, local = dist_setup(args.gpus)
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local)
+    import powerllel_channel_b200 as plb
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([x], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return x
+
+    def timed(ch, K, W, body):
+        for _ in range(W):
+            body()
+        ch.synchronize()
+        torch.cuda.synchronize()
+        st = torch.cuda.ExternalStream(ch.stream_handle)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        torch.cuda.synchronize()
+        e0.record(st)
+        for _ in range(K):
+            body()
+        e1.record(st)
+        ch.synchronize()
+        torch.cuda.synchronize()
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1))
+
+    cfg64 = plb.ChannelConfig(nx=NX, ny=NY, nz=NZ, stretch_ratio=STRETCH, re_tau=RE_TAU, dt=DT,
+                              precision=plb.PL_FP64)
+    ch = plb.Channel(cfg64)
+    ch.init_flow(SEED, NOISE)
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms64 = timed(ch, args.steps, args.warmup, lambda: ch.step(1))
+    clk = clocks.stop()
+    sps64 = world * args.steps / (ms64 / 1000.0)
+
+    # per-kernel device times -> roofline of the dominant kernel
+    prof = ch.profile(3)
+    npts = NX * NY * NZ
+    peak, peak_kind = peaks()
+    top = max(prof, key=lambda kv: kv[1])
+    alg = ALG_BYTES_FP64.get(top[0], 0) * npts
+    achieved = alg / (top[1] / 1000.0) / 1e9
+    tot_ms = sum(ms for _, ms in prof)
+    kernels = {name: {"ms": round(ms, 4), "share": round(ms / tot_ms, 4),
+                      "gbs": round(ALG_BYTES_FP64.get(name, 0) * npts / (ms / 1000.0) / 1e9, 1)}
+               for name, ms in prof}
+    traffic = traffic_from_profiles(top[0])
+    launches_per_step = 11
+
+    # end to end through the C ABI with host (pinned) buffers: every step
+    # uploads u,v,w, steps, downloads u,v,w
+    host = torch.empty(3 * ch.compact_elems, dtype=torch.float64).pin_memory()
+    ch.download_compact(host.data_ptr())
+    ch.synchronize()
+    nbytes = 3 * ch.compact_elems * 8
+    ke = max(3, min(args.steps, 10))
+
+    def e2e_body():
+        ch.upload_compact(host.data_ptr())
+        ch.step(1)
+        ch.download_compact(host.data_ptr())
+
+    ms_e2e = timed(ch, ke, 1, e2e_body)
+    e2e_sps = world * ke / (ms_e2e / 1000.0)
+    ch.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            sps_cpu, threads, sample = cpu_reference_steps(2, 1, budget_s=25.0)
+            cpu = {"value": sps_cpu, "unit": "steps/s", "cores": threads, "kind": "port", "sample": sample}
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "steps/s", "cores": cpu_threads(), "kind": "port",
+                   "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": sps64, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms64 / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "precision": "fp64", "grid": [NX, NY, NZ],
+                       "l2": "inputs larger than L2 (403 MB per FP64 field), no flush",
+                       "parallelism": "1 GPU" if world == 1 else f"{world} independent replicas"},
+            "fp64_steps_per_s": sps64,
+            "clocks": clk,
+            "e2e": {"value": e2e_sps, "unit": "steps/s", "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
+            "gpu_launches": launches_per_step * args.steps,
+            "roofline": {"bound": "hbm", "kernel": top[0], "achieved": round(achieved, 1), "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "traffic": traffic, "alg_bytes": alg},
+            "kernels": kernels,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,156 @@
+/*
+ * powerllel_b200.h -- C ABI of the B200 implementation of PowerLLEL_Channel's
+ * RK2 projection step (libpowerllel_b200.so).
+ *
+ * Plain C: pointers, sizes and status codes; no CUDA or torch types.  Device
+ * pointers are passed as void*, streams as void* (a cudaStream_t, or NULL for
+ * the library's own stream).  Every function returning int returns 0 on
+ * success and -1 on failure, with the reason in pl_last_error().
+ *
+ * Part 1 is the reference's own PPE interface, unchanged, so that a build of
+ * the Fortran driver links this library in place of src/src_c/mod_poisson_
+ * solver.c + mod_fft.c.  Parts 2-4 are the device-resident extensions.
+ */
+#ifndef POWERLLEL_B200_H
+#define POWERLLEL_B200_H
+
+#include <stdbool.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ======================================================================
+ * 1. Reference PPE interface (drop-in)
+ * ====================================================================== */
+
+/* Replaces init_poisson_solver, src/src_c/mod_poisson_solver.c:178-309
+ * (Fortran interface src/mod_poisson_solver.f90:61-75).  Same arguments:
+ * global sizes, dx, dy, dzf_global[0..nz+1], NUL-terminated BC strings
+ * (only "PP","PP","NN" -- the channel -- is supported, as in main.f90:80),
+ * neighbour table [pencil][W,E,S,N,B,T] compared against MPI_PROC_NULL.
+ * Reads decomp_main (decomp_2d.h) when the caller's process defines it (the
+ * reference decomp_2d.c kept in the link) and requires the whole domain on
+ * this rank; without it the global sizes define a 1x1 decomposition.
+ * Solver: Thomas by default (the default build, src/CMakeLists.txt:8); PDD
+ * with P z-partitions after pl_set_trid_partitions(P) (the USE_PDD build
+ * run on P ranks, p_row = 1, p_col = P).  Errors abort the process, as the
+ * reference's decomposition errors do (decomp_2d.c:114-121). */
+void init_poisson_solver(int nx_global, int ny_global, int nz_global, double dx, double dy,
+                         double *dzf_global, char bctype_x[], char bctype_y[], char bctype_z[],
+                         int neighbor_xyz[3][6]);
+
+/* Replaces execute_poisson_solver, mod_poisson_solver.c:468-605: solves in
+ * place on the caller's ghosted host array var[(nx+2)(ny+2)(nz+2)] (Fortran
+ * order); only the interior is read and overwritten. */
+void execute_poisson_solver(double *var);
+
+/* Replaces free_poisson_solver, mod_poisson_solver.c:607-632. */
+void free_poisson_solver(void);
+
+/* PDD partition count used by the next init_poisson_solver: 0 = Thomas,
+ * P >= 1 = PDD with P z-partitions (no reference counterpart: the reference
+ * selects PDD at build time with USE_PDD and takes P from p_col). */
+int pl_set_trid_partitions(int nparts);
+
+/* Message of the last failure of the calling thread ("" if none). */
+const char *pl_last_error(void);
+
+/* ======================================================================
+ * 2. Device-resident PPE
+ * ====================================================================== */
+
+enum { PL_FP64 = 0, PL_MIXED = 1 };
+
+typedef struct pl_ppe pl_ppe;
+
+/* Same setup as init_poisson_solver (mod_poisson_solver.c:178-309) as an
+ * object: nparts 0 = Thomas, P >= 1 = PDD; precision PL_FP64 or PL_MIXED. */
+int pl_ppe_create(pl_ppe **out, int nx, int ny, int nz, double dx, double dy, const double *dzf_global,
+                  int nparts, int precision);
+/* In place on a device array of nx*ny*nz values (double for PL_FP64, float
+ * for PL_MIXED), layout [k][j][i], i fastest, no ghosts.  Asynchronous on
+ * `stream`.  Same operator as execute_poisson_solver (:468-605). */
+int pl_ppe_solve(pl_ppe *s, void *d_var, void *stream);
+int pl_ppe_destroy(pl_ppe *s);
+
+/* ======================================================================
+ * 3. Whole time step (main.f90:131-208) on device-resident fields
+ * ====================================================================== */
+
+typedef struct {
+    int nx, ny, nz;          /* global grid, nx and ny even (mod_parameters.f90:264-267) */
+    double lx, ly, lz;       /* domain */
+    int mesh_type;           /* 0 uniform, 1 stretched (mod_mesh.f90:134-158) */
+    int stretch_func;        /* 0 tanh, 1 sin */
+    double stretch_ratio;
+    double re, u_ref, l_ref; /* re_inv = u_ref*l_ref/re (mod_parameters.f90:187) */
+    double dt, u_crf;
+    int is_forced[3];
+    double vel_force[3];
+    int trid_parts;          /* 0 Thomas, P >= 1 PDD */
+    int precision;           /* PL_FP64 or PL_MIXED */
+} pl_channel_config;
+
+typedef struct pl_channel pl_channel;
+
+typedef struct {
+    double div_max;   /* max |div u| (calcMaxDiv, mod_utils.f90:257-318) */
+    double cfl_max;   /* max CFL, times dt (calcMaxCFL, :193-255) */
+    int div_ijk[3];   /* 1-based location of div_max */
+    int cfl_ijk[3];
+    int nan_count;    /* NaNs in u, v, w incl. wall ghosts (checkNaN, :352-394) */
+} pl_diag;
+
+int pl_channel_create(pl_channel **out, const pl_channel_config *cfg);
+int pl_channel_destroy(pl_channel *c);
+/* initFlow 'poi' + noise (mod_initFlow.f90:19-81) with a counter-based
+ * SplitMix64 stream (u, then v, then w, interior i-fastest; value n is
+ * splitmix64(seed + (n+1)*0x9E3779B97F4A7C15) >> 11 scaled by 2^-53), then
+ * transform2CRF and the boundary fills (main.f90:98-102). */
+int pl_channel_init_flow(pl_channel *c, uint64_t seed, double noise_intensity);
+/* nsteps RK2 projection steps, asynchronous on the channel's stream */
+int pl_channel_step(pl_channel *c, int nsteps);
+int pl_channel_synchronize(pl_channel *c);
+int pl_channel_diagnostics(pl_channel *c, pl_diag *out);
+/* host copies in the reference's ghosted Fortran layout (nx+2)(ny+2)(nz+2);
+ * any pointer may be NULL.  p is the last pressure (interior + ghosts). */
+int pl_channel_get_fields(pl_channel *c, double *u, double *v, double *w, double *p);
+int pl_channel_set_fields(pl_channel *c, const double *u, const double *v, const double *w);
+/* one field (numbering of pl_channel_field) to a host array in the ghosted
+ * layout, converted to double; the stage-1 fields of the mixed path are
+ * returned as u1 = u + increment */
+int pl_channel_get_field(pl_channel *c, int which, double *host_ghosted);
+/* host copies in the device layout nx*ny*(nz+2) per component (wall ghost
+ * planes included), u then v then w; with pinned memory these are single
+ * DMA transfers (used for end-to-end timing) */
+int pl_channel_upload_compact(pl_channel *c, const double *uvw);
+int pl_channel_download_compact(pl_channel *c, double *uvw);
+/* device pointers of the current fields (for per-phase entries and tests):
+ * which = 0..2 u,v,w (FP64, nx*ny*(nz+2)), 3 = p (interior), 4..6 = stage-1
+ * fields u1,v1,w1 (FP64 path) or stage-1 increments (mixed path, FP32) */
+void *pl_channel_field(pl_channel *c, int which);
+void *pl_channel_stream(pl_channel *c);
+
+/* ======================================================================
+ * 4. Per-phase entries on the channel's device fields (one kernel each,
+ *    asynchronous; the step calls them in this order)
+ * ====================================================================== */
+int pl_phase_rk1(pl_channel *c);        /* timeIntVelRK1 + updateBoundVel(u1) */
+int pl_phase_rk2(pl_channel *c);        /* timeIntVelRK2 + updateBoundVel(u) */
+int pl_phase_calc_rhs(pl_channel *c);   /* calcRHS into p */
+int pl_phase_poisson(pl_channel *c);    /* execute_poisson_solver(p) */
+int pl_phase_correct_force(pl_channel *c); /* updateBoundP, correctVel, forceVel, updateBoundVel */
+
+/* Per-kernel device time: runs nsteps steps with a CUDA event between every
+ * kernel launch (same kernels and order as pl_channel_step) and writes the
+ * mean milliseconds per step of each launch slot to ms[0..nslots) and its
+ * name to names (nslots*32 bytes, NUL-padded).  Returns the slot count, or -1. */
+int pl_channel_profile(pl_channel *c, int nsteps, double *ms, char *names, int max_slots);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

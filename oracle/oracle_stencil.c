@@ -270,6 +270,7 @@ void orc_rk1(const orc_grid *g, const double *u, const double *v, const double *
              double *w1)
 {
     const double dt = g->dt;
+    #pragma omp parallel for schedule(static)
     for (int k = 1; k <= g->nz; k++)
         for (int j = 1; j <= g->ny; j++)
             for (int i = 1; i <= g->nx; i++) {
@@ -286,6 +287,7 @@ void orc_rk2(const orc_grid *g, double *u, double *v, double *w, const double *u
              const double *w1)
 {
     const double dt = g->dt;
+    #pragma omp parallel for schedule(static)
     for (int k = 1; k <= g->nz; k++)
         for (int j = 1; j <= g->ny; j++)
             for (int i = 1; i <= g->nx; i++) {
@@ -301,6 +303,7 @@ void orc_rk2(const orc_grid *g, double *u, double *v, double *w, const double *u
 void orc_calc_rhs(const orc_grid *g, const double *u, const double *v, const double *w, double *rhs)
 {
     const double dti = 1.0 / g->dt, dtidxi = dti * g->dx_inv, dtidyi = dti * g->dy_inv;
+    #pragma omp parallel for schedule(static)
     for (int k = 1; k <= g->nz; k++)
         for (int j = 1; j <= g->ny; j++)
             for (int i = 1; i <= g->nx; i++)
@@ -313,6 +316,7 @@ void orc_calc_rhs(const orc_grid *g, const double *u, const double *v, const dou
 void orc_correct_vel(const orc_grid *g, const double *p, double *u, double *v, double *w)
 {
     const double dt = g->dt, dtdxi = dt * g->dx_inv, dtdyi = dt * g->dy_inv;
+    #pragma omp parallel for schedule(static)
     for (int k = 1; k <= g->nz; k++)
         for (int j = 1; j <= g->ny; j++)
             for (int i = 1; i <= g->nx; i++) {
@@ -325,10 +329,20 @@ void orc_correct_vel(const orc_grid *g, const double *p, double *u, double *v, d
 /* Mean_h, mod_utils.f90:105-131 (one rank: the ALLREDUCE is the identity) */
 double orc_mean_h(const orc_grid *g, const double *var)
 {
-    double m = 0.0;
-    for (int k = 1; k <= g->nz; k++)
+    /* the reference sums with an OpenMP reduction over k (thread-count
+     * dependent order); here each k-plane is summed in j, i order and the
+     * plane sums are added in k order, for any thread count */
+    double *plane = (double *)calloc((size_t)g->nz + 1, sizeof(double));
+#pragma omp parallel for schedule(static)
+    for (int k = 1; k <= g->nz; k++) {
+        double s = 0.0;
         for (int j = 1; j <= g->ny; j++)
-            for (int i = 1; i <= g->nx; i++) m = m + var[IX(i, j, k)] * g->dzflzi[k];
+            for (int i = 1; i <= g->nx; i++) s = s + var[IX(i, j, k)] * g->dzflzi[k];
+        plane[k] = s;
+    }
+    double m = 0.0;
+    for (int k = 1; k <= g->nz; k++) m = m + plane[k];
+    free(plane);
     m = m / g->nx / g->ny;
     return m;
 }
@@ -341,6 +355,7 @@ void orc_force_vel(const orc_grid *g, double *u, double *v, double *w)
         if (!g->is_forced[d]) continue;
         double mean = orc_mean_h(g, f[d]);
         double force = g->vel_force[d] - mean;
+        #pragma omp parallel for schedule(static)
         for (int k = 1; k <= g->nz; k++)
             for (int j = 1; j <= g->ny; j++)
                 for (int i = 1; i <= g->nx; i++) f[d][IX(i, j, k)] = f[d][IX(i, j, k)] + force;

@@ -1,0 +1,608 @@
+// channel.cu -- the C ABI: the reference's PPE interface (drop-in), the
+// device-resident PPE object, and the whole RK2 projection step.
+//
+// Step order (main.f90:137-208): RK1 -> RK2 -> calcRHS -> PPE -> correctVel ->
+// forceVel, with updateBoundVel / updateBoundP folded into the kernels that
+// write the fields (see stencil.cu).
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/powerllel_b200.h"
+#include "ppe.cuh"
+#include "stencil.cuh"
+
+namespace pl {
+
+static thread_local std::string g_err;
+void set_error(const std::string &msg) { g_err = msg; }
+const char *get_error() { return g_err.c_str(); }
+
+} // namespace pl
+
+using namespace pl;
+
+// ------------------------------------------------------------------------
+// decomp_main of the reference's decomp_2d.h, read when the process defines
+// it (layout identical to struct DECOMP_2D_INFO, decomp_2d.h:27-51).
+// ------------------------------------------------------------------------
+typedef struct DECOMP_2D_INFO {
+    int *x1cnts, *x1disp, *y1cnts, *y1disp, *y2cnts, *y2disp, *z2cnts, *z2disp;
+    int x1count, y1count, y2count, z2count;
+    int xst[3], xen[3], xsz[3];
+    int yst[3], yen[3], ysz[3];
+    int zst[3], zen[3], zsz[3];
+    int *x1st, *x1en, *x1dist, *y1st, *y1en, *y1dist, *y2st, *y2en, *y2dist, *z2st, *z2en, *z2dist;
+    bool even;
+} pl_decomp_2d_info;
+
+extern "C" {
+extern pl_decomp_2d_info decomp_main __attribute__((weak));
+}
+
+// ------------------------------------------------------------------------
+// 1. Reference PPE interface
+// ------------------------------------------------------------------------
+namespace {
+std::mutex g_legacy_mu;
+Ppe g_legacy;
+bool g_legacy_live = false;
+int g_legacy_parts = 0;
+double *g_legacy_stage = nullptr;
+double *g_legacy_work = nullptr;
+int g_gnx = 0, g_gny = 0, g_gnz = 0;
+
+[[noreturn]] void legacy_abort(const std::string &msg)
+{
+    std::fprintf(stderr, "powerllel_b200 ERROR: %s\n", msg.c_str());
+    std::fflush(stderr);
+    std::abort();
+}
+} // namespace
+
+extern "C" int pl_set_trid_partitions(int nparts)
+{
+    if (nparts < 0) {
+        set_error("pl_set_trid_partitions: nparts must be >= 0");
+        return -1;
+    }
+    g_legacy_parts = nparts;
+    return 0;
+}
+
+extern "C" const char *pl_last_error(void) { return get_error(); }
+
+extern "C" void init_poisson_solver(int nx_global, int ny_global, int nz_global, double dx, double dy,
+                                    double *dzf_global, char bctype_x[], char bctype_y[], char bctype_z[],
+                                    int neighbor_xyz[3][6])
+{
+    std::lock_guard<std::mutex> lk(g_legacy_mu);
+    if (g_legacy_live) legacy_abort("init_poisson_solver called twice without free_poisson_solver");
+    if (std::strcmp(bctype_x, "PP") || std::strcmp(bctype_y, "PP") || std::strcmp(bctype_z, "NN"))
+        legacy_abort("only the channel boundary types PP, PP, NN are implemented");
+    if (&decomp_main != nullptr) {
+        const int *xs = decomp_main.xsz;
+        if (xs[0] != 0 && (xs[0] != nx_global || xs[1] != ny_global || xs[2] != nz_global))
+            legacy_abort("decomp_main describes a multi-rank decomposition; this library holds the whole domain "
+                         "on one GPU (p_row = p_col = 1)");
+    }
+    (void)neighbor_xyz; // one rank: every wall neighbour is MPI_PROC_NULL, y/x periodic
+    if (ppe_create(&g_legacy, nx_global, ny_global, nz_global, dx, dy, dzf_global, g_legacy_parts, PREC_FP64))
+        legacy_abort(std::string("init_poisson_solver: ") + get_error());
+    const size_t ng = (size_t)(nx_global + 2) * (ny_global + 2) * (nz_global + 2);
+    if (cudaMalloc(&g_legacy_stage, sizeof(double) * ng) != cudaSuccess ||
+        cudaMalloc(&g_legacy_work, sizeof(double) * (size_t)nx_global * ny_global * nz_global) != cudaSuccess)
+        legacy_abort("init_poisson_solver: device allocation failed");
+    g_gnx = nx_global;
+    g_gny = ny_global;
+    g_gnz = nz_global;
+    g_legacy_live = true;
+}
+
+extern "C" void execute_poisson_solver(double *var)
+{
+    std::lock_guard<std::mutex> lk(g_legacy_mu);
+    if (!g_legacy_live) legacy_abort("execute_poisson_solver before init_poisson_solver");
+    const size_t gx = (size_t)g_gnx + 2, gxy = gx * (g_gny + 2), ng = gxy * (g_gnz + 2);
+    if (cudaMemcpy(g_legacy_stage, var, sizeof(double) * ng, cudaMemcpyHostToDevice) != cudaSuccess)
+        legacy_abort("execute_poisson_solver: host to device copy failed");
+    if (ppe_solve_fp64_strided(&g_legacy, g_legacy_stage, g_legacy_stage, 1 + gx + gxy, gx, gxy, g_legacy_work,
+                               nullptr))
+        legacy_abort(std::string("execute_poisson_solver: ") + get_error());
+    if (cudaMemcpy(var, g_legacy_stage, sizeof(double) * ng, cudaMemcpyDeviceToHost) != cudaSuccess)
+        legacy_abort("execute_poisson_solver: device to host copy failed");
+}
+
+extern "C" void free_poisson_solver(void)
+{
+    std::lock_guard<std::mutex> lk(g_legacy_mu);
+    if (!g_legacy_live) return;
+    ppe_destroy(&g_legacy);
+    cudaFree(g_legacy_stage);
+    cudaFree(g_legacy_work);
+    g_legacy_stage = g_legacy_work = nullptr;
+    g_legacy_live = false;
+}
+
+// ------------------------------------------------------------------------
+// 2. Device-resident PPE
+// ------------------------------------------------------------------------
+struct pl_ppe {
+    Ppe s;
+};
+
+extern "C" int pl_ppe_create(pl_ppe **out, int nx, int ny, int nz, double dx, double dy, const double *dzf_global,
+                             int nparts, int precision)
+{
+    *out = nullptr;
+    if (precision != PL_FP64 && precision != PL_MIXED) {
+        set_error("pl_ppe_create: precision must be PL_FP64 or PL_MIXED");
+        return -1;
+    }
+    pl_ppe *p = new pl_ppe();
+    if (ppe_create(&p->s, nx, ny, nz, dx, dy, dzf_global, nparts, precision)) {
+        ppe_destroy(&p->s);
+        delete p;
+        return -1;
+    }
+    *out = p;
+    return 0;
+}
+
+extern "C" int pl_ppe_solve(pl_ppe *p, void *d_var, void *stream)
+{
+    if (!p || !d_var) {
+        set_error("pl_ppe_solve: null argument");
+        return -1;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    if (p->s.prec == PREC_FP64) return ppe_solve_fp64(&p->s, (double *)d_var, st);
+    return ppe_solve_fp32(&p->s, (float *)d_var, st);
+}
+
+extern "C" int pl_ppe_destroy(pl_ppe *p)
+{
+    if (!p) return 0;
+    ppe_destroy(&p->s);
+    delete p;
+    return 0;
+}
+
+// ------------------------------------------------------------------------
+// 3. Whole step
+// ------------------------------------------------------------------------
+struct pl_channel {
+    pl_channel_config cfg{};
+    int nx = 0, ny = 0, nz = 0;
+    size_t nf = 0;  // elements of a velocity-like field, nx*ny*(nz+2)
+    size_t np = 0;  // elements of p, nx*ny*nz
+    StepParams sp{};
+    std::vector<double> dzf_global, zc_global, dzf, dzf_inv, dzc, dzc_inv, dzflzi, prof;
+    double *d_mesh = nullptr;
+    MeshDev m{};
+    double *u = nullptr, *v = nullptr, *w = nullptr;
+    double *u1 = nullptr, *v1 = nullptr, *w1 = nullptr;
+    double *p = nullptr;
+    Ppe ppe;
+    ReduceBuf rb;
+    double *d_diag = nullptr;
+    int *d_loc = nullptr;
+    double *d_dpart = nullptr;
+    long long *d_dipart = nullptr;
+    int max_blocks = 0;
+    cudaStream_t stream = nullptr;
+    // profiling marks (pl_channel_profile)
+    std::vector<cudaEvent_t> *prof_events = nullptr;
+    std::vector<std::string> *prof_names = nullptr;
+};
+
+static void channel_mark(void *ctx, const char *name)
+{
+    pl_channel *c = (pl_channel *)ctx;
+    if (!c->prof_events) return;
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    cudaEventRecord(e, c->stream);
+    c->prof_events->push_back(e);
+    c->prof_names->push_back(name);
+}
+
+// mod_mesh.f90:26-84 with initMeshByFunc :120-162 (one rank)
+static void build_mesh(pl_channel *c)
+{
+    const pl_channel_config &g = c->cfg;
+    const int nz = g.nz, n1 = nz + 2;
+    c->dzf_global.assign(n1, 0.0);
+    c->zc_global.assign(n1, 0.0);
+    const double pi = acos(-1.0);
+    if (g.stretch_ratio == 0.0 || g.mesh_type == 0) {
+        for (int k = 0; k < n1; k++) c->dzf_global[k] = g.lz / nz;
+    } else {
+        std::vector<double> zf(nz + 1, 0.0);
+        for (int k = 1; k <= nz; k++) {
+            double z0 = k / (1.0 * nz);
+            if (g.stretch_func == 0)
+                zf[k] = 0.5 * (1.0 + tanh((z0 - 0.5) * g.stretch_ratio) / tanh(g.stretch_ratio / 2.0));
+            else
+                zf[k] = 0.5 * (1.0 + sin((z0 - 0.5) * g.stretch_ratio * pi) / sin(g.stretch_ratio * pi / 2.0));
+        }
+        for (int k = 1; k <= nz; k++) c->dzf_global[k] = g.lz * (zf[k] - zf[k - 1]);
+        c->dzf_global[0] = c->dzf_global[1];
+        c->dzf_global[nz + 1] = c->dzf_global[nz];
+    }
+    c->zc_global[0] = -0.5 * c->dzf_global[0];
+    for (int k = 1; k <= nz + 1; k++)
+        c->zc_global[k] = c->zc_global[k - 1] + 0.5 * (c->dzf_global[k - 1] + c->dzf_global[k]);
+    c->dzf = c->dzf_global;
+    c->dzf_inv.assign(n1, 0.0);
+    c->dzc.assign(n1, 0.0);
+    c->dzc_inv.assign(n1, 0.0);
+    c->dzflzi.assign(n1, 0.0);
+    for (int k = 0; k <= nz + 1; k++) c->dzf_inv[k] = 1.0 / c->dzf[k];
+    for (int k = 0; k <= nz; k++) {
+        c->dzc[k] = 0.5 * (c->dzf[k] + c->dzf[k + 1]);
+        c->dzc_inv[k] = 1.0 / c->dzc[k];
+    }
+    c->dzc[nz + 1] = c->dzc[nz]; // never assigned nor read by the reference
+    c->dzc_inv[nz + 1] = c->dzc_inv[nz];
+    for (int k = 0; k <= nz + 1; k++) c->dzflzi[k] = c->dzf[k] / g.lz;
+    // Poiseuille profile, setProfile_Poiseuille (mod_initFlow.f90:83-97)
+    c->prof.assign(n1, 0.0);
+    for (int k = 1; k <= nz; k++) {
+        double zn = c->zc_global[k] / g.lz;
+        c->prof[k] = 6.0 * (1.0 - zn) * zn * g.u_ref;
+    }
+}
+
+static void channel_free(pl_channel *c)
+{
+    cudaFree(c->d_mesh);
+    cudaFree(c->u);
+    cudaFree(c->v);
+    cudaFree(c->w);
+    cudaFree(c->u1);
+    cudaFree(c->v1);
+    cudaFree(c->w1);
+    cudaFree(c->p);
+    cudaFree(c->rb.partial);
+    cudaFree(c->rb.scalar);
+    cudaFree(c->d_diag);
+    cudaFree(c->d_loc);
+    cudaFree(c->d_dpart);
+    cudaFree(c->d_dipart);
+    ppe_destroy(&c->ppe);
+    if (c->stream) cudaStreamDestroy(c->stream);
+}
+
+extern "C" int pl_channel_create(pl_channel **out, const pl_channel_config *cfg)
+{
+    *out = nullptr;
+    if (cfg->precision != PL_FP64) {
+        set_error("pl_channel_create: only PL_FP64 is available in this build");
+        return -1;
+    }
+    if (cfg->nx < 2 || cfg->ny < 2 || cfg->nz < 2 || (cfg->nx & 1) || (cfg->ny & 1) || (cfg->nz & 1)) {
+        set_error("pl_channel_create: nx, ny, nz must be even (mod_parameters.f90:264-267)");
+        return -1;
+    }
+    pl_channel *c = new pl_channel();
+    c->cfg = *cfg;
+    c->nx = cfg->nx;
+    c->ny = cfg->ny;
+    c->nz = cfg->nz;
+    c->nf = (size_t)c->nx * c->ny * (c->nz + 2);
+    c->np = (size_t)c->nx * c->ny * c->nz;
+    build_mesh(c);
+    c->sp.nx = c->nx;
+    c->sp.ny = c->ny;
+    c->sp.nz = c->nz;
+    c->sp.dx_inv = 1.0 / (cfg->lx / cfg->nx);
+    c->sp.dy_inv = 1.0 / (cfg->ly / cfg->ny);
+    c->sp.re_inv = cfg->u_ref * cfg->l_ref / cfg->re;
+    c->sp.dt = cfg->dt;
+    c->sp.u_crf = cfg->u_crf;
+    const double dx = cfg->lx / cfg->nx, dy = cfg->ly / cfg->ny;
+    auto fail = [&](void) {
+        channel_free(c);
+        delete c;
+        return -1;
+    };
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        set_error("pl_channel_create: stream creation failed");
+        return fail();
+    }
+    const size_t n1 = c->nz + 2;
+    if (cudaMalloc(&c->d_mesh, sizeof(double) * n1 * 4) != cudaSuccess) return fail();
+    cudaMemcpy(c->d_mesh, c->dzf.data(), sizeof(double) * n1, cudaMemcpyHostToDevice);
+    cudaMemcpy(c->d_mesh + n1, c->dzf_inv.data(), sizeof(double) * n1, cudaMemcpyHostToDevice);
+    cudaMemcpy(c->d_mesh + 2 * n1, c->dzc_inv.data(), sizeof(double) * n1, cudaMemcpyHostToDevice);
+    cudaMemcpy(c->d_mesh + 3 * n1, c->dzflzi.data(), sizeof(double) * n1, cudaMemcpyHostToDevice);
+    c->m.dzf = c->d_mesh;
+    c->m.dzf_inv = c->d_mesh + n1;
+    c->m.dzc_inv = c->d_mesh + 2 * n1;
+    c->m.dzflzi = c->d_mesh + 3 * n1;
+    double **fields[6] = {&c->u, &c->v, &c->w, &c->u1, &c->v1, &c->w1};
+    for (auto f : fields) {
+        if (cudaMalloc(f, sizeof(double) * c->nf) != cudaSuccess) {
+            set_error("pl_channel_create: out of device memory for the fields");
+            return fail();
+        }
+        cudaMemset(*f, 0, sizeof(double) * c->nf);
+    }
+    if (cudaMalloc(&c->p, sizeof(double) * c->np) != cudaSuccess) {
+        set_error("pl_channel_create: out of device memory for p");
+        return fail();
+    }
+    cudaMemset(c->p, 0, sizeof(double) * c->np);
+    if (ppe_create(&c->ppe, c->nx, c->ny, c->nz, dx, dy, c->dzf_global.data(), cfg->trid_parts, PREC_FP64))
+        return fail();
+    c->max_blocks = ((c->nx + 63) / 64) * ((c->ny + 3) / 4) * c->nz;
+    c->rb.max_blocks = c->max_blocks;
+    if (cudaMalloc(&c->rb.partial, sizeof(double) * 3 * c->max_blocks) != cudaSuccess ||
+        cudaMalloc(&c->rb.scalar, sizeof(double) * 8) != cudaSuccess ||
+        cudaMalloc(&c->d_diag, sizeof(double) * 4) != cudaSuccess ||
+        cudaMalloc(&c->d_loc, sizeof(int) * 8) != cudaSuccess ||
+        cudaMalloc(&c->d_dpart, sizeof(double) * 3 * c->max_blocks) != cudaSuccess ||
+        cudaMalloc(&c->d_dipart, sizeof(long long) * 2 * c->max_blocks) != cudaSuccess) {
+        set_error("pl_channel_create: out of device memory for reductions");
+        return fail();
+    }
+    if (cudaDeviceSynchronize() != cudaSuccess) {
+        set_error("pl_channel_create: device error during setup");
+        return fail();
+    }
+    *out = c;
+    return 0;
+}
+
+extern "C" int pl_channel_destroy(pl_channel *c)
+{
+    if (!c) return 0;
+    cudaStreamSynchronize(c->stream);
+    channel_free(c);
+    delete c;
+    return 0;
+}
+
+extern "C" int pl_channel_init_flow(pl_channel *c, uint64_t seed, double noise)
+{
+    double *dprof = nullptr;
+    PL_CUDA_TRY(cudaMalloc(&dprof, sizeof(double) * (c->nz + 2)));
+    PL_CUDA_TRY(cudaMemcpy(dprof, c->prof.data(), sizeof(double) * (c->nz + 2), cudaMemcpyHostToDevice));
+    PL_CUDA_TRY(cudaMemsetAsync(c->u, 0, sizeof(double) * c->nf, c->stream));
+    PL_CUDA_TRY(cudaMemsetAsync(c->v, 0, sizeof(double) * c->nf, c->stream));
+    PL_CUDA_TRY(cudaMemsetAsync(c->w, 0, sizeof(double) * c->nf, c->stream));
+    PL_CUDA_TRY(cudaMemsetAsync(c->p, 0, sizeof(double) * c->np, c->stream));
+    int rc = launch_init_fill(c->u, c->v, c->w, dprof, seed, noise, c->sp, c->stream);
+    if (!rc) rc = launch_mean_sum(c->u, c->sp, c->m, c->rb, 0, c->stream);
+    if (!rc) rc = launch_init_finish(c->u, c->v, c->w, c->sp, c->cfg.u_ref, c->rb, c->stream);
+    PL_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    cudaFree(dprof);
+    return rc;
+}
+
+extern "C" int pl_phase_rk1(pl_channel *c)
+{
+    int rc = launch_rk1_fp64(c->u, c->v, c->w, c->u1, c->v1, c->w1, c->sp, c->m, c->stream);
+    channel_mark(c, "rk1");
+    return rc;
+}
+
+extern "C" int pl_phase_rk2(pl_channel *c)
+{
+    int rc = launch_rk2_fp64(c->u, c->v, c->w, c->u1, c->v1, c->w1, c->sp, c->m, c->stream);
+    channel_mark(c, "rk2");
+    return rc;
+}
+
+extern "C" int pl_phase_calc_rhs(pl_channel *c)
+{
+    int rc = launch_calc_rhs_fp64(c->u, c->v, c->w, c->p, c->sp, c->m, c->stream);
+    channel_mark(c, "calc_rhs");
+    return rc;
+}
+
+extern "C" int pl_phase_poisson(pl_channel *c) { return ppe_solve_fp64(&c->ppe, c->p, c->stream); }
+
+extern "C" int pl_phase_correct_force(pl_channel *c)
+{
+    if (launch_correct_fp64(c->p, c->u, c->v, c->w, c->sp, c->m, c->cfg.is_forced, c->rb, c->stream)) return -1;
+    channel_mark(c, "correct");
+    int rc = launch_force_fp64(c->u, c->v, c->w, c->sp, c->cfg.is_forced, c->cfg.vel_force, c->rb, c->stream);
+    channel_mark(c, "force");
+    return rc;
+}
+
+extern "C" int pl_channel_profile(pl_channel *c, int nsteps, double *ms, char *names, int max_slots)
+{
+    if (nsteps < 1) {
+        set_error("pl_channel_profile: nsteps must be >= 1");
+        return -1;
+    }
+    std::vector<cudaEvent_t> ev;
+    std::vector<std::string> nm;
+    c->prof_events = &ev;
+    c->prof_names = &nm;
+    c->ppe.mark = channel_mark;
+    c->ppe.mark_ctx = c;
+    int rc = 0;
+    channel_mark(c, "start");
+    for (int s = 0; s < nsteps && rc == 0; s++) rc = pl_channel_step(c, 1);
+    c->ppe.mark = nullptr;
+    c->prof_events = nullptr;
+    c->prof_names = nullptr;
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    int nslot = ((int)ev.size() - 1) / nsteps;
+    if (rc == 0 && e == cudaSuccess) {
+        for (int q = 0; q < nslot && q < max_slots; q++) {
+            double acc = 0.0;
+            for (int s = 0; s < nsteps; s++) {
+                float t = 0.f;
+                cudaEventElapsedTime(&t, ev[(size_t)s * nslot + q], ev[(size_t)s * nslot + q + 1]);
+                acc += t;
+            }
+            ms[q] = acc / nsteps;
+            if (names) {
+                std::memset(names + 32 * q, 0, 32);
+                std::strncpy(names + 32 * q, nm[q + 1].c_str(), 31);
+            }
+        }
+    }
+    for (auto x : ev) cudaEventDestroy(x);
+    if (rc) return -1;
+    if (e != cudaSuccess) {
+        set_error(std::string("pl_channel_profile: ") + cudaGetErrorString(e));
+        return -1;
+    }
+    return nslot;
+}
+
+extern "C" int pl_channel_step(pl_channel *c, int nsteps)
+{
+    for (int s = 0; s < nsteps; s++) {
+        if (pl_phase_rk1(c) || pl_phase_rk2(c) || pl_phase_calc_rhs(c) || pl_phase_poisson(c) ||
+            pl_phase_correct_force(c))
+            return -1;
+    }
+    return 0;
+}
+
+extern "C" int pl_channel_synchronize(pl_channel *c)
+{
+    PL_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+extern "C" int pl_channel_diagnostics(pl_channel *c, pl_diag *out)
+{
+    if (launch_diagnostics_fp64(c->u, c->v, c->w, c->sp, c->m, c->d_diag, c->d_loc, c->d_dpart, c->d_dipart,
+                                c->max_blocks, c->stream))
+        return -1;
+    double h[3];
+    int loc[6];
+    PL_CUDA_TRY(cudaMemcpyAsync(h, c->d_diag, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    PL_CUDA_TRY(cudaMemcpyAsync(loc, c->d_loc, sizeof(loc), cudaMemcpyDeviceToHost, c->stream));
+    PL_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    out->div_max = h[0];
+    out->cfl_max = h[1];
+    out->nan_count = (int)h[2];
+    for (int q = 0; q < 3; q++) {
+        out->div_ijk[q] = loc[q];
+        out->cfl_ijk[q] = loc[3 + q];
+    }
+    return 0;
+}
+
+// device layout [k][j][i] (k = 0..nz+1) <-> reference ghosted (nx+2)(ny+2)(nz+2)
+static void expand_ghosted(const pl_channel *c, const double *src, double *dst, int planes_src, int k_off)
+{
+    const int nx = c->nx, ny = c->ny, nz = c->nz;
+    const size_t gx = nx + 2, gxy = gx * (ny + 2);
+    for (int k = 0; k <= nz + 1; k++) {
+        int ks = k + k_off; // source plane
+        if (ks < 0) ks = 0;
+        if (ks >= planes_src) ks = planes_src - 1;
+        for (int j = 0; j <= ny + 1; j++) {
+            const int js = (j == 0) ? ny - 1 : (j == ny + 1 ? 0 : j - 1);
+            const double *row = src + (size_t)nx * ((size_t)js + (size_t)ny * ks);
+            double *drow = dst + gx * j + gxy * k;
+            drow[0] = row[nx - 1];
+            std::memcpy(drow + 1, row, sizeof(double) * nx);
+            drow[nx + 1] = row[0];
+        }
+    }
+}
+
+extern "C" int pl_channel_get_fields(pl_channel *c, double *u, double *v, double *w, double *p)
+{
+    PL_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    std::vector<double> tmp(c->nf);
+    double *dev[3] = {c->u, c->v, c->w};
+    double *host[3] = {u, v, w};
+    for (int q = 0; q < 3; q++) {
+        if (!host[q]) continue;
+        PL_CUDA_TRY(cudaMemcpy(tmp.data(), dev[q], sizeof(double) * c->nf, cudaMemcpyDeviceToHost));
+        expand_ghosted(c, tmp.data(), host[q], c->nz + 2, 0);
+    }
+    if (p) {
+        PL_CUDA_TRY(cudaMemcpy(tmp.data(), c->p, sizeof(double) * c->np, cudaMemcpyDeviceToHost));
+        // interior planes 0..nz-1 become k = 1..nz; ghosts p(0) = p(1), p(nz+1) = p(nz)
+        expand_ghosted(c, tmp.data(), p, c->nz, -1);
+    }
+    return 0;
+}
+
+extern "C" int pl_channel_get_field(pl_channel *c, int which, double *host)
+{
+    PL_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (which < 0 || which > 6 || !host) {
+        set_error("pl_channel_get_field: which must be 0..6");
+        return -1;
+    }
+    std::vector<double> tmp(c->nf);
+    if (which == 3) {
+        PL_CUDA_TRY(cudaMemcpy(tmp.data(), c->p, sizeof(double) * c->np, cudaMemcpyDeviceToHost));
+        expand_ghosted(c, tmp.data(), host, c->nz, -1);
+        return 0;
+    }
+    const double *src = (const double *)pl_channel_field(c, which);
+    PL_CUDA_TRY(cudaMemcpy(tmp.data(), src, sizeof(double) * c->nf, cudaMemcpyDeviceToHost));
+    expand_ghosted(c, tmp.data(), host, c->nz + 2, 0);
+    return 0;
+}
+
+extern "C" int pl_channel_set_fields(pl_channel *c, const double *u, const double *v, const double *w)
+{
+    PL_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    const int nx = c->nx, ny = c->ny, nz = c->nz;
+    const size_t gx = nx + 2, gxy = gx * (ny + 2);
+    std::vector<double> tmp(c->nf);
+    const double *host[3] = {u, v, w};
+    double *dev[3] = {c->u, c->v, c->w};
+    for (int q = 0; q < 3; q++) {
+        if (!host[q]) continue;
+        for (int k = 0; k <= nz + 1; k++)
+            for (int j = 0; j < ny; j++)
+                std::memcpy(tmp.data() + (size_t)nx * ((size_t)j + (size_t)ny * k), host[q] + 1 + gx * (j + 1) + gxy * k,
+                            sizeof(double) * nx);
+        PL_CUDA_TRY(cudaMemcpy(dev[q], tmp.data(), sizeof(double) * c->nf, cudaMemcpyHostToDevice));
+    }
+    return 0;
+}
+
+extern "C" int pl_channel_upload_compact(pl_channel *c, const double *uvw)
+{
+    double *dev[3] = {c->u, c->v, c->w};
+    for (int q = 0; q < 3; q++)
+        PL_CUDA_TRY(cudaMemcpyAsync(dev[q], uvw + q * c->nf, sizeof(double) * c->nf, cudaMemcpyHostToDevice,
+                                    c->stream));
+    return 0;
+}
+
+extern "C" int pl_channel_download_compact(pl_channel *c, double *uvw)
+{
+    double *dev[3] = {c->u, c->v, c->w};
+    for (int q = 0; q < 3; q++)
+        PL_CUDA_TRY(cudaMemcpyAsync(uvw + q * c->nf, dev[q], sizeof(double) * c->nf, cudaMemcpyDeviceToHost,
+                                    c->stream));
+    return 0;
+}
+
+extern "C" void *pl_channel_field(pl_channel *c, int which)
+{
+    switch (which) {
+    case 0: return c->u;
+    case 1: return c->v;
+    case 2: return c->w;
+    case 3: return c->p;
+    case 4: return c->u1;
+    case 5: return c->v1;
+    case 6: return c->w1;
+    default: return nullptr;
+    }
+}
+
+extern "C" void *pl_channel_stream(pl_channel *c) { return (void *)c->stream; }

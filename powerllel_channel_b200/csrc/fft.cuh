@@ -1,0 +1,192 @@
+// fft.cuh -- shared-memory batched complex FFT engine and the real<->half-complex
+// pairing used by the PPE kernels.
+//
+// The reference transforms each periodic direction with FFTW's R2HC / HC2R
+// (src/src_c/mod_fft_fftw.inc:100-160): forward unnormalised, output in FFTW's
+// half-complex order r_0..r_{n/2}, i_{(n+1)/2-1}..i_1; backward unnormalised.
+// Here two real lines are packed into one complex line (z = a + i b), one
+// complex FFT of length n is run, and the two half-complex spectra are split
+// out of it (and merged back before the inverse).  Every stored value is the
+// half-complex slot FFTW would produce, so the tridiagonal stage sees the same
+// unknowns as the reference.
+//
+// The complex FFT is a Stockham autosort decimation-in-time transform over a
+// batch held in shared memory, ping-ponging between two buffers, with radix
+// 4, 2 and 3 passes.  Twiddles exp(-2 pi i t / n) come from a table computed on
+// the host in long double.
+#pragma once
+
+#include "common.cuh"
+
+namespace pl {
+
+constexpr int FFT_MAX_STAGES = 16;
+
+// A length-n transform plan: radix of each stage and the twiddle table
+// (device pointer, n complex entries of type V).
+template <typename V> struct FftPlanDev {
+    int n;
+    int nstages;
+    int radix[FFT_MAX_STAGES];
+    const V *tw; // exp(-2 pi i t / n), t < n
+};
+
+template <typename V, bool FWD>
+__device__ __forceinline__ V twiddle(const V *tw, int t)
+{
+    V w = __ldg(tw + t);
+    if (!FWD) w.y = -w.y;
+    return w;
+}
+
+// R-point DFTs on registers.  FWD selects the sign of the exponent.
+template <typename V, bool FWD> __device__ __forceinline__ void dft2(V &a0, V &a1)
+{
+    V t = a0;
+    a0 = cadd(t, a1);
+    a1 = csub(t, a1);
+}
+
+template <typename V, bool FWD> __device__ __forceinline__ void dft4(V &a0, V &a1, V &a2, V &a3)
+{
+    V t0 = cadd(a0, a2), t1 = csub(a0, a2), t2 = cadd(a1, a3), d = csub(a1, a3);
+    V t3;
+    if (FWD) { // -i * d
+        t3.x = d.y;
+        t3.y = -d.x;
+    } else { // +i * d
+        t3.x = -d.y;
+        t3.y = d.x;
+    }
+    a0 = cadd(t0, t2);
+    a2 = csub(t0, t2);
+    a1 = cadd(t1, t3);
+    a3 = csub(t1, t3);
+}
+
+template <typename V, bool FWD> __device__ __forceinline__ void dft3(V &a0, V &a1, V &a2)
+{
+    using T = decltype(a0.x);
+    const T c = T(-0.5);
+    const T s = FWD ? T(-0.86602540378443864676372317075293618) : T(0.86602540378443864676372317075293618);
+    V sum = cadd(a1, a2), dif = csub(a1, a2);
+    V t;
+    t.x = a0.x + c * sum.x;
+    t.y = a0.y + c * sum.y;
+    // i * s * dif
+    V u;
+    u.x = -s * dif.y;
+    u.y = s * dif.x;
+    a0 = cadd(a0, sum);
+    a1 = cadd(t, u);
+    a2 = csub(t, u);
+}
+
+// One Stockham stage over a batch of `nb` sequences of length n.
+// Element (m, b) of a buffer lives at buf[m * sm + b * sb].
+// BATCH_FAST: consecutive threads take consecutive b (use when sb == 1).
+template <typename V, bool FWD, bool BATCH_FAST>
+__device__ __forceinline__ void fft_stage(const V *__restrict__ src, V *__restrict__ dst, int n, int nb, int sm,
+                                          int sb, int R, int Ns, const V *tw, int tid, int nthr)
+{
+    const int nbf = n / R;           // butterflies per sequence
+    const int tstep = n / (Ns * R);  // twiddle index step
+    const int total = nbf * nb;
+    for (int q = tid; q < total; q += nthr) {
+        int b, j;
+        if (BATCH_FAST) {
+            b = q % nb;
+            j = q / nb;
+        } else {
+            j = q % nbf;
+            b = q / nbf;
+        }
+        const V *s = src + (size_t)b * sb;
+        V *d = dst + (size_t)b * sb;
+        const int jm = j % Ns;
+        const int idxD = (j / Ns) * Ns * R + jm;
+        if (R == 4) {
+            V a0 = s[(j)*sm], a1 = s[(j + nbf) * sm], a2 = s[(j + 2 * nbf) * sm], a3 = s[(j + 3 * nbf) * sm];
+            if (Ns > 1) {
+                a1 = cmul(a1, twiddle<V, FWD>(tw, jm * tstep));
+                a2 = cmul(a2, twiddle<V, FWD>(tw, 2 * jm * tstep));
+                a3 = cmul(a3, twiddle<V, FWD>(tw, 3 * jm * tstep));
+            }
+            dft4<V, FWD>(a0, a1, a2, a3);
+            d[(idxD)*sm] = a0;
+            d[(idxD + Ns) * sm] = a1;
+            d[(idxD + 2 * Ns) * sm] = a2;
+            d[(idxD + 3 * Ns) * sm] = a3;
+        } else if (R == 2) {
+            V a0 = s[(j)*sm], a1 = s[(j + nbf) * sm];
+            if (Ns > 1) a1 = cmul(a1, twiddle<V, FWD>(tw, jm * tstep));
+            dft2<V, FWD>(a0, a1);
+            d[(idxD)*sm] = a0;
+            d[(idxD + Ns) * sm] = a1;
+        } else { // R == 3
+            V a0 = s[(j)*sm], a1 = s[(j + nbf) * sm], a2 = s[(j + 2 * nbf) * sm];
+            if (Ns > 1) {
+                a1 = cmul(a1, twiddle<V, FWD>(tw, jm * tstep));
+                a2 = cmul(a2, twiddle<V, FWD>(tw, 2 * jm * tstep));
+            }
+            dft3<V, FWD>(a0, a1, a2);
+            d[(idxD)*sm] = a0;
+            d[(idxD + Ns) * sm] = a1;
+            d[(idxD + 2 * Ns) * sm] = a2;
+        }
+    }
+}
+
+// Full transform; data starts in buf0, result pointer returned (buf0 or buf1).
+// Ends with a __syncthreads().
+template <typename V, bool FWD, bool BATCH_FAST>
+__device__ V *fft_batch(V *buf0, V *buf1, const FftPlanDev<V> &p, int nb, int sm, int sb, int tid, int nthr)
+{
+    V *src = buf0, *dst = buf1;
+    int Ns = 1;
+    for (int s = 0; s < p.nstages; s++) {
+        const int R = p.radix[s];
+        fft_stage<V, FWD, BATCH_FAST>(src, dst, p.n, nb, sm, sb, R, Ns, p.tw, tid, nthr);
+        __syncthreads();
+        Ns *= R;
+        V *t = src;
+        src = dst;
+        dst = t;
+    }
+    return src;
+}
+
+// Split the spectrum Z of z = a + i b (length n, even) into the two FFTW
+// half-complex arrays of a and b, returned as the pair (hc_a[m], hc_b[m]).
+template <typename V> __device__ __forceinline__ V split_hc(V A, V Bc, int m, int n)
+{
+    using T = decltype(A.x);
+    V r;
+    if (2 * m <= n) {
+        r.x = T(0.5) * (A.x + Bc.x);
+        r.y = T(0.5) * (A.y + Bc.y);
+    } else {
+        r.x = T(0.5) * (Bc.y - A.y);
+        r.y = T(0.5) * (A.x - Bc.x);
+    }
+    return r;
+}
+
+// Inverse of split_hc: from the half-complex pair P = (hc_a[m], hc_b[m]) and
+// Q = (hc_a[n-m], hc_b[n-m]) rebuild Z_m = A_m + i B_m.
+template <typename V> __device__ __forceinline__ V merge_hc(V P, V Q, int m, int n)
+{
+    V z;
+    if (m == 0 || 2 * m == n) {
+        z = P;
+    } else if (2 * m < n) {
+        z.x = P.x - Q.y;
+        z.y = Q.x + P.y;
+    } else {
+        z.x = Q.x + P.y;
+        z.y = Q.y - P.x;
+    }
+    return z;
+}
+
+} // namespace pl

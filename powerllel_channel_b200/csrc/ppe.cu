@@ -1,0 +1,627 @@
+// ppe.cu -- kernels and host plan of the pressure Poisson solver.
+//
+// Reference: src/src_c/mod_poisson_solver.c (init :178-309, Thomas :311-359,
+// PDD :105-176/:361-466, execute :468-605), src/src_c/mod_fft_fftw.inc
+// (plans :100-155, eigenvalues :175-198).
+//
+// Kernels (one launch each per solve):
+//   k_xfft<fwd>  rows of the k-plane, two rows per complex line (x: contiguous)
+//   k_yfft<fwd>  columns of the k-plane, two columns per complex line
+//   k_thomas / k_pdd   one wall-normal system per (x-slot, y-slot) column
+// Pivots and PDD spikes depend on the column only through its eigenvalue
+// lambda_x(ix) + lambda_y(jy), and slots p and n-p of a half-complex array
+// share the eigenvalue, so they are stored once per class
+// (ix <= nx/2, jy <= ny/2): a quarter of the reference's b array.
+#include <cmath>
+#include <cstring>
+
+#include "ppe.cuh"
+
+namespace pl {
+
+// ------------------------------------------------------------------------
+// FFT kernels
+// ------------------------------------------------------------------------
+
+// x direction.  CTA = `pb` row pairs (j = 2p, 2p+1) of plane k.  Input element
+// (i,j,k) at in[in_off + i + j*in_sj + k*in_sk]; output in the interior-only
+// layout (fwd) or at out[out_off + i + j*out_sj + k*out_sk] (bwd).
+template <typename T, bool FWD>
+__global__ void __launch_bounds__(256) k_xfft(const T *__restrict__ in, size_t in_off, size_t in_sj, size_t in_sk,
+                                              T *__restrict__ out, size_t out_off, size_t out_sj, size_t out_sk,
+                                              FftPlanDev<typename cplx_of<T>::type> plan, int ny, int pb, T scale)
+{
+    using V = typename cplx_of<T>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = plan.n; // = nx
+    V *buf0 = reinterpret_cast<V *>(smem_raw);
+    V *buf1 = buf0 + (size_t)pb * n;
+    const int k = blockIdx.y;
+    const int p0 = blockIdx.x * pb;
+    const int nb = min(pb, ny / 2 - p0);
+    const int tid = threadIdx.x, nthr = blockDim.x;
+
+    for (int e = tid; e < nb * 2 * n; e += nthr) {
+        const int m = e % n, r = (e / n) & 1, b = e / (2 * n);
+        const int j = 2 * (p0 + b) + r;
+        T val = in[in_off + (size_t)m + (size_t)j * in_sj + (size_t)k * in_sk];
+        reinterpret_cast<T *>(&buf0[(size_t)b * n + m])[r] = val;
+    }
+    __syncthreads();
+    if (FWD) {
+        V *res = fft_batch<V, true, false>(buf0, buf1, plan, nb, 1, n, tid, nthr);
+        for (int e = tid; e < nb * n; e += nthr) {
+            const int m = e % n, b = e / n;
+            V A = res[(size_t)b * n + m], Bc = res[(size_t)b * n + (m == 0 ? 0 : n - m)];
+            V h = split_hc(A, Bc, m, n);
+            const int j = 2 * (p0 + b);
+            out[out_off + (size_t)m + (size_t)j * out_sj + (size_t)k * out_sk] = h.x;
+            out[out_off + (size_t)m + (size_t)(j + 1) * out_sj + (size_t)k * out_sk] = h.y;
+        }
+    } else {
+        for (int e = tid; e < nb * n; e += nthr) {
+            const int m = e % n, b = e / n;
+            V P = buf0[(size_t)b * n + m], Q = buf0[(size_t)b * n + (m == 0 ? 0 : n - m)];
+            buf1[(size_t)b * n + m] = merge_hc(P, Q, m, n);
+        }
+        __syncthreads();
+        V *res = fft_batch<V, false, false>(buf1, buf0, plan, nb, 1, n, tid, nthr);
+        for (int e = tid; e < nb * n; e += nthr) {
+            const int m = e % n, b = e / n;
+            V z = res[(size_t)b * n + m];
+            const int j = 2 * (p0 + b);
+            out[out_off + (size_t)m + (size_t)j * out_sj + (size_t)k * out_sk] = z.x * scale;
+            out[out_off + (size_t)m + (size_t)(j + 1) * out_sj + (size_t)k * out_sk] = z.y * scale;
+        }
+    }
+}
+
+// y direction, in place on the interior-only array.  Columns 2c, 2c+1 of a row
+// are adjacent, so the complex line of pair c is the V-typed column c of the
+// plane viewed as [ny][nx/2] complex.  CTA = `w` pairs of plane k.
+template <typename T, bool FWD>
+__global__ void __launch_bounds__(256) k_yfft(T *__restrict__ data, FftPlanDev<typename cplx_of<T>::type> plan,
+                                              int nx, int w)
+{
+    using V = typename cplx_of<T>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = plan.n; // = ny
+    const int ncol = nx / 2;
+    V *buf0 = reinterpret_cast<V *>(smem_raw);
+    V *buf1 = buf0 + (size_t)w * n;
+    const int k = blockIdx.y;
+    const int c0 = blockIdx.x * w;
+    const int nb = min(w, ncol - c0);
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    V *plane = reinterpret_cast<V *>(data) + (size_t)k * n * ncol;
+
+    for (int e = tid; e < nb * n; e += nthr) {
+        const int c = e % nb, m = e / nb;
+        buf0[(size_t)m * w + c] = plane[(size_t)m * ncol + c0 + c];
+    }
+    __syncthreads();
+    if (FWD) {
+        V *res = fft_batch<V, true, true>(buf0, buf1, plan, nb, w, 1, tid, nthr);
+        for (int e = tid; e < nb * n; e += nthr) {
+            const int c = e % nb, m = e / nb;
+            V A = res[(size_t)m * w + c], Bc = res[(size_t)(m == 0 ? 0 : n - m) * w + c];
+            plane[(size_t)m * ncol + c0 + c] = split_hc(A, Bc, m, n);
+        }
+    } else {
+        for (int e = tid; e < nb * n; e += nthr) {
+            const int c = e % nb, m = e / nb;
+            V P = buf0[(size_t)m * w + c], Q = buf0[(size_t)(m == 0 ? 0 : n - m) * w + c];
+            buf1[(size_t)m * w + c] = merge_hc(P, Q, m, n);
+        }
+        __syncthreads();
+        V *res = fft_batch<V, false, true>(buf1, buf0, plan, nb, w, 1, tid, nthr);
+        for (int e = tid; e < nb * n; e += nthr) {
+            const int c = e % nb, m = e / nb;
+            plane[(size_t)m * ncol + c0 + c] = res[(size_t)m * w + c];
+        }
+    }
+}
+
+// ------------------------------------------------------------------------
+// Tridiagonal kernels (FP64 arithmetic in both precision modes)
+// ------------------------------------------------------------------------
+
+struct TridDev {
+    int nx, ny, nz, ncx, ncy;
+    const double *mult, *rb, *c;
+};
+
+__device__ __forceinline__ size_t trid_class(int px, int py, const TridDev &t)
+{
+    const int ix = min(px, t.nx - px), jy = min(py, t.ny - py);
+    return (size_t)ix + (size_t)t.ncx * jy;
+}
+
+constexpr int TRID_UNROLL = 8;
+
+// Thomas on rows [k0, k0+ke) of one column.  Reads the right-hand side from
+// `xin` (type T), keeps the forward-swept values in `xs` (double; may alias
+// xin when T is double) and writes the solution to `xout` (type T).
+template <typename T>
+__device__ __forceinline__ void thomas_column(const T *xin, double *xs, T *xout, size_t col, size_t cls,
+                                              size_t stride, size_t cstride, int k0, int ke, const TridDev &t)
+{
+    // forward elimination: x_k -= (a_k / b_{k-1}) x_{k-1}   (ssolve_trid :319-330)
+    double xp = (double)xin[col + (size_t)k0 * stride];
+    xs[col + (size_t)k0 * stride] = xp;
+    for (int kb = 1; kb < ke; kb += TRID_UNROLL) {
+        double xv[TRID_UNROLL], mv[TRID_UNROLL];
+#pragma unroll
+        for (int u = 0; u < TRID_UNROLL; u++) {
+            const int k = k0 + kb + u;
+            if (kb + u < ke) {
+                xv[u] = (double)xin[col + (size_t)k * stride];
+                mv[u] = __ldg(t.mult + cls + (size_t)k * cstride);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < TRID_UNROLL; u++) {
+            if (kb + u < ke) {
+                xp = xv[u] - mv[u] * xp;
+                xs[col + (size_t)(k0 + kb + u) * stride] = xp;
+            }
+        }
+    }
+    // last row: x /= b, or 0 where b == 0 (:332-344); rb holds 1/b or 0
+    const int kl = k0 + ke - 1;
+    xp = xp * __ldg(t.rb + cls + (size_t)kl * cstride);
+    xout[col + (size_t)kl * stride] = (T)xp;
+    // back substitution: x_k = (x_k - c_k x_{k+1}) / b_k   (:346-356)
+    for (int kb = ke - 2; kb >= 0; kb -= TRID_UNROLL) {
+        double xv[TRID_UNROLL], rv[TRID_UNROLL];
+#pragma unroll
+        for (int u = 0; u < TRID_UNROLL; u++) {
+            const int k = k0 + kb - u;
+            if (kb - u >= 0) {
+                xv[u] = xs[col + (size_t)k * stride];
+                rv[u] = __ldg(t.rb + cls + (size_t)k * cstride);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < TRID_UNROLL; u++) {
+            const int k = k0 + kb - u;
+            if (kb - u >= 0) {
+                xp = (xv[u] - __ldg(t.c + k) * xp) * rv[u];
+                xout[col + (size_t)k * stride] = (T)xp;
+            }
+        }
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128) k_thomas(const T *xin, double *xs, T *xout, TridDev t)
+{
+    const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y;
+    if (px >= t.nx) return;
+    const size_t col = (size_t)px + (size_t)t.nx * py, stride = (size_t)t.nx * t.ny;
+    const size_t cls = trid_class(px, py, t), cstride = (size_t)t.ncx * t.ncy;
+    thomas_column<T>(xin, xs, xout, col, cls, stride, cstride, 0, t.nz, t);
+}
+
+constexpr int PDD_MAX_PARTS = 64;
+
+struct PddDev {
+    int nparts;
+    int kst[PDD_MAX_PARTS], ksz[PDD_MAX_PARTS];
+    const double *v, *w, *tmpv;
+};
+
+// PDD (psolve_trid :361-466) for all nparts z-partitions of one column:
+// local Thomas per partition, then for each internal interface the truncated
+// 2x2 reduced system (:423-438), y3 of partition m becoming y1 of m+1
+// (:444-446), and the correction x -= v*y1 + w*y2 (:452-464).  The bottom
+// partition keeps y1 = 0 and the top one y2 = 0, as in the reference where
+// those arrays are zeroed at init and never received.
+template <typename T>
+__global__ void __launch_bounds__(128) k_pdd(double *xs, T *xout, TridDev t, PddDev p)
+{
+    const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y;
+    if (px >= t.nx) return;
+    const size_t col = (size_t)px + (size_t)t.nx * py, stride = (size_t)t.nx * t.ny;
+    const size_t cls = trid_class(px, py, t), cstride = (size_t)t.ncx * t.ncy;
+    // local solves in FP64, in place in xs
+    for (int m = 0; m < p.nparts; m++)
+        thomas_column<double>(xs, xs, xs, col, cls, stride, cstride, p.kst[m], p.ksz[m], t);
+    double y1 = 0.0;
+    for (int m = 0; m < p.nparts; m++) {
+        double y2 = 0.0, y3 = 0.0;
+        if (m + 1 < p.nparts) {
+            const int kt = p.kst[m] + p.ksz[m] - 1;
+            const double wt = __ldg(p.w + cls + (size_t)kt * cstride);
+            const double tv = __ldg(p.tmpv + cls + (size_t)m * cstride);
+            const double xt = xs[col + (size_t)kt * stride];
+            const double tvar = xs[col + (size_t)p.kst[m + 1] * stride];
+            const double det = wt * tv - 1.0;
+            y2 = (xt * tv - tvar) / det;
+            y3 = (tvar * wt - xt) / det;
+        }
+        for (int k = p.kst[m]; k < p.kst[m] + p.ksz[m]; k++) {
+            const size_t g = col + (size_t)k * stride;
+            const size_t gc = cls + (size_t)k * cstride;
+            xout[g] = (T)(xs[g] - __ldg(p.v + gc) * y1 - __ldg(p.w + gc) * y2);
+        }
+        y1 = y3;
+    }
+}
+
+// mixed path: widen the FP32 right-hand side into the FP64 sweep buffer
+__global__ void k_widen(const float *__restrict__ in, double *__restrict__ out, size_t n)
+{
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x)
+        out[q] = (double)in[q];
+}
+
+// ------------------------------------------------------------------------
+// Host plan
+// ------------------------------------------------------------------------
+
+static int factor_radices(int n, int *radix, int *nstages)
+{
+    int s = 0, m = n;
+    while (m % 4 == 0 && s < FFT_MAX_STAGES) {
+        radix[s++] = 4;
+        m /= 4;
+    }
+    if (m % 2 == 0 && s < FFT_MAX_STAGES) {
+        radix[s++] = 2;
+        m /= 2;
+    }
+    while (m % 3 == 0 && s < FFT_MAX_STAGES) {
+        radix[s++] = 3;
+        m /= 3;
+    }
+    if (m != 1) return -1;
+    *nstages = s;
+    return 0;
+}
+
+template <typename V> static int upload_twiddles(int n, V **dptr)
+{
+    std::vector<V> h(n);
+    const long double two_pi = 6.283185307179586476925286766559005768L;
+    for (int t = 0; t < n; t++) {
+        long double a = -two_pi * (long double)t / (long double)n;
+        h[t].x = (decltype(h[t].x))cosl(a);
+        h[t].y = (decltype(h[t].y))sinl(a);
+    }
+    PL_CUDA_TRY(cudaMalloc(dptr, sizeof(V) * n));
+    PL_CUDA_TRY(cudaMemcpy(*dptr, h.data(), sizeof(V) * n, cudaMemcpyHostToDevice));
+    return 0;
+}
+
+// decomp_2d.c:261-283
+static void distribute(int num, int nprocs, std::vector<int> &st0, std::vector<int> &sz)
+{
+    std::vector<int> st(nprocs), en(nprocs);
+    sz.assign(nprocs, 0);
+    int size = num / nprocs;
+    int nu = num - size * nprocs;
+    int nl = nprocs - nu;
+    st[0] = 1;
+    sz[0] = size;
+    en[0] = size;
+    for (int i = 1; i < nl; i++) {
+        st[i] = st[i - 1] + size;
+        sz[i] = size;
+        en[i] = en[i - 1] + size;
+    }
+    size++;
+    for (int i = nl; i < nprocs; i++) {
+        st[i] = en[i - 1] + 1;
+        sz[i] = size;
+        en[i] = en[i - 1] + size;
+    }
+    en[nprocs - 1] = num;
+    sz[nprocs - 1] = num - st[nprocs - 1] + 1;
+    st0.resize(nprocs);
+    for (int i = 0; i < nprocs; i++) st0[i] = st[i] - 1;
+}
+
+template <typename V> static void set_plan(FftPlanDev<V> &p, int n, const int *radix, int ns, const V *tw)
+{
+    p.n = n;
+    p.nstages = ns;
+    for (int s = 0; s < ns; s++) p.radix[s] = radix[s];
+    p.tw = tw;
+}
+
+int ppe_create(Ppe *s, int nx, int ny, int nz, double dx, double dy, const double *dzf_global, int nparts,
+               int prec)
+{
+    *s = Ppe();
+    if (nx < 2 || ny < 2 || nz < 1 || (nx & 1) || (ny & 1)) {
+        set_error("ppe_create: nx and ny must be even and >= 2, nz >= 1 (the reference requires even sizes, "
+                  "mod_parameters.f90:264-267)");
+        return -1;
+    }
+    if (nparts < 0 || nparts > PDD_MAX_PARTS || nparts > nz) {
+        set_error("ppe_create: PDD partition count must be in [0, min(nz, 64)]");
+        return -1;
+    }
+    s->nx = nx;
+    s->ny = ny;
+    s->nz = nz;
+    s->nparts = nparts;
+    s->prec = prec;
+    s->ncx = nx / 2 + 1;
+    s->ncy = ny / 2 + 1;
+    s->norm = 1.0 / (1.0 * nx * 1.0 * ny); // mod_fft_fftw.inc:154, PP/PP
+    const int P = nparts >= 1 ? nparts : 1;
+    distribute(nz, P, s->kst, s->ksz);
+
+    int rx[FFT_MAX_STAGES], ry[FFT_MAX_STAGES], nsx = 0, nsy = 0;
+    if (factor_radices(nx, rx, &nsx) || factor_radices(ny, ry, &nsy)) {
+        set_error("ppe_create: nx and ny must be of the form 2^a 3^b");
+        return -1;
+    }
+    if (upload_twiddles<double2>(nx, &s->d_twx64) || upload_twiddles<double2>(ny, &s->d_twy64) ||
+        upload_twiddles<float2>(nx, &s->d_twx32) || upload_twiddles<float2>(ny, &s->d_twy32))
+        return -1;
+    set_plan(s->px64, nx, rx, nsx, s->d_twx64);
+    set_plan(s->py64, ny, ry, nsy, s->d_twy64);
+    set_plan(s->px32, nx, rx, nsx, s->d_twx32);
+    set_plan(s->py32, ny, ry, nsy, s->d_twy32);
+
+    // eigenvalues, mod_poisson_solver.c:227-242 with mod_fft_fftw.inc:180-183
+    const double pi = acos(-1.0);
+    std::vector<double> lx(nx), ly(ny);
+    for (int i = 1; i <= nx; i++) lx[i - 1] = 2.0 * (cos(2.0 * pi * (i - 1.0) / nx) - 1.0);
+    for (int i = 0; i < nx; i++) lx[i] /= (dx * dx);
+    for (int i = 1; i <= ny; i++) ly[i - 1] = 2.0 * (cos(2.0 * pi * (i - 1.0) / ny) - 1.0);
+    for (int i = 0; i < ny; i++) ly[i] /= (dy * dy);
+
+    // coefficients per partition (set_trid_coeff :40-103, 'c', NN), pivots
+    // (:255-276) and PDD spikes (init_pdd_array :105-170), per class
+    const size_t ncls = (size_t)s->ncx * s->ncy;
+    std::vector<double> a(nz), c(nz), bt(nz);
+    std::vector<double> mult(ncls * nz), rb(ncls * nz), b(nz), v, w, tmpv;
+    if (nparts >= 1) {
+        v.assign(ncls * nz, 0.0);
+        w.assign(ncls * nz, 0.0);
+        tmpv.assign(ncls * P, 0.0);
+    }
+    for (int m = 0; m < P; m++) {
+        const int k0 = s->kst[m], ke = s->ksz[m];
+        const double *dzf = dzf_global + k0; // dzf_global[st-1+i], i = 0..ke+1
+        for (int k = 0; k < ke; k++) {
+            a[k0 + k] = 2.0 / (dzf[k + 1] * (dzf[k] + dzf[k + 1]));
+            c[k0 + k] = 2.0 / (dzf[k + 1] * (dzf[k + 2] + dzf[k + 1]));
+        }
+        for (int k = 0; k < ke; k++) bt[k0 + k] = -a[k0 + k] - c[k0 + k];
+        const double factor = 1.0; // 'N'
+        if (m == 0) {
+            bt[k0] += factor * a[k0];
+            a[k0] *= fabs(factor) - 1.0;
+        }
+        if (m == P - 1) {
+            bt[k0 + ke - 1] += factor * c[k0 + ke - 1];
+            c[k0 + ke - 1] *= fabs(factor) - 1.0;
+        }
+    }
+    std::vector<double> a_orig = a, c_orig = c;
+    for (int jy = 0; jy < s->ncy; jy++)
+        for (int ix = 0; ix < s->ncx; ix++) {
+            const size_t cl = (size_t)ix + (size_t)s->ncx * jy;
+            const double lam = lx[ix] + ly[jy];
+            for (int m = 0; m < P; m++) {
+                const int k0 = s->kst[m], ke = s->ksz[m];
+                for (int k = 0; k < ke; k++) b[k0 + k] = bt[k0 + k] + lam;
+                mult[cl + ncls * k0] = 0.0;
+                for (int k = 1; k < ke; k++) {
+                    double a_tmp = a[k0 + k] / b[k0 + k - 1];
+                    b[k0 + k] -= (a_tmp * c[k0 + k - 1]);
+                    mult[cl + ncls * (k0 + k)] = a_tmp;
+                }
+                for (int k = 0; k < ke; k++) rb[cl + ncls * (k0 + k)] = (b[k0 + k] != 0.0) ? 1.0 / b[k0 + k] : 0.0;
+                if (nparts >= 1) {
+                    // spikes with the partition's original a[0], c[ke-1]
+                    std::vector<double> vv(ke, 0.0), ww(ke, 0.0);
+                    vv[0] = a_orig[k0];
+                    ww[ke - 1] = c_orig[k0 + ke - 1];
+                    for (int k = 1; k < ke; k++) {
+                        double a_tmp = a[k0 + k] / b[k0 + k - 1];
+                        vv[k] -= a_tmp * vv[k - 1];
+                        ww[k] -= a_tmp * ww[k - 1];
+                    }
+                    if (b[k0 + ke - 1] != 0.0) {
+                        vv[ke - 1] /= b[k0 + ke - 1];
+                        ww[ke - 1] /= b[k0 + ke - 1];
+                    } else {
+                        vv[ke - 1] = 0.0;
+                        ww[ke - 1] = 0.0;
+                    }
+                    for (int k = ke - 2; k >= 0; k--) {
+                        vv[k] = (vv[k] - c[k0 + k] * vv[k + 1]) / b[k0 + k];
+                        ww[k] = (ww[k] - c[k0 + k] * ww[k + 1]) / b[k0 + k];
+                    }
+                    for (int k = 0; k < ke; k++) {
+                        v[cl + ncls * (k0 + k)] = vv[k];
+                        w[cl + ncls * (k0 + k)] = ww[k];
+                    }
+                }
+            }
+            if (nparts >= 1)
+                for (int m = 0; m + 1 < P; m++) tmpv[cl + ncls * m] = v[cl + ncls * s->kst[m + 1]];
+        }
+    // the PDD zeroing of a[0], c[ke-1] (:132-133) does not enter the local
+    // sweeps (they read a[k>=1] and c[k<=ke-2]); c is uploaded as set above
+    PL_CUDA_TRY(cudaMalloc(&s->d_mult, sizeof(double) * ncls * nz));
+    PL_CUDA_TRY(cudaMalloc(&s->d_rb, sizeof(double) * ncls * nz));
+    PL_CUDA_TRY(cudaMalloc(&s->d_c, sizeof(double) * nz));
+    PL_CUDA_TRY(cudaMemcpy(s->d_mult, mult.data(), sizeof(double) * ncls * nz, cudaMemcpyHostToDevice));
+    PL_CUDA_TRY(cudaMemcpy(s->d_rb, rb.data(), sizeof(double) * ncls * nz, cudaMemcpyHostToDevice));
+    PL_CUDA_TRY(cudaMemcpy(s->d_c, c.data(), sizeof(double) * nz, cudaMemcpyHostToDevice));
+    if (nparts >= 1) {
+        PL_CUDA_TRY(cudaMalloc(&s->d_v, sizeof(double) * ncls * nz));
+        PL_CUDA_TRY(cudaMalloc(&s->d_w, sizeof(double) * ncls * nz));
+        PL_CUDA_TRY(cudaMalloc(&s->d_tmpv, sizeof(double) * ncls * P));
+        PL_CUDA_TRY(cudaMemcpy(s->d_v, v.data(), sizeof(double) * ncls * nz, cudaMemcpyHostToDevice));
+        PL_CUDA_TRY(cudaMemcpy(s->d_w, w.data(), sizeof(double) * ncls * nz, cudaMemcpyHostToDevice));
+        PL_CUDA_TRY(cudaMemcpy(s->d_tmpv, tmpv.data(), sizeof(double) * ncls * P, cudaMemcpyHostToDevice));
+    }
+    if (prec == PREC_MIXED || nparts >= 1) {
+        s->scratch_elems = (size_t)nx * ny * nz;
+        PL_CUDA_TRY(cudaMalloc(&s->d_scratch, sizeof(double) * s->scratch_elems));
+    }
+    // kernels with > 48 KB of dynamic shared memory
+    PL_CUDA_TRY(cudaFuncSetAttribute(k_yfft<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    PL_CUDA_TRY(cudaFuncSetAttribute(k_yfft<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    PL_CUDA_TRY(cudaFuncSetAttribute(k_yfft<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    PL_CUDA_TRY(cudaFuncSetAttribute(k_yfft<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    PL_CUDA_TRY(cudaFuncSetAttribute(k_xfft<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    PL_CUDA_TRY(cudaFuncSetAttribute(k_xfft<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    PL_CUDA_TRY(cudaFuncSetAttribute(k_xfft<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    PL_CUDA_TRY(cudaFuncSetAttribute(k_xfft<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    return 0;
+}
+
+void ppe_destroy(Ppe *s)
+{
+    cudaFree(s->d_twx64);
+    cudaFree(s->d_twy64);
+    cudaFree(s->d_twx32);
+    cudaFree(s->d_twy32);
+    cudaFree(s->d_mult);
+    cudaFree(s->d_rb);
+    cudaFree(s->d_c);
+    cudaFree(s->d_v);
+    cudaFree(s->d_w);
+    cudaFree(s->d_tmpv);
+    cudaFree(s->d_scratch);
+    cudaFree(s->d_mode0);
+    *s = Ppe();
+}
+
+// launch geometry ---------------------------------------------------------
+static int x_pairs_per_cta(int nx, int ny)
+{
+    int pb = 1024 / nx;
+    if (pb < 1) pb = 1;
+    if (pb > ny / 2) pb = ny / 2;
+    return pb;
+}
+
+static int y_cols_per_cta(int nx, int ny)
+{
+    int w = 2048 / ny;
+    if (w < 1) w = 1;
+    if (w > 8) w = 8;
+    if (w > nx / 2) w = nx / 2;
+    return w;
+}
+
+template <typename T>
+static int launch_x(const Ppe *s, bool fwd, const T *in, size_t in_off, size_t in_sj, size_t in_sk, T *out,
+                    size_t out_off, size_t out_sj, size_t out_sk, T scale, cudaStream_t st)
+{
+    using V = typename cplx_of<T>::type;
+    const int pb = x_pairs_per_cta(s->nx, s->ny);
+    dim3 grid((s->ny / 2 + pb - 1) / pb, s->nz);
+    const size_t shm = 2 * sizeof(V) * (size_t)pb * s->nx;
+    const FftPlanDev<V> &plan = *reinterpret_cast<const FftPlanDev<V> *>(
+        sizeof(T) == 8 ? (const void *)&s->px64 : (const void *)&s->px32);
+    if (fwd)
+        k_xfft<T, true><<<grid, 256, shm, st>>>(in, in_off, in_sj, in_sk, out, out_off, out_sj, out_sk, plan, s->ny,
+                                                pb, scale);
+    else
+        k_xfft<T, false><<<grid, 256, shm, st>>>(in, in_off, in_sj, in_sk, out, out_off, out_sj, out_sk, plan,
+                                                 s->ny, pb, scale);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
+template <typename T> static int launch_y(const Ppe *s, bool fwd, T *data, cudaStream_t st)
+{
+    using V = typename cplx_of<T>::type;
+    const int w = y_cols_per_cta(s->nx, s->ny);
+    dim3 grid((s->nx / 2 + w - 1) / w, s->nz);
+    const size_t shm = 2 * sizeof(V) * (size_t)w * s->ny;
+    const FftPlanDev<V> &plan = *reinterpret_cast<const FftPlanDev<V> *>(
+        sizeof(T) == 8 ? (const void *)&s->py64 : (const void *)&s->py32);
+    if (fwd)
+        k_yfft<T, true><<<grid, 256, shm, st>>>(data, plan, s->nx, w);
+    else
+        k_yfft<T, false><<<grid, 256, shm, st>>>(data, plan, s->nx, w);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
+template <typename T> static int launch_trid(Ppe *s, T *x, cudaStream_t st)
+{
+    TridDev t{s->nx, s->ny, s->nz, s->ncx, s->ncy, s->d_mult, s->d_rb, s->d_c};
+    dim3 grid((s->nx + 127) / 128, s->ny);
+    double *xs = (sizeof(T) == 8 && s->nparts == 0) ? reinterpret_cast<double *>(x) : s->d_scratch;
+    if (s->nparts == 0) {
+        k_thomas<T><<<grid, 128, 0, st>>>(x, xs, x, t);
+    } else {
+        if (sizeof(T) == 4) {
+            k_widen<<<1184, 256, 0, st>>>(reinterpret_cast<const float *>(x), xs, s->scratch_elems);
+            PL_CHECK_LAUNCH();
+        } else {
+            PL_CUDA_TRY(cudaMemcpyAsync(xs, x, sizeof(double) * s->scratch_elems, cudaMemcpyDeviceToDevice, st));
+        }
+        PddDev p{};
+        p.nparts = s->nparts;
+        for (int m = 0; m < s->nparts; m++) {
+            p.kst[m] = s->kst[m];
+            p.ksz[m] = s->ksz[m];
+        }
+        p.v = s->d_v;
+        p.w = s->d_w;
+        p.tmpv = s->d_tmpv;
+        k_pdd<T><<<grid, 128, 0, st>>>(xs, x, t, p);
+    }
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
+static inline void mark(const Ppe *s, const char *name)
+{
+    if (s->mark) s->mark(s->mark_ctx, name);
+}
+
+int ppe_solve_fp64_strided(Ppe *s, const double *in, double *out, size_t off, size_t sj, size_t sk,
+                           double *d_work, cudaStream_t st)
+{
+    const size_t nxl = s->nx, nxy = (size_t)s->nx * s->ny;
+    if (launch_x<double>(s, true, in, off, sj, sk, d_work, 0, nxl, nxy, 1.0, st)) return -1;
+    mark(s, "ppe_xfft_fwd");
+    if (launch_y<double>(s, true, d_work, st)) return -1;
+    mark(s, "ppe_yfft_fwd");
+    if (launch_trid<double>(s, d_work, st)) return -1;
+    mark(s, s->nparts ? "ppe_pdd" : "ppe_thomas");
+    if (launch_y<double>(s, false, d_work, st)) return -1;
+    mark(s, "ppe_yfft_bwd");
+    if (launch_x<double>(s, false, d_work, 0, nxl, nxy, out, off, sj, sk, s->norm, st)) return -1;
+    mark(s, "ppe_xfft_bwd");
+    return 0;
+}
+
+int ppe_solve_fp64(Ppe *s, double *d_var, cudaStream_t st)
+{
+    const size_t nxl = s->nx, nxy = (size_t)s->nx * s->ny;
+    return ppe_solve_fp64_strided(s, d_var, d_var, 0, nxl, nxy, d_var, st);
+}
+
+int ppe_solve_fp32(Ppe *s, float *d_var, cudaStream_t st)
+{
+    const size_t nxl = s->nx, nxy = (size_t)s->nx * s->ny;
+    if (launch_x<float>(s, true, d_var, 0, nxl, nxy, d_var, 0, nxl, nxy, 1.0f, st)) return -1;
+    mark(s, "ppe_xfft_fwd");
+    if (launch_y<float>(s, true, d_var, st)) return -1;
+    mark(s, "ppe_yfft_fwd");
+    if (launch_trid<float>(s, d_var, st)) return -1;
+    mark(s, s->nparts ? "ppe_pdd" : "ppe_thomas");
+    if (launch_y<float>(s, false, d_var, st)) return -1;
+    mark(s, "ppe_yfft_bwd");
+    if (launch_x<float>(s, false, d_var, 0, nxl, nxy, d_var, 0, nxl, nxy, (float)s->norm, st)) return -1;
+    mark(s, "ppe_xfft_bwd");
+    return 0;
+}
+
+} // namespace pl

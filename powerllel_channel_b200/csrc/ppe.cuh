@@ -1,0 +1,66 @@
+// ppe.cuh -- pressure Poisson solver (PPE) on one B200: host-side plan.
+//
+// Restates src/src_c/mod_poisson_solver.c for one GPU holding the whole
+// domain (the reference's 1x1 decomposition, where every pencil transpose is
+// an identity: mod_poisson_solver.c:195-206,501,538,578):
+//   forward R2HC along x and y, one tridiagonal system per half-complex slot
+//   (Thomas, :311-359, or PDD over P z-partitions, :105-176 and :361-466),
+//   backward HC2R along y and x, scale by 1/(nx*ny) (:587-599).
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+#include "fft.cuh"
+
+namespace pl {
+
+enum Precision { PREC_FP64 = 0, PREC_MIXED = 1 };
+
+struct Ppe {
+    int nx = 0, ny = 0, nz = 0;
+    int nparts = 0; // 0: Thomas, >= 1: PDD with nparts z-partitions
+    int prec = PREC_FP64;
+    int ncx = 0, ncy = 0; // eigenvalue classes: nx/2+1, ny/2+1
+    double norm = 1.0;
+    std::vector<int> kst, ksz; // partition start (0-based) and size
+
+    // FFT plans (both precisions share the radix lists)
+    FftPlanDev<double2> px64{}, py64{};
+    FftPlanDev<float2> px32{}, py32{};
+    double2 *d_twx64 = nullptr, *d_twy64 = nullptr;
+    float2 *d_twx32 = nullptr, *d_twy32 = nullptr;
+
+    // tridiagonal coefficients, per eigenvalue class (ix <= nx/2, jy <= ny/2)
+    // layout [k][jy][ix]; mult[k] = a[k]/b[k-1] (k-th row of each partition,
+    // 0 at a partition's first row), rb[k] = 1/b[k] (0 where b == 0)
+    double *d_mult = nullptr, *d_rb = nullptr;
+    double *d_c = nullptr;   // c[k], nz (partition-local values)
+    double *d_v = nullptr, *d_w = nullptr; // PDD spikes, class tables
+    double *d_tmpv = nullptr;              // PDD: v of partition m+1 at its k=0, [m][jy][ix]
+    double *d_scratch = nullptr;           // mixed path: FP64 forward-sweep values
+    size_t scratch_elems = 0;
+
+    // (0,0) mode (mixed path): FP64 plane sums of the right-hand side
+    double *d_mode0 = nullptr;
+
+    // optional per-launch marker (profiling): called after every kernel launch
+    void (*mark)(void *ctx, const char *name) = nullptr;
+    void *mark_ctx = nullptr;
+};
+
+int ppe_create(Ppe *s, int nx, int ny, int nz, double dx, double dy, const double *dzf_global, int nparts,
+               int prec);
+void ppe_destroy(Ppe *s);
+
+// In-place solve on the interior-only device array (layout [k][j][i]).
+int ppe_solve_fp64(Ppe *s, double *d_var, cudaStream_t st);
+int ppe_solve_fp32(Ppe *s, float *d_var, cudaStream_t st);
+
+// Solve reading from / writing to a strided device array (the reference's
+// ghosted layout): element (i,j,k), 0-based interior, at base[off + i +
+// j*sj + k*sk].  The interior-only work array receives the transform.
+int ppe_solve_fp64_strided(Ppe *s, const double *in, double *out, size_t off, size_t sj, size_t sk,
+                           double *d_work, cudaStream_t st);
+
+} // namespace pl

@@ -1,0 +1,640 @@
+// stencil.cu -- RK2 momentum stencils, divergence, projection, forcing, wall
+// fills, diagnostics and the initial field.
+//
+// One thread per grid point, (i, j) over the block, k over blockIdx.z;
+// neighbour values come through L1/L2 (each field is streamed from HBM once).
+// x and y neighbours wrap periodically; the wall ghost planes k = 0, nz+1 are
+// stored and refreshed by the kernel that writes the adjacent interior plane,
+// which reproduces imposeNoSlipBC (mod_updateBound.f90:312-368) applied after
+// the periodic fills.
+#include "stencil.cuh"
+
+namespace pl {
+
+// ------------------------------------------------------------------------
+// momentum right-hand side (timeIntVelRK1_kernel, mod_calcVel.f90:74-138;
+// timeIntVelRK2_kernel evaluates the same expressions on u1, :262-326)
+// ------------------------------------------------------------------------
+struct Nb {
+    size_t c, xm, xp, ym, yp, zm, zp, xpym, xmyp, xpzm, xmzp, ypzm, ymzp;
+};
+
+__device__ __forceinline__ Nb neighbours(int i, int j, int k, int nx, int ny)
+{
+    const int im = (i == 0) ? nx - 1 : i - 1, ip = (i == nx - 1) ? 0 : i + 1;
+    const int jm = (j == 0) ? ny - 1 : j - 1, jp = (j == ny - 1) ? 0 : j + 1;
+    const size_t sk = (size_t)nx * ny;
+    const size_t row = (size_t)nx * j + sk * k, rowm = (size_t)nx * jm + sk * k, rowp = (size_t)nx * jp + sk * k;
+    Nb n;
+    n.c = row + i;
+    n.xm = row + im;
+    n.xp = row + ip;
+    n.ym = rowm + i;
+    n.yp = rowp + i;
+    n.zm = n.c - sk;
+    n.zp = n.c + sk;
+    n.xpym = rowm + ip; // (i+1, j-1)
+    n.xmyp = rowp + im; // (i-1, j+1)
+    n.xpzm = n.xp - sk; // (i+1, k-1)
+    n.xmzp = n.xm + sk; // (i-1, k+1)
+    n.ypzm = n.yp - sk; // (j+1, k-1)
+    n.ymzp = n.ym + sk; // (j-1, k+1)
+    return n;
+}
+
+// Field accessor: plain load converted to the compute type.
+template <typename TS, typename TC> struct LoadF {
+    const TS *__restrict__ a;
+    __device__ __forceinline__ TC operator()(size_t q) const { return (TC)__ldg(a + q); }
+};
+
+// Accessor of the mixed path's stage-1 field u1 = u + d1 (u FP64, d1 FP32),
+// rounded to FP32 for the FP32 stencil arithmetic.
+struct LoadSum {
+    const double *__restrict__ a;
+    const float *__restrict__ d;
+    __device__ __forceinline__ float operator()(size_t q) const
+    {
+        return (float)(__ldg(a + q) + (double)__ldg(d + q));
+    }
+};
+
+template <typename TC, typename AU, typename AV, typename AW>
+__device__ __forceinline__ void momentum_rhs(const AU &u, const AV &v, const AW &w, const Nb &n, int k,
+                                             const StepParams &p, const MeshDev &m, TC &ru, TC &rv, TC &rw)
+{
+    const TC dx_inv = (TC)p.dx_inv, dy_inv = (TC)p.dy_inv, re_inv = (TC)p.re_inv, u_crf = (TC)p.u_crf;
+    const TC dzf_k = (TC)__ldg(m.dzf + k), dzf_kp = (TC)__ldg(m.dzf + k + 1), dzf_km = (TC)__ldg(m.dzf + k - 1);
+    const TC dzci_k = (TC)__ldg(m.dzc_inv + k), dzci_km = (TC)__ldg(m.dzc_inv + k - 1);
+    const TC dzfi_k = (TC)__ldg(m.dzf_inv + k), dzfi_kp = (TC)__ldg(m.dzf_inv + k + 1);
+    const TC h = (TC)0.25, half = (TC)0.5;
+
+    const TC uc = u(n.c), uxp = u(n.xp), uxm = u(n.xm), uyp = u(n.yp), uym = u(n.ym), uzp = u(n.zp), uzm = u(n.zm);
+    const TC vc = v(n.c), vxp = v(n.xp), vxm = v(n.xm), vyp = v(n.yp), vym = v(n.ym), vzp = v(n.zp), vzm = v(n.zm);
+    const TC wc = w(n.c), wxp = w(n.xp), wxm = w(n.xm), wyp = w(n.yp), wym = w(n.ym), wzp = w(n.zp), wzm = w(n.zm);
+    TC ue, uw, un, us, ut, ub, vn, vs, wt, wb, ve, vw, vt, vb, we, ww, wn, ws;
+    TC dqe, dqw, dqn, dqs, dqt, dqb, conv, visc;
+
+    // u-equation (:74-94)
+    ue = (uc + uxp);
+    uw = (uxm + uc);
+    un = (uc + uyp);
+    us = (uym + uc);
+    ut = (uc * dzf_kp + uzp * dzf_k) * dzci_k;
+    ub = (uc * dzf_km + uzm * dzf_k) * dzci_km;
+    vn = (vc + vxp);
+    vs = (vym + v(n.xpym));
+    wt = (wc + wxp);
+    wb = (wzm + w(n.xpzm));
+    dqe = (uxp - uc) * dx_inv;
+    dqw = (uc - uxm) * dx_inv;
+    dqn = (uyp - uc) * dy_inv;
+    dqs = (uc - uym) * dy_inv;
+    dqt = (uzp - uc) * dzci_k;
+    dqb = (uc - uzm) * dzci_km;
+    conv = h * ((ue * ue - uw * uw) * dx_inv + (un * vn - us * vs) * dy_inv + (ut * wt - ub * wb) * dzfi_k);
+    conv = conv + half * u_crf * (ue - uw) * dx_inv;
+    visc = ((dqe - dqw) * dx_inv + (dqn - dqs) * dy_inv + (dqt - dqb) * dzfi_k) * re_inv;
+    ru = visc - conv;
+
+    // v-equation (:96-116)
+    ve = (vc + vxp);
+    vw = (vxm + vc);
+    vn = (vc + vyp);
+    vs = (vym + vc);
+    vt = (vc * dzf_kp + vzp * dzf_k) * dzci_k;
+    vb = (vc * dzf_km + vzm * dzf_k) * dzci_km;
+    ue = (uc + uyp);
+    uw = (uxm + u(n.xmyp));
+    wt = (wc + wyp);
+    wb = (wzm + w(n.ypzm));
+    dqe = (vxp - vc) * dx_inv;
+    dqw = (vc - vxm) * dx_inv;
+    dqn = (vyp - vc) * dy_inv;
+    dqs = (vc - vym) * dy_inv;
+    dqt = (vzp - vc) * dzci_k;
+    dqb = (vc - vzm) * dzci_km;
+    conv = h * ((ue * ve - uw * vw) * dx_inv + (vn * vn - vs * vs) * dy_inv + (wt * vt - wb * vb) * dzfi_k);
+    conv = conv + half * u_crf * (ve - vw) * dx_inv;
+    visc = ((dqe - dqw) * dx_inv + (dqn - dqs) * dy_inv + (dqt - dqb) * dzfi_k) * re_inv;
+    rv = visc - conv;
+
+    // w-equation (:118-138)
+    we = (wc + wxp);
+    ww = (wxm + wc);
+    wn = (wc + wyp);
+    ws = (wym + wc);
+    wt = (wc + wzp);
+    wb = (wc + wzm);
+    ue = (uc * dzf_kp + uzp * dzf_k) * dzci_k;
+    uw = (uxm * dzf_kp + u(n.xmzp) * dzf_k) * dzci_k;
+    vn = (vc * dzf_kp + vzp * dzf_k) * dzci_k;
+    vs = (vym * dzf_kp + v(n.ymzp) * dzf_k) * dzci_k;
+    dqe = (wxp - wc) * dx_inv;
+    dqw = (wc - wxm) * dx_inv;
+    dqn = (wyp - wc) * dy_inv;
+    dqs = (wc - wym) * dy_inv;
+    dqt = (wzp - wc) * dzfi_kp;
+    dqb = (wc - wzm) * dzfi_k;
+    conv = h * ((ue * we - uw * ww) * dx_inv + (vn * wn - vs * ws) * dy_inv + (wt * wt - wb * wb) * dzci_k);
+    conv = conv + half * u_crf * (we - ww) * dx_inv;
+    visc = ((dqe - dqw) * dx_inv + (dqn - dqs) * dy_inv + (dqt - dqb) * dzci_k) * re_inv;
+    rw = visc - conv;
+}
+
+#define PL_POINT_INDEX()                                                                   \
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;                                   \
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;                                   \
+    const int k = blockIdx.z + 1;                                                          \
+    if (i >= p.nx || j >= p.ny) return;                                                    \
+    const size_t sk = (size_t)p.nx * p.ny;
+
+// wall fills of imposeNoSlipBC for the plane just written (k == 1 or nz)
+template <typename T>
+__device__ __forceinline__ void wall_fill(T *u, T *v, T *w, size_t c, int k, size_t sk, int nz, T bcu, T uval,
+                                          T vval)
+{
+    if (k == 1) {
+        u[c - sk] = (T)2.0 * bcu - uval;
+        v[c - sk] = -vval;
+        w[c - sk] = (T)0;
+    }
+    if (k == nz) {
+        u[c + sk] = (T)2.0 * bcu - uval;
+        v[c + sk] = -vval;
+        w[c] = (T)0;
+        w[c + sk] = (T)0;
+    }
+}
+
+// RK1: u1 = u + dt*(visc - conv) (mod_calcVel.f90:94,116,138) + wall fill
+__global__ void __launch_bounds__(256) k_rk1_fp64(const double *__restrict__ u, const double *__restrict__ v,
+                                                  const double *__restrict__ w, double *__restrict__ u1,
+                                                  double *__restrict__ v1, double *__restrict__ w1, StepParams p,
+                                                  MeshDev m)
+{
+    PL_POINT_INDEX();
+    const Nb n = neighbours(i, j, k, p.nx, p.ny);
+    double ru, rv, rw;
+    momentum_rhs<double>(LoadF<double, double>{u}, LoadF<double, double>{v}, LoadF<double, double>{w}, n, k, p, m,
+                         ru, rv, rw);
+    const double nu = __ldg(u + n.c) + p.dt * ru;
+    const double nv = __ldg(v + n.c) + p.dt * rv;
+    u1[n.c] = nu;
+    v1[n.c] = nv;
+    if (k != p.nz) w1[n.c] = __ldg(w + n.c) + p.dt * rw;
+    wall_fill<double>(u1, v1, w1, n.c, k, sk, p.nz, 0.0 - p.u_crf, nu, nv);
+}
+
+// RK2: u = (u1 + dt*(visc - conv)(u1) + u) * 0.5 (:282,304,326) + wall fill.
+// u is read at the centre only, so the update is in place.
+__global__ void __launch_bounds__(256) k_rk2_fp64(double *u, double *v, double *w, const double *__restrict__ u1,
+                                                  const double *__restrict__ v1, const double *__restrict__ w1,
+                                                  StepParams p, MeshDev m)
+{
+    PL_POINT_INDEX();
+    const Nb n = neighbours(i, j, k, p.nx, p.ny);
+    double ru, rv, rw;
+    momentum_rhs<double>(LoadF<double, double>{u1}, LoadF<double, double>{v1}, LoadF<double, double>{w1}, n, k, p,
+                         m, ru, rv, rw);
+    const double nu = (__ldg(u1 + n.c) + p.dt * ru + u[n.c]) * 0.5;
+    const double nv = (__ldg(v1 + n.c) + p.dt * rv + v[n.c]) * 0.5;
+    u[n.c] = nu;
+    v[n.c] = nv;
+    if (k != p.nz) w[n.c] = (__ldg(w1 + n.c) + p.dt * rw + w[n.c]) * 0.5;
+    wall_fill<double>(u, v, w, n.c, k, sk, p.nz, 0.0 - p.u_crf, nu, nv);
+}
+
+// calcRHS (mod_calcRHS.f90:19-33): rhs = div(u)/dt into the interior-only array
+__global__ void __launch_bounds__(256) k_calc_rhs_fp64(const double *__restrict__ u, const double *__restrict__ v,
+                                                       const double *__restrict__ w, double *__restrict__ rhs,
+                                                       StepParams p, MeshDev m)
+{
+    PL_POINT_INDEX();
+    const Nb n = neighbours(i, j, k, p.nx, p.ny);
+    const double dti = 1.0 / p.dt, dtidxi = dti * p.dx_inv, dtidyi = dti * p.dy_inv;
+    rhs[n.c - sk] = (__ldg(u + n.c) - __ldg(u + n.xm)) * dtidxi + (__ldg(v + n.c) - __ldg(v + n.ym)) * dtidyi +
+                    (__ldg(w + n.c) - __ldg(w + n.zm)) * dti * __ldg(m.dzf_inv + k);
+}
+
+// block-wide sum of three values; result valid in thread 0
+__device__ __forceinline__ void block_sum3(double &a, double &b, double &c)
+{
+    __shared__ double sh[3][32];
+    const int lane = (threadIdx.x + threadIdx.y * blockDim.x) & 31;
+    const int wid = (threadIdx.x + threadIdx.y * blockDim.x) >> 5;
+    const int nw = (blockDim.x * blockDim.y + 31) >> 5;
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+        c += __shfl_down_sync(0xffffffffu, c, o);
+    }
+    if (lane == 0) {
+        sh[0][wid] = a;
+        sh[1][wid] = b;
+        sh[2][wid] = c;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        a = lane < nw ? sh[0][lane] : 0.0;
+        b = lane < nw ? sh[1][lane] : 0.0;
+        c = lane < nw ? sh[2][lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_down_sync(0xffffffffu, a, o);
+            b += __shfl_down_sync(0xffffffffu, b, o);
+            c += __shfl_down_sync(0xffffffffu, c, o);
+        }
+    }
+}
+
+// correctVel (mod_calcVel.f90:436-450) + dz-weighted sums for Mean_h
+// (mod_utils.f90:105-131) of the corrected components + wall fill of v.
+// p is interior-only; p(nz+1) = p(nz) (imposeZeroGradBC) makes the w
+// correction of the top plane zero.
+template <typename TP>
+__global__ void __launch_bounds__(256) k_correct(const TP *__restrict__ pp, double *u, double *v, double *w,
+                                                 StepParams p, MeshDev m, double *partial)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z + 1;
+    double su = 0.0, sv = 0.0, sw = 0.0;
+    if (i < p.nx && j < p.ny) {
+        const size_t sk = (size_t)p.nx * p.ny;
+        const Nb n = neighbours(i, j, k, p.nx, p.ny);
+        const double dt = p.dt, dtdxi = dt * p.dx_inv, dtdyi = dt * p.dy_inv;
+        const size_t pc = n.c - sk;
+        const double p0 = (double)__ldg(pp + pc);
+        const double pxp = (double)__ldg(pp + n.xp - sk), pyp = (double)__ldg(pp + n.yp - sk);
+        const double pzp = (k < p.nz) ? (double)__ldg(pp + pc + sk) : p0;
+        const double nu = u[n.c] - (pxp - p0) * dtdxi;
+        const double nv = v[n.c] - (pyp - p0) * dtdyi;
+        const double nw = w[n.c] - (pzp - p0) * dt * __ldg(m.dzc_inv + k);
+        u[n.c] = nu;
+        v[n.c] = nv;
+        w[n.c] = nw;
+        // wall fill of the corrected u, v (w(0) = w(nz) = 0 are unchanged);
+        // a forced component is refilled after its shift by k_force
+        const double bcu = 0.0 - p.u_crf;
+        if (k == 1) {
+            u[n.c - sk] = 2.0 * bcu - nu;
+            v[n.c - sk] = -nv;
+        }
+        if (k == p.nz) {
+            u[n.c + sk] = 2.0 * bcu - nu;
+            v[n.c + sk] = -nv;
+        }
+        const double wz = __ldg(m.dzflzi + k);
+        su = nu * wz;
+        sv = nv * wz;
+        sw = nw * wz;
+    }
+    block_sum3(su, sv, sw);
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        const size_t b = blockIdx.x + (size_t)gridDim.x * (blockIdx.y + (size_t)gridDim.y * blockIdx.z);
+        const size_t nb = (size_t)gridDim.x * gridDim.y * gridDim.z;
+        partial[b] = su;
+        partial[nb + b] = sv;
+        partial[2 * nb + b] = sw;
+    }
+}
+
+// fixed-order final sum of the block partials (deterministic), then
+// Mean_h = sum / nx / ny and the forceVel shift vel_force - mean
+__global__ void k_finish_means(const double *partial, int nb, double dnx, double dny, double f0, double f1,
+                               double f2, double *scalar)
+{
+    const int comp = blockIdx.x;
+    double s = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) s += partial[(size_t)comp * nb + b];
+    __shared__ double sh[1024];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double mean = sh[0] / dnx / dny; // Mean_h/nx_global/ny_global (mod_utils.f90:128)
+        scalar[comp] = mean;
+        const double f = comp == 0 ? f0 : (comp == 1 ? f1 : f2);
+        scalar[3 + comp] = f - mean;
+    }
+}
+
+// forceVel (mod_calcVel.f90:463-506) + wall fill of the forced components
+__global__ void __launch_bounds__(256) k_force(double *u, double *v, double *w, StepParams p, int fx, int fy,
+                                               int fz, const double *scalar)
+{
+    PL_POINT_INDEX();
+    const size_t c = (size_t)i + (size_t)p.nx * j + sk * k;
+    const double bcu = 0.0 - p.u_crf;
+    if (fx) {
+        const double nu = u[c] + scalar[3];
+        u[c] = nu;
+        if (k == 1) u[c - sk] = 2.0 * bcu - nu;
+        if (k == p.nz) u[c + sk] = 2.0 * bcu - nu;
+    }
+    if (fy) {
+        const double nv = v[c] + scalar[4];
+        v[c] = nv;
+        if (k == 1) v[c - sk] = -nv;
+        if (k == p.nz) v[c + sk] = -nv;
+    }
+    if (fz) {
+        if (k != p.nz) w[c] = w[c] + scalar[5];
+    }
+}
+
+// ------------------------------------------------------------------------
+// diagnostics (checkNaN, calcMaxCFL, calcMaxDiv: mod_utils.f90:193-394)
+// ------------------------------------------------------------------------
+// lexicographic (value desc, linear index asc): the first strict maximum in
+// k, j, i order, as the sequential loops of the reference find it
+__device__ __forceinline__ void better(double &v, long long &ix, double ov, long long oix)
+{
+    if (ov > v || (ov == v && oix < ix)) {
+        v = ov;
+        ix = oix;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_diag(const double *__restrict__ u, const double *__restrict__ v,
+                                              const double *__restrict__ w, StepParams p, MeshDev m,
+                                              double *part, long long *ipart)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z + 1;
+    double dv = -1.0, cv = -1.0, nan = 0.0;
+    long long di = 0x7fffffffffffffffLL, ci = 0x7fffffffffffffffLL;
+    if (i < p.nx && j < p.ny) {
+        const Nb n = neighbours(i, j, k, p.nx, p.ny);
+        const double dzfi = __ldg(m.dzf_inv + k);
+        const double uc = __ldg(u + n.c), vc = __ldg(v + n.c), wc = __ldg(w + n.c);
+        const double um = __ldg(u + n.xm), vm = __ldg(v + n.ym), wm = __ldg(w + n.zm);
+        dv = fabs((uc - um) * p.dx_inv + (vc - vm) * p.dy_inv + (wc - wm) * dzfi);
+        cv = fabs((uc + um) * 0.5) * p.dx_inv + fabs((vc + vm) * 0.5) * p.dy_inv + fabs((wc + wm) * 0.5) * dzfi;
+        const long long lin = (long long)i + (long long)p.nx * (j + (long long)p.ny * (k - 1));
+        di = ci = lin;
+        nan = (uc != uc) + (vc != vc) + (wc != wc);
+        if (k == 1) nan += (__ldg(u + n.zm) != __ldg(u + n.zm)) + (vm != vm) + (wm != wm);
+        if (k == p.nz)
+            nan += (__ldg(u + n.zp) != __ldg(u + n.zp)) + (__ldg(v + n.zp) != __ldg(v + n.zp)) +
+                   (__ldg(w + n.zp) != __ldg(w + n.zp));
+        // NaN compares false: map a NaN residual to +inf so it is reported
+        if (dv != dv) dv = __longlong_as_double(0x7ff0000000000000LL);
+        if (cv != cv) cv = __longlong_as_double(0x7ff0000000000000LL);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        double odv = __shfl_down_sync(0xffffffffu, dv, o), ocv = __shfl_down_sync(0xffffffffu, cv, o);
+        long long odi = __shfl_down_sync(0xffffffffu, di, o), oci = __shfl_down_sync(0xffffffffu, ci, o);
+        nan += __shfl_down_sync(0xffffffffu, nan, o);
+        better(dv, di, odv, odi);
+        better(cv, ci, ocv, oci);
+    }
+    __shared__ double sd[32], sc[32], sn[32];
+    __shared__ long long sdi[32], sci[32];
+    const int t = threadIdx.x + threadIdx.y * blockDim.x, lane = t & 31, wid = t >> 5;
+    const int nw = (blockDim.x * blockDim.y + 31) >> 5;
+    if (lane == 0) {
+        sd[wid] = dv;
+        sc[wid] = cv;
+        sn[wid] = nan;
+        sdi[wid] = di;
+        sci[wid] = ci;
+    }
+    __syncthreads();
+    if (t == 0) {
+        for (int q = 1; q < nw; q++) {
+            better(dv, di, sd[q], sdi[q]);
+            better(cv, ci, sc[q], sci[q]);
+            nan += sn[q];
+        }
+        const size_t b = blockIdx.x + (size_t)gridDim.x * (blockIdx.y + (size_t)gridDim.y * blockIdx.z);
+        const size_t nb = (size_t)gridDim.x * gridDim.y * gridDim.z;
+        part[b] = dv;
+        part[nb + b] = cv;
+        part[2 * nb + b] = nan;
+        ipart[b] = di;
+        ipart[nb + b] = ci;
+    }
+}
+
+__global__ void k_diag_finish(const double *part, const long long *ipart, int nb, StepParams p, double *out,
+                              int *loc)
+{
+    if (threadIdx.x != 0) return;
+    double dv = -1.0, cv = -1.0, nan = 0.0;
+    long long di = 0x7fffffffffffffffLL, ci = 0x7fffffffffffffffLL;
+    for (int b = 0; b < nb; b++) {
+        better(dv, di, part[b], ipart[b]);
+        better(cv, ci, part[nb + b], ipart[nb + b]);
+        nan += part[2 * nb + b];
+    }
+    out[0] = dv;
+    out[1] = cv * p.dt;
+    out[2] = nan;
+    const long long nxy = (long long)p.nx * p.ny;
+    loc[0] = (int)(di % p.nx) + 1;
+    loc[1] = (int)((di / p.nx) % p.ny) + 1;
+    loc[2] = (int)(di / nxy) + 1;
+    loc[3] = (int)(ci % p.nx) + 1;
+    loc[4] = (int)((ci / p.nx) % p.ny) + 1;
+    loc[5] = (int)(ci / nxy) + 1;
+}
+
+// ------------------------------------------------------------------------
+// initial field (mod_initFlow.f90:28-78 with the repository PRNG)
+// ------------------------------------------------------------------------
+__device__ __forceinline__ double splitmix_uniform(uint64_t seed, uint64_t n)
+{
+    uint64_t z = seed + (n + 1) * 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    z = z ^ (z >> 31);
+    return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+__global__ void __launch_bounds__(256) k_init_fill(double *u, double *v, double *w, const double *prof,
+                                                   uint64_t seed, double noise, StepParams p)
+{
+    PL_POINT_INDEX();
+    const size_t c = (size_t)i + (size_t)p.nx * j + sk * k;
+    const uint64_t nint = (uint64_t)p.nx * p.ny * p.nz;
+    const uint64_t lin = (uint64_t)i + (uint64_t)p.nx * ((uint64_t)j + (uint64_t)p.ny * (uint64_t)(k - 1));
+    // var + 2*(rn - 0.5)*norm (mod_initFlow.f90:372), rounded op by op like the
+    // reference (no fused multiply-add)
+    u[c] = __dadd_rn(__ldg(prof + k), __dmul_rn(__dmul_rn(2.0, splitmix_uniform(seed, lin) - 0.5), noise));
+    v[c] = __dadd_rn(0.0, __dmul_rn(__dmul_rn(2.0, splitmix_uniform(seed, nint + lin) - 0.5), noise));
+    w[c] = __dadd_rn(0.0, __dmul_rn(__dmul_rn(2.0, splitmix_uniform(seed, 2 * nint + lin) - 0.5), noise));
+}
+
+__global__ void __launch_bounds__(256) k_sum_comp(const double *__restrict__ var, StepParams p, MeshDev m,
+                                                  double *partial, int comp)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z + 1;
+    double s = 0.0, z0 = 0.0, z1 = 0.0;
+    if (i < p.nx && j < p.ny) {
+        const size_t c = (size_t)i + (size_t)p.nx * j + (size_t)p.nx * p.ny * k;
+        s = __ldg(var + c) * __ldg(m.dzflzi + k);
+    }
+    block_sum3(s, z0, z1);
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        const size_t b = blockIdx.x + (size_t)gridDim.x * (blockIdx.y + (size_t)gridDim.y * blockIdx.z);
+        const size_t nb = (size_t)gridDim.x * gridDim.y * gridDim.z;
+        partial[(size_t)comp * nb + b] = s;
+    }
+}
+
+// u = u/meanold*u_ref (if meanold != 0), transform2CRF u -= u_crf, wall fills
+__global__ void __launch_bounds__(256) k_init_finish(double *u, double *v, double *w, StepParams p, double u_ref,
+                                                     const double *scalar)
+{
+    PL_POINT_INDEX();
+    const size_t c = (size_t)i + (size_t)p.nx * j + sk * k;
+    const double meanold = scalar[0];
+    double nu = u[c];
+    if (meanold != 0.0) nu = nu / meanold * u_ref;
+    nu = nu - p.u_crf;
+    u[c] = nu;
+    wall_fill<double>(u, v, w, c, k, sk, p.nz, 0.0 - p.u_crf, nu, v[c]);
+}
+
+__global__ void __launch_bounds__(256) k_fill_bc(double *u, double *v, double *w, StepParams p)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= p.nx || j >= p.ny) return;
+    const size_t sk = (size_t)p.nx * p.ny;
+    const double bcu = 0.0 - p.u_crf;
+    const size_t c1 = (size_t)i + (size_t)p.nx * j + sk, cn = c1 + sk * (p.nz - 1);
+    u[c1 - sk] = 2.0 * bcu - u[c1];
+    v[c1 - sk] = -v[c1];
+    w[c1 - sk] = 0.0;
+    u[cn + sk] = 2.0 * bcu - u[cn];
+    v[cn + sk] = -v[cn];
+    w[cn] = 0.0;
+    w[cn + sk] = 0.0;
+}
+
+// ------------------------------------------------------------------------
+// launchers
+// ------------------------------------------------------------------------
+static inline dim3 point_block() { return dim3(64, 4, 1); }
+static inline dim3 point_grid(const StepParams &p)
+{
+    return dim3((p.nx + 63) / 64, (p.ny + 3) / 4, p.nz);
+}
+
+int launch_rk1_fp64(const double *u, const double *v, const double *w, double *u1, double *v1, double *w1,
+                    const StepParams &p, const MeshDev &m, cudaStream_t st)
+{
+    k_rk1_fp64<<<point_grid(p), point_block(), 0, st>>>(u, v, w, u1, v1, w1, p, m);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
+int launch_rk2_fp64(double *u, double *v, double *w, const double *u1, const double *v1, const double *w1,
+                    const StepParams &p, const MeshDev &m, cudaStream_t st)
+{
+    k_rk2_fp64<<<point_grid(p), point_block(), 0, st>>>(u, v, w, u1, v1, w1, p, m);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
+int launch_calc_rhs_fp64(const double *u, const double *v, const double *w, double *rhs, const StepParams &p,
+                         const MeshDev &m, cudaStream_t st)
+{
+    k_calc_rhs_fp64<<<point_grid(p), point_block(), 0, st>>>(u, v, w, rhs, p, m);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
+static int nblocks(const StepParams &p)
+{
+    dim3 g = point_grid(p);
+    return (int)(g.x * g.y * g.z);
+}
+
+int launch_correct_fp64(const double *p_, double *u, double *v, double *w, const StepParams &p, const MeshDev &m,
+                        const int forced[3], ReduceBuf &rb, cudaStream_t st)
+{
+    (void)forced;
+    if (nblocks(p) > rb.max_blocks) {
+        set_error("reduction buffer too small");
+        return -1;
+    }
+    k_correct<double><<<point_grid(p), point_block(), 0, st>>>(p_, u, v, w, p, m, rb.partial);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
+int launch_force_fp64(double *u, double *v, double *w, const StepParams &p, const int forced[3],
+                      const double vel_force[3], ReduceBuf &rb, cudaStream_t st)
+{
+    if (!(forced[0] || forced[1] || forced[2])) return 0;
+    k_finish_means<<<3, 1024, 0, st>>>(rb.partial, nblocks(p), (double)p.nx, (double)p.ny, vel_force[0], vel_force[1],
+                                       vel_force[2], rb.scalar);
+    PL_CHECK_LAUNCH();
+    k_force<<<point_grid(p), point_block(), 0, st>>>(u, v, w, p, forced[0], forced[1], forced[2], rb.scalar);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
+int launch_diagnostics_fp64(const double *u, const double *v, const double *w, const StepParams &p,
+                            const MeshDev &m, double *d_out, int *d_loc, double *d_part, long long *d_ipart,
+                            int max_blocks, cudaStream_t st)
+{
+    if (nblocks(p) > max_blocks) {
+        set_error("diagnostics buffer too small");
+        return -1;
+    }
+    k_diag<<<point_grid(p), point_block(), 0, st>>>(u, v, w, p, m, d_part, d_ipart);
+    PL_CHECK_LAUNCH();
+    k_diag_finish<<<1, 32, 0, st>>>(d_part, d_ipart, nblocks(p), p, d_out, d_loc);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
+int launch_init_fill(double *u, double *v, double *w, const double *prof, uint64_t seed, double noise,
+                     const StepParams &p, cudaStream_t st)
+{
+    k_init_fill<<<point_grid(p), point_block(), 0, st>>>(u, v, w, prof, seed, noise, p);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
+int launch_mean_sum(const double *var, const StepParams &p, const MeshDev &m, ReduceBuf &rb, int comp,
+                    cudaStream_t st)
+{
+    if (nblocks(p) > rb.max_blocks) {
+        set_error("reduction buffer too small");
+        return -1;
+    }
+    k_sum_comp<<<point_grid(p), point_block(), 0, st>>>(var, p, m, rb.partial, comp);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
+int launch_init_finish(double *u, double *v, double *w, const StepParams &p, double u_ref, ReduceBuf &rb,
+                       cudaStream_t st)
+{
+    k_finish_means<<<3, 1024, 0, st>>>(rb.partial, nblocks(p), (double)p.nx, (double)p.ny, 0.0, 0.0, 0.0, rb.scalar);
+    PL_CHECK_LAUNCH();
+    k_init_finish<<<point_grid(p), point_block(), 0, st>>>(u, v, w, p, u_ref, rb.scalar);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
+int launch_fill_bc_vel(double *u, double *v, double *w, const StepParams &p, cudaStream_t st)
+{
+    dim3 g((p.nx + 63) / 64, (p.ny + 3) / 4, 1);
+    k_fill_bc<<<g, point_block(), 0, st>>>(u, v, w, p);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
+} // namespace pl

@@ -1,0 +1,67 @@
+// stencil.cuh -- momentum, divergence, projection and boundary kernels of the
+// RK2 projection step (Fortran reference: src/mod_calcVel.f90,
+// src/mod_calcRHS.f90, src/mod_updateBound.f90, src/mod_utils.f90).
+#pragma once
+
+#include "common.cuh"
+
+namespace pl {
+
+struct MeshDev {
+    const double *dzf, *dzf_inv, *dzc_inv, *dzflzi; // index 0 .. nz+1 as in mod_mesh.f90:36-38
+};
+
+struct StepParams {
+    int nx, ny, nz;
+    double dx_inv, dy_inv, re_inv, dt, u_crf;
+};
+
+// Reduction scratch: per-block partial results and the final scalars.
+struct ReduceBuf {
+    double *partial = nullptr; // >= max blocks * 3
+    double *scalar = nullptr;  // [0..2] component means, [3..5] forcing shift
+    int max_blocks = 0;
+};
+
+// FP64 step kernels (one launch each)
+int launch_rk1_fp64(const double *u, const double *v, const double *w, double *u1, double *v1, double *w1,
+                    const StepParams &p, const MeshDev &m, cudaStream_t st);
+int launch_rk2_fp64(double *u, double *v, double *w, const double *u1, const double *v1, const double *w1,
+                    const StepParams &p, const MeshDev &m, cudaStream_t st);
+int launch_calc_rhs_fp64(const double *u, const double *v, const double *w, double *rhs, const StepParams &p,
+                         const MeshDev &m, cudaStream_t st);
+// correctVel + the dz-weighted sums of Mean_h for the forced components
+int launch_correct_fp64(const double *p_, double *u, double *v, double *w, const StepParams &p, const MeshDev &m,
+                        const int forced[3], ReduceBuf &rb, cudaStream_t st);
+// forceVel shift (from the sums) + wall fill of the forced components
+int launch_force_fp64(double *u, double *v, double *w, const StepParams &p, const int forced[3],
+                      const double vel_force[3], ReduceBuf &rb, cudaStream_t st);
+
+// mixed-precision step kernels: u,v,w FP64; RK increments and p FP32
+int launch_rk1_mixed(const double *u, const double *v, const double *w, float *d1u, float *d1v, float *d1w,
+                     const StepParams &p, const MeshDev &m, cudaStream_t st);
+int launch_rk2_mixed(const double *u, const double *v, const double *w, const float *d1u, const float *d1v,
+                     const float *d1w, double *uo, double *vo, double *wo, const StepParams &p, const MeshDev &m,
+                     cudaStream_t st);
+int launch_calc_rhs_mixed(const double *u, const double *v, const double *w, float *rhs, double *rhs_mode0,
+                          const StepParams &p, const MeshDev &m, cudaStream_t st);
+int launch_correct_mixed(const float *p_, double *u, double *v, double *w, const StepParams &p, const MeshDev &m,
+                         const int forced[3], ReduceBuf &rb, cudaStream_t st);
+
+// diagnostics: out[0] = max|div| , out[1] = max CFL (already * dt), out[2] =
+// NaN count over u,v,w (ghosts included); loc[0..2] ijk of the div max,
+// loc[3..5] of the CFL max (1-based interior indices, reference convention)
+int launch_diagnostics_fp64(const double *u, const double *v, const double *w, const StepParams &p,
+                            const MeshDev &m, double *d_out, int *d_loc, double *d_part, long long *d_ipart,
+                            int max_blocks, cudaStream_t st);
+
+// initial field: Poiseuille profile + counter-based SplitMix64 noise
+int launch_init_fill(double *u, double *v, double *w, const double *prof, uint64_t seed, double noise,
+                     const StepParams &p, cudaStream_t st);
+int launch_mean_sum(const double *var, const StepParams &p, const MeshDev &m, ReduceBuf &rb, int comp,
+                    cudaStream_t st);
+int launch_init_finish(double *u, double *v, double *w, const StepParams &p, double u_ref, ReduceBuf &rb,
+                       cudaStream_t st);
+int launch_fill_bc_vel(double *u, double *v, double *w, const StepParams &p, cudaStream_t st);
+
+} // namespace pl

