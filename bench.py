@@ -34,14 +34,18 @@ RE_TAU, STRETCH, SEED, NOISE, DT = 1000.0, 2.0, 11, 0.1, 1e-4
 METRIC = "RK2 steps/s @512x384x256: mixed vs FP64 on same GPU at rel err<=1e-5"
 WORKLOAD = "channel 512x384x256, Re_tau 1000, tanh stretch 2.0, Thomas, dt 1e-4, seed 11, noise 0.1"
 
-# algorithmic bytes per grid point per launch (FP64 path), by kernel; see
-# DESIGN.md "kernels and rooflines" (SURVEY's per-pass table with the Mean_h
-# read fused into correctVel)
-ALG_BYTES_FP64 = {
-    "rk1": 48, "rk2": 72, "calc_rhs": 32,
-    "ppe_xfft_fwd": 16, "ppe_yfft_fwd": 16, "ppe_thomas": 24, "ppe_pdd": 40,
-    "ppe_yfft_bwd": 16, "ppe_xfft_bwd": 16, "correct": 56, "force": 16,
+# algorithmic bytes per grid point per launch slot, by kernel and path: the
+# compulsory field passes (reads + writes of whole fields at their storage
+# width); Mean_h of forceVel is fused into RK2 and the shift into the
+# correction, so no separate force pass exists
+ALG_BYTES = {
+    "fp64": {"rk1": 48, "rk2": 72, "calc_rhs": 32, "ppe_xfft_fwd": 16, "ppe_yfft_fwd": 16, "ppe_thomas": 24,
+             "ppe_pdd": 40, "ppe_yfft_bwd": 16, "ppe_xfft_bwd": 16, "correct_force": 56},
+    "mixed": {"rk1": 36, "rk2": 60, "calc_rhs": 36, "ppe_xfft_fwd": 8, "ppe_yfft_fwd": 8, "ppe_thomas": 16,
+              "ppe_pdd": 24, "ppe_yfft_bwd": 8, "ppe_xfft_bwd": 8, "correct_force": 68},
 }
+# kernel launches per step (this library's kernels only)
+LAUNCHES = {"fp64": 9, "mixed": 11}
 
 
 def peaks():
@@ -171,7 +175,8 @@ def dist_setup(n_gpus):
 
 
 def run_reference(args):
-    world, rank, _ = dist_setup(args.gpus)
+    # the CPU arm needs no process group: rank 0 alone runs, the others exit
+    rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     sps, threads, sample = cpu_reference_steps(args.steps, args.warmup)
@@ -224,46 +229,75 @@ def run_b200(args):
         barrier()
         return max_over_ranks(e0.elapsed_time(e1))
 
-    cfg64 = plb.ChannelConfig(nx=NX, ny=NY, nz=NZ, stretch_ratio=STRETCH, re_tau=RE_TAU, dt=DT,
-                              precision=plb.PL_FP64)
-    ch = plb.Channel(cfg64)
-    ch.init_flow(SEED, NOISE)
-    clocks = ClockSampler(local)
-    clocks.start()
-    ms64 = timed(ch, args.steps, args.warmup, lambda: ch.step(1))
-    clk = clocks.stop()
-    sps64 = world * args.steps / (ms64 / 1000.0)
-
-    # per-kernel device times -> roofline of the dominant kernel
-    prof = ch.profile(3)
-    npts = NX * NY * NZ
     peak, peak_kind = peaks()
-    top = max(prof, key=lambda kv: kv[1])
-    alg = ALG_BYTES_FP64.get(top[0], 0) * npts
+    npts = NX * NY * NZ
+
+    def measure(prec_name, prec):
+        cfg = plb.ChannelConfig(nx=NX, ny=NY, nz=NZ, stretch_ratio=STRETCH, re_tau=RE_TAU, dt=DT, precision=prec)
+        ch = plb.Channel(cfg)
+        ch.init_flow(SEED, NOISE)
+        clocks = ClockSampler(local)
+        clocks.start()
+        ms = timed(ch, args.steps, args.warmup, lambda: ch.step(1))
+        clk = clocks.stop()
+        prof = ch.profile(3)
+        alg = ALG_BYTES[prec_name]
+        tot_ms = sum(t for _, t in prof)
+        kernels = {name: {"ms": round(t, 4), "share": round(t / tot_ms, 4),
+                          "alg_gbs": round(alg.get(name, 0) * npts / (t / 1000.0) / 1e9, 1)}
+                   for name, t in prof}
+        return ch, ms, clk, prof, kernels
+
+    ch64, ms64, clk64, prof64, kern64 = measure("fp64", plb.PL_FP64)
+    ch64.close()
+    chm, msm, clkm, profm, kernm = measure("mixed", plb.PL_MIXED)
+    sps64 = world * args.steps / (ms64 / 1000.0)
+    spsm = world * args.steps / (msm / 1000.0)
+
+    # dominant kernel of the headline (mixed) step -> roofline
+    top = max(profm, key=lambda kv: kv[1])
+    alg = ALG_BYTES["mixed"].get(top[0], 0) * npts
     achieved = alg / (top[1] / 1000.0) / 1e9
-    tot_ms = sum(ms for _, ms in prof)
-    kernels = {name: {"ms": round(ms, 4), "share": round(ms / tot_ms, 4),
-                      "gbs": round(ALG_BYTES_FP64.get(name, 0) * npts / (ms / 1000.0) / 1e9, 1)}
-               for name, ms in prof}
     traffic = traffic_from_profiles(top[0])
-    launches_per_step = 11
 
     # end to end through the C ABI with host (pinned) buffers: every step
     # uploads u,v,w, steps, downloads u,v,w
-    host = torch.empty(3 * ch.compact_elems, dtype=torch.float64).pin_memory()
-    ch.download_compact(host.data_ptr())
-    ch.synchronize()
-    nbytes = 3 * ch.compact_elems * 8
+    host = torch.empty(3 * chm.compact_elems, dtype=torch.float64).pin_memory()
+    chm.download_compact(host.data_ptr())
+    chm.synchronize()
+    nbytes = 3 * chm.compact_elems * 8
     ke = max(3, min(args.steps, 10))
 
     def e2e_body():
-        ch.upload_compact(host.data_ptr())
-        ch.step(1)
-        ch.download_compact(host.data_ptr())
+        chm.upload_compact(host.data_ptr())
+        chm.step(1)
+        chm.download_compact(host.data_ptr())
 
-    ms_e2e = timed(ch, ke, 1, e2e_body)
+    ms_e2e = timed(chm, ke, 1, e2e_body)
     e2e_sps = world * ke / (ms_e2e / 1000.0)
-    ch.close()
+    chm.close()
+    del host
+
+    # accuracy of the mixed path after 100 steps from the same initial field,
+    # against the FP64 path (parity-pinned to the oracle at small sizes)
+    acc = None
+    if not args.no_accuracy:
+        out = {}
+        for name, prec in (("fp64", plb.PL_FP64), ("mixed", plb.PL_MIXED)):
+            cfg = plb.ChannelConfig(nx=NX, ny=NY, nz=NZ, stretch_ratio=STRETCH, re_tau=RE_TAU, dt=DT, precision=prec)
+            ch = plb.Channel(cfg)
+            ch.init_flow(SEED, NOISE)
+            ch.step(100)
+            out[name] = [ch.get_field(q)[1:-1, 1:-1, 1:-1] for q in range(3)] + [ch.diagnostics()]
+            ch.close()
+        acc = {"steps": 100, "reference": "this library's FP64 path"}
+        for q, n in enumerate("uvw"):
+            a, b = out["mixed"][q], out["fp64"][q]
+            acc[f"{n}_rel_l2"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+            acc[f"{n}_rel_max"] = float(np.abs(a - b).max() / np.abs(b).max())
+        acc["div_max_mixed"] = out["mixed"][3]["div_max"]
+        acc["div_max_fp64"] = out["fp64"][3]["div_max"]
+        del out
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -276,20 +310,23 @@ def run_b200(args):
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": sps64, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms64 / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "precision": "fp64", "grid": [NX, NY, NZ],
+            "metric": METRIC, "value": spsm, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": msm / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "mixed: f32 stencils/FFT, f64 u,v,w,p and tridiagonal",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "precision": "mixed", "grid": [NX, NY, NZ],
                        "l2": "inputs larger than L2 (403 MB per FP64 field), no flush",
                        "parallelism": "1 GPU" if world == 1 else f"{world} independent replicas"},
-            "fp64_steps_per_s": sps64,
-            "clocks": clk,
+            "fp64_steps_per_s": sps64, "fp64_ms_per_step": ms64 / args.steps,
+            "mixed_over_fp64": spsm / sps64,
+            "accuracy_after_100_steps": acc,
+            "clocks": clkm, "clocks_fp64": clk64,
             "e2e": {"value": e2e_sps, "unit": "steps/s", "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
-            "gpu_launches": launches_per_step * args.steps,
+            "gpu_launches": LAUNCHES["mixed"] * args.steps,
             "roofline": {"bound": "hbm", "kernel": top[0], "achieved": round(achieved, 1), "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                          "traffic": traffic, "alg_bytes": alg},
-            "kernels": kernels,
+            "kernels_mixed": kernm, "kernels_fp64": kern64,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
@@ -305,9 +342,17 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the 100-step accuracy comparison")
+    ap.add_argument("--grid", type=int, nargs=3, default=None,
+                    help="override the grid (profiling captures on a smaller case); the bench line is only "
+                         "valid at the default 512 384 256")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.grid:
+        global NX, NY, NZ, WORKLOAD
+        NX, NY, NZ = args.grid
+        WORKLOAD = WORKLOAD.replace("512x384x256", f"{NX}x{NY}x{NZ}")
     if args.impl == "reference":
         run_reference(args)
     else:

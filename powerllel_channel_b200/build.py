@@ -13,7 +13,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libpowerllel_b200.so")
 SOURCES = ["ppe.cu", "stencil.cu", "channel.cu"]
-HEADERS = ["common.cuh", "fft.cuh", "ppe.cuh", "stencil.cuh"]
+HEADERS = ["common.cuh", "fft.cuh", "ppe.cuh", "stencil.cuh", "trid_tables.h"]
 
 NVCC_FLAGS = [
     "-std=c++17", "-O3", "-lineinfo",

@@ -8,6 +8,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <utility>
 #include <string>
 #include <vector>
 
@@ -160,7 +161,7 @@ extern "C" int pl_ppe_solve(pl_ppe *p, void *d_var, void *stream)
     }
     cudaStream_t st = (cudaStream_t)stream;
     if (p->s.prec == PREC_FP64) return ppe_solve_fp64(&p->s, (double *)d_var, st);
-    return ppe_solve_fp32(&p->s, (float *)d_var, st);
+    return ppe_solve_fp32(&p->s, (float *)d_var, nullptr, st);
 }
 
 extern "C" int pl_ppe_destroy(pl_ppe *p)
@@ -183,11 +184,20 @@ struct pl_channel {
     std::vector<double> dzf_global, zc_global, dzf, dzf_inv, dzc, dzc_inv, dzflzi, prof;
     double *d_mesh = nullptr;
     MeshDev m{};
+    // FP64 path: u,v,w = ua,va,wa; stage-1 fields u1,v1,w1; p
+    // mixed path: u,v,w ping-pong between (ua,va,wa) and (ub,vb,wb); stage-1
+    // increments d1u,d1v,d1w (FP32); p ping-pong between p and pb (FP64); the
+    // PPE works in place on r32 (FP32)
     double *u = nullptr, *v = nullptr, *w = nullptr;
     double *u1 = nullptr, *v1 = nullptr, *w1 = nullptr;
     double *p = nullptr;
+    double *ub = nullptr, *vb = nullptr, *wb = nullptr, *pb = nullptr;
+    float *d1u = nullptr, *d1v = nullptr, *d1w = nullptr, *r32 = nullptr;
+    double *plane_part = nullptr, *mode0 = nullptr;
+    int incremental = 1;
     Ppe ppe;
     ReduceBuf rb;
+    MeanState ms;
     double *d_diag = nullptr;
     int *d_loc = nullptr;
     double *d_dpart = nullptr;
@@ -267,6 +277,18 @@ static void channel_free(pl_channel *c)
     cudaFree(c->v1);
     cudaFree(c->w1);
     cudaFree(c->p);
+    cudaFree(c->ub);
+    cudaFree(c->vb);
+    cudaFree(c->wb);
+    cudaFree(c->pb);
+    cudaFree(c->d1u);
+    cudaFree(c->d1v);
+    cudaFree(c->d1w);
+    cudaFree(c->r32);
+    cudaFree(c->plane_part);
+    cudaFree(c->mode0);
+    cudaFree(c->ms.partial);
+    cudaFree(c->ms.counter);
     cudaFree(c->rb.partial);
     cudaFree(c->rb.scalar);
     cudaFree(c->d_diag);
@@ -280,8 +302,8 @@ static void channel_free(pl_channel *c)
 extern "C" int pl_channel_create(pl_channel **out, const pl_channel_config *cfg)
 {
     *out = nullptr;
-    if (cfg->precision != PL_FP64) {
-        set_error("pl_channel_create: only PL_FP64 is available in this build");
+    if (cfg->precision != PL_FP64 && cfg->precision != PL_MIXED) {
+        set_error("pl_channel_create: precision must be PL_FP64 or PL_MIXED");
         return -1;
     }
     if (cfg->nx < 2 || cfg->ny < 2 || cfg->nz < 2 || (cfg->nx & 1) || (cfg->ny & 1) || (cfg->nz & 1)) {
@@ -324,20 +346,34 @@ extern "C" int pl_channel_create(pl_channel **out, const pl_channel_config *cfg)
     c->m.dzf_inv = c->d_mesh + n1;
     c->m.dzc_inv = c->d_mesh + 2 * n1;
     c->m.dzflzi = c->d_mesh + 3 * n1;
-    double **fields[6] = {&c->u, &c->v, &c->w, &c->u1, &c->v1, &c->w1};
-    for (auto f : fields) {
-        if (cudaMalloc(f, sizeof(double) * c->nf) != cudaSuccess) {
-            set_error("pl_channel_create: out of device memory for the fields");
-            return fail();
-        }
-        cudaMemset(*f, 0, sizeof(double) * c->nf);
-    }
-    if (cudaMalloc(&c->p, sizeof(double) * c->np) != cudaSuccess) {
-        set_error("pl_channel_create: out of device memory for p");
+    const bool mixed = cfg->precision == PL_MIXED;
+    auto dalloc = [&](double **f, size_t n) {
+        if (cudaMalloc(f, sizeof(double) * n) != cudaSuccess) return false;
+        cudaMemset(*f, 0, sizeof(double) * n);
+        return true;
+    };
+    auto falloc = [&](float **f, size_t n) {
+        if (cudaMalloc(f, sizeof(float) * n) != cudaSuccess) return false;
+        cudaMemset(*f, 0, sizeof(float) * n);
+        return true;
+    };
+    bool ok = dalloc(&c->u, c->nf) && dalloc(&c->v, c->nf) && dalloc(&c->w, c->nf) && dalloc(&c->p, c->np);
+    if (ok && !mixed) ok = dalloc(&c->u1, c->nf) && dalloc(&c->v1, c->nf) && dalloc(&c->w1, c->nf);
+    if (ok && mixed)
+        ok = dalloc(&c->ub, c->nf) && dalloc(&c->vb, c->nf) && dalloc(&c->wb, c->nf) && dalloc(&c->pb, c->np) &&
+             falloc(&c->d1u, c->nf) && falloc(&c->d1v, c->nf) && falloc(&c->d1w, c->nf) && falloc(&c->r32, c->np) &&
+             dalloc(&c->mode0, c->nz) &&
+             dalloc(&c->plane_part, (size_t)((c->nx + 63) / 64) * ((c->ny + 3) / 4) * c->nz);
+    if (!ok) {
+        set_error("pl_channel_create: out of device memory for the fields");
         return fail();
     }
-    cudaMemset(c->p, 0, sizeof(double) * c->np);
-    if (ppe_create(&c->ppe, c->nx, c->ny, c->nz, dx, dy, c->dzf_global.data(), cfg->trid_parts, PREC_FP64))
+    // the mixed path solves for the pressure increment (Thomas); with PDD the
+    // reference's truncated solve is not an exact inverse, so the full
+    // pressure is solved each step as in the reference
+    c->incremental = (cfg->trid_parts == 0) ? 1 : 0;
+    if (ppe_create(&c->ppe, c->nx, c->ny, c->nz, dx, dy, c->dzf_global.data(), cfg->trid_parts,
+                   mixed ? PREC_MIXED : PREC_FP64))
         return fail();
     c->max_blocks = ((c->nx + 63) / 64) * ((c->ny + 3) / 4) * c->nz;
     c->rb.max_blocks = c->max_blocks;
@@ -346,8 +382,19 @@ extern "C" int pl_channel_create(pl_channel **out, const pl_channel_config *cfg)
         cudaMalloc(&c->d_diag, sizeof(double) * 4) != cudaSuccess ||
         cudaMalloc(&c->d_loc, sizeof(int) * 8) != cudaSuccess ||
         cudaMalloc(&c->d_dpart, sizeof(double) * 3 * c->max_blocks) != cudaSuccess ||
-        cudaMalloc(&c->d_dipart, sizeof(long long) * 2 * c->max_blocks) != cudaSuccess) {
+        cudaMalloc(&c->d_dipart, sizeof(long long) * 2 * c->max_blocks) != cudaSuccess ||
+        cudaMalloc(&c->ms.partial, sizeof(double) * c->max_blocks) != cudaSuccess ||
+        cudaMalloc(&c->ms.counter, sizeof(unsigned int)) != cudaSuccess) {
         set_error("pl_channel_create: out of device memory for reductions");
+        return fail();
+    }
+    cudaMemset(c->ms.counter, 0, sizeof(unsigned int));
+    cudaMemset(c->rb.scalar, 0, sizeof(double) * 8);
+    c->ms.scalar = c->rb.scalar;
+    c->ms.max_blocks = c->max_blocks;
+    c->ms.vel_force = cfg->vel_force[0];
+    if (cfg->is_forced[1] || cfg->is_forced[2]) {
+        set_error("pl_channel_create: forcing is implemented for x only (is_forced = T,F,F, the channel)");
         return fail();
     }
     if (cudaDeviceSynchronize() != cudaSuccess) {
@@ -376,6 +423,7 @@ extern "C" int pl_channel_init_flow(pl_channel *c, uint64_t seed, double noise)
     PL_CUDA_TRY(cudaMemsetAsync(c->v, 0, sizeof(double) * c->nf, c->stream));
     PL_CUDA_TRY(cudaMemsetAsync(c->w, 0, sizeof(double) * c->nf, c->stream));
     PL_CUDA_TRY(cudaMemsetAsync(c->p, 0, sizeof(double) * c->np, c->stream));
+    if (c->pb) PL_CUDA_TRY(cudaMemsetAsync(c->pb, 0, sizeof(double) * c->np, c->stream));
     int rc = launch_init_fill(c->u, c->v, c->w, dprof, seed, noise, c->sp, c->stream);
     if (!rc) rc = launch_mean_sum(c->u, c->sp, c->m, c->rb, 0, c->stream);
     if (!rc) rc = launch_init_finish(c->u, c->v, c->w, c->sp, c->cfg.u_ref, c->rb, c->stream);
@@ -384,35 +432,64 @@ extern "C" int pl_channel_init_flow(pl_channel *c, uint64_t seed, double noise)
     return rc;
 }
 
+static inline bool is_mixed(const pl_channel *c) { return c->cfg.precision == PL_MIXED; }
+
 extern "C" int pl_phase_rk1(pl_channel *c)
 {
-    int rc = launch_rk1_fp64(c->u, c->v, c->w, c->u1, c->v1, c->w1, c->sp, c->m, c->stream);
+    int rc = is_mixed(c) ? launch_rk1_mixed(c->u, c->v, c->w, c->d1u, c->d1v, c->d1w, c->sp, c->m, c->stream)
+                         : launch_rk1_fp64(c->u, c->v, c->w, c->u1, c->v1, c->w1, c->sp, c->m, c->stream);
     channel_mark(c, "rk1");
     return rc;
 }
 
 extern "C" int pl_phase_rk2(pl_channel *c)
 {
-    int rc = launch_rk2_fp64(c->u, c->v, c->w, c->u1, c->v1, c->w1, c->sp, c->m, c->stream);
+    int rc;
+    if (is_mixed(c)) {
+        rc = launch_rk2_mixed(c->u, c->v, c->w, c->d1u, c->d1v, c->d1w, c->ub, c->vb, c->wb, c->sp, c->m, c->ms,
+                              c->stream);
+        std::swap(c->u, c->ub);
+        std::swap(c->v, c->vb);
+        std::swap(c->w, c->wb);
+    } else {
+        rc = launch_rk2m_fp64(c->u, c->v, c->w, c->u1, c->v1, c->w1, c->sp, c->m, c->ms, c->stream);
+    }
     channel_mark(c, "rk2");
     return rc;
 }
 
 extern "C" int pl_phase_calc_rhs(pl_channel *c)
 {
-    int rc = launch_calc_rhs_fp64(c->u, c->v, c->w, c->p, c->sp, c->m, c->stream);
+    int rc;
+    if (is_mixed(c)) {
+        const double dx = c->cfg.lx / c->nx, dy = c->cfg.ly / c->ny;
+        rc = launch_rhs_mixed(c->u, c->v, c->w, c->p, c->r32, c->plane_part, c->mode0, c->sp, c->m, c->ppe.d_a,
+                              c->ppe.d_bt, c->ppe.d_c, 1.0 / (dx * dx), 1.0 / (dy * dy), c->incremental, c->stream);
+    } else {
+        rc = launch_calc_rhs_fp64(c->u, c->v, c->w, c->p, c->sp, c->m, c->stream);
+    }
     channel_mark(c, "calc_rhs");
     return rc;
 }
 
-extern "C" int pl_phase_poisson(pl_channel *c) { return ppe_solve_fp64(&c->ppe, c->p, c->stream); }
+extern "C" int pl_phase_poisson(pl_channel *c)
+{
+    if (is_mixed(c)) return ppe_solve_fp32(&c->ppe, c->r32, c->incremental ? c->mode0 : nullptr, c->stream);
+    return ppe_solve_fp64(&c->ppe, c->p, c->stream);
+}
 
 extern "C" int pl_phase_correct_force(pl_channel *c)
 {
-    if (launch_correct_fp64(c->p, c->u, c->v, c->w, c->sp, c->m, c->cfg.is_forced, c->rb, c->stream)) return -1;
-    channel_mark(c, "correct");
-    int rc = launch_force_fp64(c->u, c->v, c->w, c->sp, c->cfg.is_forced, c->cfg.vel_force, c->rb, c->stream);
-    channel_mark(c, "force");
+    int rc;
+    if (is_mixed(c)) {
+        rc = launch_correct_mixed(c->p, c->r32, c->pb, c->u, c->v, c->w, c->sp, c->m, c->cfg.is_forced[0],
+                                  c->ms.scalar, c->incremental, c->stream);
+        std::swap(c->p, c->pb);
+    } else {
+        rc = launch_correct_force_fp64(c->p, c->u, c->v, c->w, c->sp, c->m, c->cfg.is_forced[0], c->ms.scalar,
+                                       c->stream);
+    }
+    channel_mark(c, "correct_force");
     return rc;
 }
 
@@ -548,6 +625,17 @@ extern "C" int pl_channel_get_field(pl_channel *c, int which, double *host)
         expand_ghosted(c, tmp.data(), host, c->nz, -1);
         return 0;
     }
+    if (which >= 4 && is_mixed(c)) {
+        // u1 = u + d1 (the stage-1 field the mixed path keeps as an increment)
+        std::vector<float> inc(c->nf);
+        const double *base = which == 4 ? c->u : (which == 5 ? c->v : c->w);
+        const float *d = which == 4 ? c->d1u : (which == 5 ? c->d1v : c->d1w);
+        PL_CUDA_TRY(cudaMemcpy(tmp.data(), base, sizeof(double) * c->nf, cudaMemcpyDeviceToHost));
+        PL_CUDA_TRY(cudaMemcpy(inc.data(), d, sizeof(float) * c->nf, cudaMemcpyDeviceToHost));
+        for (size_t q = 0; q < c->nf; q++) tmp[q] += (double)inc[q];
+        expand_ghosted(c, tmp.data(), host, c->nz + 2, 0);
+        return 0;
+    }
     const double *src = (const double *)pl_channel_field(c, which);
     PL_CUDA_TRY(cudaMemcpy(tmp.data(), src, sizeof(double) * c->nf, cudaMemcpyDeviceToHost));
     expand_ghosted(c, tmp.data(), host, c->nz + 2, 0);
@@ -598,9 +686,9 @@ extern "C" void *pl_channel_field(pl_channel *c, int which)
     case 1: return c->v;
     case 2: return c->w;
     case 3: return c->p;
-    case 4: return c->u1;
-    case 5: return c->v1;
-    case 6: return c->w1;
+    case 4: return is_mixed(c) ? (void *)c->d1u : (void *)c->u1;
+    case 5: return is_mixed(c) ? (void *)c->d1v : (void *)c->v1;
+    case 6: return is_mixed(c) ? (void *)c->d1w : (void *)c->w1;
     default: return nullptr;
     }
 }

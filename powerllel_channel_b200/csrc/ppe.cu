@@ -16,6 +16,7 @@
 #include <cstring>
 
 #include "ppe.cuh"
+#include "trid_tables.h"
 
 namespace pl {
 
@@ -249,6 +250,30 @@ __global__ void __launch_bounds__(128) k_pdd(double *xs, T *xout, TridDev t, Pdd
     }
 }
 
+// Mixed path, (kx,ky) = (0,0): the Neumann system is singular (its last pivot
+// is round-off), so its FP32-transformed right-hand side cannot be trusted to
+// the consistency the division needs.  Solve it in FP64 from the FP64 plane
+// sums with the gauge x[nz-1] = 0 (fixes the free constant) and store the
+// result in the transformed array.  One thread; nz sequential rows.
+__global__ void k_mode0(float *x, double *xs, const double *__restrict__ mode0, TridDev t)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    // class 0 and column 0 are the (0,0) slot; xs is the FP64 sweep buffer
+    const size_t stride = (size_t)t.nx * t.ny, cstride = (size_t)t.ncx * t.ncy;
+    double xp = mode0[0];
+    xs[0] = xp;
+    for (int k = 1; k < t.nz; k++) {
+        xp = mode0[k] - __ldg(t.mult + (size_t)k * cstride) * xp;
+        xs[(size_t)k * stride] = xp;
+    }
+    double xn = 0.0; // gauge: x[nz-1] = 0 instead of dividing by the round-off pivot
+    x[(size_t)(t.nz - 1) * stride] = 0.0f;
+    for (int k = t.nz - 2; k >= 0; k--) {
+        xn = (xs[(size_t)k * stride] - __ldg(t.c + k) * xn) * __ldg(t.rb + (size_t)k * cstride);
+        x[(size_t)k * stride] = (float)xn;
+    }
+}
+
 // mixed path: widen the FP32 right-hand side into the FP64 sweep buffer
 __global__ void k_widen(const float *__restrict__ in, double *__restrict__ out, size_t n)
 {
@@ -294,34 +319,6 @@ template <typename V> static int upload_twiddles(int n, V **dptr)
     return 0;
 }
 
-// decomp_2d.c:261-283
-static void distribute(int num, int nprocs, std::vector<int> &st0, std::vector<int> &sz)
-{
-    std::vector<int> st(nprocs), en(nprocs);
-    sz.assign(nprocs, 0);
-    int size = num / nprocs;
-    int nu = num - size * nprocs;
-    int nl = nprocs - nu;
-    st[0] = 1;
-    sz[0] = size;
-    en[0] = size;
-    for (int i = 1; i < nl; i++) {
-        st[i] = st[i - 1] + size;
-        sz[i] = size;
-        en[i] = en[i - 1] + size;
-    }
-    size++;
-    for (int i = nl; i < nprocs; i++) {
-        st[i] = en[i - 1] + 1;
-        sz[i] = size;
-        en[i] = en[i - 1] + size;
-    }
-    en[nprocs - 1] = num;
-    sz[nprocs - 1] = num - st[nprocs - 1] + 1;
-    st0.resize(nprocs);
-    for (int i = 0; i < nprocs; i++) st0[i] = st[i] - 1;
-}
-
 template <typename V> static void set_plan(FftPlanDev<V> &p, int n, const int *radix, int ns, const V *tw)
 {
     p.n = n;
@@ -352,7 +349,6 @@ int ppe_create(Ppe *s, int nx, int ny, int nz, double dx, double dy, const doubl
     s->ncy = ny / 2 + 1;
     s->norm = 1.0 / (1.0 * nx * 1.0 * ny); // mod_fft_fftw.inc:154, PP/PP
     const int P = nparts >= 1 ? nparts : 1;
-    distribute(nz, P, s->kst, s->ksz);
 
     int rx[FFT_MAX_STAGES], ry[FFT_MAX_STAGES], nsx = 0, nsy = 0;
     if (factor_radices(nx, rx, &nsx) || factor_radices(ny, ry, &nsy)) {
@@ -367,89 +363,17 @@ int ppe_create(Ppe *s, int nx, int ny, int nz, double dx, double dy, const doubl
     set_plan(s->px32, nx, rx, nsx, s->d_twx32);
     set_plan(s->py32, ny, ry, nsy, s->d_twy32);
 
-    // eigenvalues, mod_poisson_solver.c:227-242 with mod_fft_fftw.inc:180-183
-    const double pi = acos(-1.0);
-    std::vector<double> lx(nx), ly(ny);
-    for (int i = 1; i <= nx; i++) lx[i - 1] = 2.0 * (cos(2.0 * pi * (i - 1.0) / nx) - 1.0);
-    for (int i = 0; i < nx; i++) lx[i] /= (dx * dx);
-    for (int i = 1; i <= ny; i++) ly[i - 1] = 2.0 * (cos(2.0 * pi * (i - 1.0) / ny) - 1.0);
-    for (int i = 0; i < ny; i++) ly[i] /= (dy * dy);
-
-    // coefficients per partition (set_trid_coeff :40-103, 'c', NN), pivots
-    // (:255-276) and PDD spikes (init_pdd_array :105-170), per class
+    // tridiagonal coefficients, pivots and PDD spikes per eigenvalue class
+    TridTables tt;
+    trid_build(tt, nx, ny, nz, dx, dy, dzf_global, nparts);
+    s->kst = tt.kst;
+    s->ksz = tt.ksz;
     const size_t ncls = (size_t)s->ncx * s->ncy;
-    std::vector<double> a(nz), c(nz), bt(nz);
-    std::vector<double> mult(ncls * nz), rb(ncls * nz), b(nz), v, w, tmpv;
-    if (nparts >= 1) {
-        v.assign(ncls * nz, 0.0);
-        w.assign(ncls * nz, 0.0);
-        tmpv.assign(ncls * P, 0.0);
-    }
-    for (int m = 0; m < P; m++) {
-        const int k0 = s->kst[m], ke = s->ksz[m];
-        const double *dzf = dzf_global + k0; // dzf_global[st-1+i], i = 0..ke+1
-        for (int k = 0; k < ke; k++) {
-            a[k0 + k] = 2.0 / (dzf[k + 1] * (dzf[k] + dzf[k + 1]));
-            c[k0 + k] = 2.0 / (dzf[k + 1] * (dzf[k + 2] + dzf[k + 1]));
-        }
-        for (int k = 0; k < ke; k++) bt[k0 + k] = -a[k0 + k] - c[k0 + k];
-        const double factor = 1.0; // 'N'
-        if (m == 0) {
-            bt[k0] += factor * a[k0];
-            a[k0] *= fabs(factor) - 1.0;
-        }
-        if (m == P - 1) {
-            bt[k0 + ke - 1] += factor * c[k0 + ke - 1];
-            c[k0 + ke - 1] *= fabs(factor) - 1.0;
-        }
-    }
-    std::vector<double> a_orig = a, c_orig = c;
-    for (int jy = 0; jy < s->ncy; jy++)
-        for (int ix = 0; ix < s->ncx; ix++) {
-            const size_t cl = (size_t)ix + (size_t)s->ncx * jy;
-            const double lam = lx[ix] + ly[jy];
-            for (int m = 0; m < P; m++) {
-                const int k0 = s->kst[m], ke = s->ksz[m];
-                for (int k = 0; k < ke; k++) b[k0 + k] = bt[k0 + k] + lam;
-                mult[cl + ncls * k0] = 0.0;
-                for (int k = 1; k < ke; k++) {
-                    double a_tmp = a[k0 + k] / b[k0 + k - 1];
-                    b[k0 + k] -= (a_tmp * c[k0 + k - 1]);
-                    mult[cl + ncls * (k0 + k)] = a_tmp;
-                }
-                for (int k = 0; k < ke; k++) rb[cl + ncls * (k0 + k)] = (b[k0 + k] != 0.0) ? 1.0 / b[k0 + k] : 0.0;
-                if (nparts >= 1) {
-                    // spikes with the partition's original a[0], c[ke-1]
-                    std::vector<double> vv(ke, 0.0), ww(ke, 0.0);
-                    vv[0] = a_orig[k0];
-                    ww[ke - 1] = c_orig[k0 + ke - 1];
-                    for (int k = 1; k < ke; k++) {
-                        double a_tmp = a[k0 + k] / b[k0 + k - 1];
-                        vv[k] -= a_tmp * vv[k - 1];
-                        ww[k] -= a_tmp * ww[k - 1];
-                    }
-                    if (b[k0 + ke - 1] != 0.0) {
-                        vv[ke - 1] /= b[k0 + ke - 1];
-                        ww[ke - 1] /= b[k0 + ke - 1];
-                    } else {
-                        vv[ke - 1] = 0.0;
-                        ww[ke - 1] = 0.0;
-                    }
-                    for (int k = ke - 2; k >= 0; k--) {
-                        vv[k] = (vv[k] - c[k0 + k] * vv[k + 1]) / b[k0 + k];
-                        ww[k] = (ww[k] - c[k0 + k] * ww[k + 1]) / b[k0 + k];
-                    }
-                    for (int k = 0; k < ke; k++) {
-                        v[cl + ncls * (k0 + k)] = vv[k];
-                        w[cl + ncls * (k0 + k)] = ww[k];
-                    }
-                }
-            }
-            if (nparts >= 1)
-                for (int m = 0; m + 1 < P; m++) tmpv[cl + ncls * m] = v[cl + ncls * s->kst[m + 1]];
-        }
-    // the PDD zeroing of a[0], c[ke-1] (:132-133) does not enter the local
-    // sweeps (they read a[k>=1] and c[k<=ke-2]); c is uploaded as set above
+    const std::vector<double> &mult = tt.mult, &rb = tt.rb, &c = tt.c, &v = tt.v, &w = tt.w, &tmpv = tt.tmpv;
+    PL_CUDA_TRY(cudaMalloc(&s->d_a, sizeof(double) * nz));
+    PL_CUDA_TRY(cudaMalloc(&s->d_bt, sizeof(double) * nz));
+    PL_CUDA_TRY(cudaMemcpy(s->d_a, tt.a.data(), sizeof(double) * nz, cudaMemcpyHostToDevice));
+    PL_CUDA_TRY(cudaMemcpy(s->d_bt, tt.bt.data(), sizeof(double) * nz, cudaMemcpyHostToDevice));
     PL_CUDA_TRY(cudaMalloc(&s->d_mult, sizeof(double) * ncls * nz));
     PL_CUDA_TRY(cudaMalloc(&s->d_rb, sizeof(double) * ncls * nz));
     PL_CUDA_TRY(cudaMalloc(&s->d_c, sizeof(double) * nz));
@@ -489,6 +413,8 @@ void ppe_destroy(Ppe *s)
     cudaFree(s->d_mult);
     cudaFree(s->d_rb);
     cudaFree(s->d_c);
+    cudaFree(s->d_a);
+    cudaFree(s->d_bt);
     cudaFree(s->d_v);
     cudaFree(s->d_w);
     cudaFree(s->d_tmpv);
@@ -608,7 +534,7 @@ int ppe_solve_fp64(Ppe *s, double *d_var, cudaStream_t st)
     return ppe_solve_fp64_strided(s, d_var, d_var, 0, nxl, nxy, d_var, st);
 }
 
-int ppe_solve_fp32(Ppe *s, float *d_var, cudaStream_t st)
+int ppe_solve_fp32(Ppe *s, float *d_var, const double *mode0, cudaStream_t st)
 {
     const size_t nxl = s->nx, nxy = (size_t)s->nx * s->ny;
     if (launch_x<float>(s, true, d_var, 0, nxl, nxy, d_var, 0, nxl, nxy, 1.0f, st)) return -1;
@@ -616,6 +542,11 @@ int ppe_solve_fp32(Ppe *s, float *d_var, cudaStream_t st)
     if (launch_y<float>(s, true, d_var, st)) return -1;
     mark(s, "ppe_yfft_fwd");
     if (launch_trid<float>(s, d_var, st)) return -1;
+    if (mode0 && s->nparts == 0) {
+        TridDev t{s->nx, s->ny, s->nz, s->ncx, s->ncy, s->d_mult, s->d_rb, s->d_c};
+        k_mode0<<<1, 32, 0, st>>>(d_var, s->d_scratch, mode0, t);
+        PL_CHECK_LAUNCH();
+    }
     mark(s, s->nparts ? "ppe_pdd" : "ppe_thomas");
     if (launch_y<float>(s, false, d_var, st)) return -1;
     mark(s, "ppe_yfft_bwd");

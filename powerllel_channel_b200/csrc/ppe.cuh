@@ -36,6 +36,7 @@ struct Ppe {
     // 0 at a partition's first row), rb[k] = 1/b[k] (0 where b == 0)
     double *d_mult = nullptr, *d_rb = nullptr;
     double *d_c = nullptr;   // c[k], nz (partition-local values)
+    double *d_a = nullptr, *d_bt = nullptr; // a[k], b_tmp[k]: the z rows of the operator
     double *d_v = nullptr, *d_w = nullptr; // PDD spikes, class tables
     double *d_tmpv = nullptr;              // PDD: v of partition m+1 at its k=0, [m][jy][ix]
     double *d_scratch = nullptr;           // mixed path: FP64 forward-sweep values
@@ -55,7 +56,10 @@ void ppe_destroy(Ppe *s);
 
 // In-place solve on the interior-only device array (layout [k][j][i]).
 int ppe_solve_fp64(Ppe *s, double *d_var, cudaStream_t st);
-int ppe_solve_fp32(Ppe *s, float *d_var, cudaStream_t st);
+// mode0 (optional, FP64 [nz]): the plane sums of the right-hand side; when
+// given, the (kx,ky) = (0,0) system is solved from them in FP64 with the
+// gauge x[nz-1] = 0 (Thomas only) instead of from the FP32 transform.
+int ppe_solve_fp32(Ppe *s, float *d_var, const double *mode0, cudaStream_t st);
 
 // Solve reading from / writing to a strided device array (the reference's
 // ghosted layout): element (i,j,k), 0-based interior, at base[off + i +

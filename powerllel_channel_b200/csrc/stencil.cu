@@ -521,6 +521,254 @@ __global__ void __launch_bounds__(256) k_fill_bc(double *u, double *v, double *w
 }
 
 // ------------------------------------------------------------------------
+// Mean_h of the new streamwise velocity, fused into the RK2 kernels.
+// forceVel (mod_calcVel.f90:463-476) shifts u by vel_force - Mean_h(u) after
+// correctVel.  correctVel changes sum_i u by -dt/dx * sum_i (p_{i+1} - p_i),
+// which telescopes to zero on the periodic x lines, so Mean_h of the
+// corrected u equals Mean_h of the RK2 output (up to round-off): the shift is
+// computed here and applied by the correction kernel, saving a pass.
+// Block partials are summed by the last block in a fixed order
+// (deterministic).
+// ------------------------------------------------------------------------
+struct MeanRed {
+    double *partial;        // one per block
+    unsigned int *counter;  // zero between launches
+    double *scalar;         // [0] = Mean_h, [3] = vel_force - Mean_h
+    double dnx, dny, vel_force;
+};
+
+__device__ __forceinline__ void mean_reduce(double su, const MeanRed &r)
+{
+    double z0 = 0.0, z1 = 0.0;
+    block_sum3(su, z0, z1);
+    __shared__ bool last;
+    const int t = threadIdx.x + threadIdx.y * blockDim.x;
+    const unsigned int nb = gridDim.x * gridDim.y * gridDim.z;
+    if (t == 0) {
+        const size_t b = blockIdx.x + (size_t)gridDim.x * (blockIdx.y + (size_t)gridDim.y * blockIdx.z);
+        r.partial[b] = su;
+        __threadfence();
+        last = (atomicAdd(r.counter, 1u) == nb - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    const int nthr = blockDim.x * blockDim.y;
+    double s = 0.0;
+    for (unsigned int q = t; q < nb; q += nthr) s += __ldcg(r.partial + q);
+    z0 = z1 = 0.0;
+    __syncthreads();
+    block_sum3(s, z0, z1);
+    if (t == 0) {
+        const double mean = s / r.dnx / r.dny;
+        r.scalar[0] = mean;
+        r.scalar[3] = r.vel_force - mean;
+        *r.counter = 0u;
+    }
+}
+
+// RK2 (FP64) with the fused Mean_h of the new u
+__global__ void __launch_bounds__(256) k_rk2m_fp64(double *u, double *v, double *w, const double *__restrict__ u1,
+                                                   const double *__restrict__ v1, const double *__restrict__ w1,
+                                                   StepParams p, MeshDev m, MeanRed red)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z + 1;
+    const size_t sk = (size_t)p.nx * p.ny;
+    double su = 0.0;
+    if (i < p.nx && j < p.ny) {
+        const Nb n = neighbours(i, j, k, p.nx, p.ny);
+        double ru, rv, rw;
+        momentum_rhs<double>(LoadF<double, double>{u1}, LoadF<double, double>{v1}, LoadF<double, double>{w1}, n, k,
+                             p, m, ru, rv, rw);
+        const double nu = (__ldg(u1 + n.c) + p.dt * ru + u[n.c]) * 0.5;
+        const double nv = (__ldg(v1 + n.c) + p.dt * rv + v[n.c]) * 0.5;
+        u[n.c] = nu;
+        v[n.c] = nv;
+        if (k != p.nz) w[n.c] = (__ldg(w1 + n.c) + p.dt * rw + w[n.c]) * 0.5;
+        wall_fill<double>(u, v, w, n.c, k, sk, p.nz, 0.0 - p.u_crf, nu, nv);
+        su = nu * __ldg(m.dzflzi + k);
+    }
+    mean_reduce(su, red);
+}
+
+// correctVel + forceVel (shift from the fused mean) + wall fill
+template <typename TP>
+__global__ void __launch_bounds__(256) k_correct_force(const TP *__restrict__ pp, double *u, double *v, double *w,
+                                                       StepParams p, MeshDev m, int forced_x, const double *scalar)
+{
+    PL_POINT_INDEX();
+    const Nb n = neighbours(i, j, k, p.nx, p.ny);
+    const double dt = p.dt, dtdxi = dt * p.dx_inv, dtdyi = dt * p.dy_inv;
+    const size_t pc = n.c - sk;
+    const double p0 = (double)__ldg(pp + pc);
+    const double pxp = (double)__ldg(pp + n.xp - sk), pyp = (double)__ldg(pp + n.yp - sk);
+    const double pzp = (k < p.nz) ? (double)__ldg(pp + pc + sk) : p0;
+    double nu = u[n.c] - (pxp - p0) * dtdxi;
+    if (forced_x) nu = nu + __ldg(scalar + 3);
+    const double nv = v[n.c] - (pyp - p0) * dtdyi;
+    const double nw = w[n.c] - (pzp - p0) * dt * __ldg(m.dzc_inv + k);
+    u[n.c] = nu;
+    v[n.c] = nv;
+    w[n.c] = nw;
+    const double bcu = 0.0 - p.u_crf;
+    if (k == 1) {
+        u[n.c - sk] = 2.0 * bcu - nu;
+        v[n.c - sk] = -nv;
+    }
+    if (k == p.nz) {
+        u[n.c + sk] = 2.0 * bcu - nu;
+        v[n.c + sk] = -nv;
+    }
+}
+
+// ------------------------------------------------------------------------
+// mixed precision (u, v, w, p in FP64; stage increments and PPE in FP32)
+// ------------------------------------------------------------------------
+
+// RK1: d1 = dt * (visc - conv)(u) in FP32, i.e. u1 = u + d1.  Wall fill of
+// u1 (imposeNoSlipBC) in increment form: u1(0) = 2 bc - u1(1) and u(0) = 2 bc
+// - u(1) give d1(0) = -d1(1); w1 = w = 0 on the walls gives d1w = 0 there.
+__global__ void __launch_bounds__(256) k_rk1_mixed(const double *__restrict__ u, const double *__restrict__ v,
+                                                   const double *__restrict__ w, float *__restrict__ du,
+                                                   float *__restrict__ dv, float *__restrict__ dw, StepParams p,
+                                                   MeshDev m)
+{
+    PL_POINT_INDEX();
+    const Nb n = neighbours(i, j, k, p.nx, p.ny);
+    float ru, rv, rw;
+    momentum_rhs<float>(LoadF<double, float>{u}, LoadF<double, float>{v}, LoadF<double, float>{w}, n, k, p, m, ru,
+                        rv, rw);
+    const float dtf = (float)p.dt;
+    const float a = dtf * ru, b = dtf * rv;
+    du[n.c] = a;
+    dv[n.c] = b;
+    if (k != p.nz) dw[n.c] = dtf * rw;
+    wall_fill<float>(du, dv, dw, n.c, k, sk, p.nz, 0.0f, a, b);
+}
+
+// RK2: u_new = (u1 + dt*(visc - conv)(u1) + u) * 0.5 with u1 = u + d1, the
+// right-hand side in FP32 and the update in FP64; out of place (u is read
+// at the neighbours to rebuild u1).  Fused Mean_h of u_new.
+__global__ void __launch_bounds__(256) k_rk2_mixed(const double *__restrict__ u, const double *__restrict__ v,
+                                                   const double *__restrict__ w, const float *__restrict__ du,
+                                                   const float *__restrict__ dv, const float *__restrict__ dw,
+                                                   double *__restrict__ uo, double *__restrict__ vo,
+                                                   double *__restrict__ wo, StepParams p, MeshDev m, MeanRed red)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z + 1;
+    const size_t sk = (size_t)p.nx * p.ny;
+    double su = 0.0;
+    if (i < p.nx && j < p.ny) {
+        const Nb n = neighbours(i, j, k, p.nx, p.ny);
+        float ru, rv, rw;
+        momentum_rhs<float>(LoadSum{u, du}, LoadSum{v, dv}, LoadSum{w, dw}, n, k, p, m, ru, rv, rw);
+        const float dtf = (float)p.dt;
+        const double uc = __ldg(u + n.c), vc = __ldg(v + n.c), wc = __ldg(w + n.c);
+        const double nu = ((uc + (double)__ldg(du + n.c)) + (double)(dtf * ru) + uc) * 0.5;
+        const double nv = ((vc + (double)__ldg(dv + n.c)) + (double)(dtf * rv) + vc) * 0.5;
+        uo[n.c] = nu;
+        vo[n.c] = nv;
+        if (k != p.nz) wo[n.c] = ((wc + (double)__ldg(dw + n.c)) + (double)(dtf * rw) + wc) * 0.5;
+        wall_fill<double>(uo, vo, wo, n.c, k, sk, p.nz, 0.0 - p.u_crf, nu, nv);
+        su = nu * __ldg(m.dzflzi + k);
+    }
+    mean_reduce(su, red);
+}
+
+// Incremental pressure residual: r = div(u)/dt - L p_prev in FP64, stored in
+// FP32 (it is the small increment's right-hand side), with the FP64 plane
+// sums of r (the (kx,ky) = (0,0) right-hand side, solved in FP64).
+// L is exactly the operator the PPE inverts: periodic second differences
+// over dx^2, dy^2 and the partition's tridiagonal row a, bt, c in z.
+struct ZOp {
+    const double *a, *bt, *c; // per k (0-based interior), set_trid_coeff rows
+};
+
+__global__ void __launch_bounds__(256) k_rhs_mixed(const double *__restrict__ u, const double *__restrict__ v,
+                                                   const double *__restrict__ w, const double *__restrict__ pp,
+                                                   float *__restrict__ r, double *__restrict__ plane_part,
+                                                   StepParams p, MeshDev m, ZOp z, double dxi2, double dyi2,
+                                                   int incremental)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z + 1;
+    const size_t sk = (size_t)p.nx * p.ny;
+    double val = 0.0;
+    if (i < p.nx && j < p.ny) {
+        const Nb n = neighbours(i, j, k, p.nx, p.ny);
+        const double dti = 1.0 / p.dt, dtidxi = dti * p.dx_inv, dtidyi = dti * p.dy_inv;
+        double rhs = (__ldg(u + n.c) - __ldg(u + n.xm)) * dtidxi + (__ldg(v + n.c) - __ldg(v + n.ym)) * dtidyi +
+                     (__ldg(w + n.c) - __ldg(w + n.zm)) * dti * __ldg(m.dzf_inv + k);
+        if (incremental) {
+            const size_t pc = n.c - sk;
+            const double p0 = __ldg(pp + pc);
+            double lp = (__ldg(pp + n.xp - sk) - 2.0 * p0 + __ldg(pp + n.xm - sk)) * dxi2 +
+                        (__ldg(pp + n.yp - sk) - 2.0 * p0 + __ldg(pp + n.ym - sk)) * dyi2;
+            const int kk = k - 1;
+            lp += __ldg(z.bt + kk) * p0;
+            if (kk > 0) lp += __ldg(z.a + kk) * __ldg(pp + pc - sk);
+            if (kk < p.nz - 1) lp += __ldg(z.c + kk) * __ldg(pp + pc + sk);
+            rhs -= lp;
+        }
+        r[n.c - sk] = (float)rhs;
+        val = rhs;
+    }
+    double z0 = 0.0, z1 = 0.0;
+    block_sum3(val, z0, z1);
+    if (threadIdx.x == 0 && threadIdx.y == 0)
+        plane_part[(size_t)blockIdx.z * gridDim.x * gridDim.y + blockIdx.x + (size_t)gridDim.x * blockIdx.y] = val;
+}
+
+// per-plane sums of the block partials (fixed order): mode0[k] = sum_ij r
+__global__ void k_plane_sums(const double *plane_part, int nbxy, int nz, double *mode0)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nz) return;
+    double s = 0.0;
+    for (int b = 0; b < nbxy; b++) s += plane_part[(size_t)k * nbxy + b];
+    mode0[k] = s;
+}
+
+// correctVel with p = p_prev + dp (FP64 + FP32 increment), the new p stored
+// in FP64 in the other buffer, + forceVel shift + wall fill
+__global__ void __launch_bounds__(256) k_correct_mixed(const double *__restrict__ pprev, const float *__restrict__ dp,
+                                                       double *__restrict__ pnew, double *u, double *v, double *w,
+                                                       StepParams p, MeshDev m, int forced_x, const double *scalar,
+                                                       int incremental)
+{
+    PL_POINT_INDEX();
+    const Nb n = neighbours(i, j, k, p.nx, p.ny);
+    const size_t pc = n.c - sk;
+    auto P = [&](size_t q) { return (incremental ? __ldg(pprev + q) : 0.0) + (double)__ldg(dp + q); };
+    const double dt = p.dt, dtdxi = dt * p.dx_inv, dtdyi = dt * p.dy_inv;
+    const double p0 = P(pc);
+    const double pxp = P(n.xp - sk), pyp = P(n.yp - sk);
+    const double pzp = (k < p.nz) ? P(pc + sk) : p0;
+    pnew[pc] = p0;
+    double nu = u[n.c] - (pxp - p0) * dtdxi;
+    if (forced_x) nu = nu + __ldg(scalar + 3);
+    const double nv = v[n.c] - (pyp - p0) * dtdyi;
+    const double nw = w[n.c] - (pzp - p0) * dt * __ldg(m.dzc_inv + k);
+    u[n.c] = nu;
+    v[n.c] = nv;
+    w[n.c] = nw;
+    const double bcu = 0.0 - p.u_crf;
+    if (k == 1) {
+        u[n.c - sk] = 2.0 * bcu - nu;
+        v[n.c - sk] = -nv;
+    }
+    if (k == p.nz) {
+        u[n.c + sk] = 2.0 * bcu - nu;
+        v[n.c + sk] = -nv;
+    }
+}
+
+// ------------------------------------------------------------------------
 // launchers
 // ------------------------------------------------------------------------
 static inline dim3 point_block() { return dim3(64, 4, 1); }
@@ -633,6 +881,73 @@ int launch_fill_bc_vel(double *u, double *v, double *w, const StepParams &p, cud
 {
     dim3 g((p.nx + 63) / 64, (p.ny + 3) / 4, 1);
     k_fill_bc<<<g, point_block(), 0, st>>>(u, v, w, p);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
+int launch_rk2m_fp64(double *u, double *v, double *w, const double *u1, const double *v1, const double *w1,
+                     const StepParams &p, const MeshDev &m, MeanState &ms, cudaStream_t st)
+{
+    if (nblocks(p) > ms.max_blocks) {
+        set_error("mean buffer too small");
+        return -1;
+    }
+    MeanRed r{ms.partial, ms.counter, ms.scalar, (double)p.nx, (double)p.ny, ms.vel_force};
+    k_rk2m_fp64<<<point_grid(p), point_block(), 0, st>>>(u, v, w, u1, v1, w1, p, m, r);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
+int launch_correct_force_fp64(const double *p_, double *u, double *v, double *w, const StepParams &p,
+                              const MeshDev &m, int forced_x, const double *scalar, cudaStream_t st)
+{
+    k_correct_force<double><<<point_grid(p), point_block(), 0, st>>>(p_, u, v, w, p, m, forced_x, scalar);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
+int launch_rk1_mixed(const double *u, const double *v, const double *w, float *d1u, float *d1v, float *d1w,
+                     const StepParams &p, const MeshDev &m, cudaStream_t st)
+{
+    k_rk1_mixed<<<point_grid(p), point_block(), 0, st>>>(u, v, w, d1u, d1v, d1w, p, m);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
+int launch_rk2_mixed(const double *u, const double *v, const double *w, const float *d1u, const float *d1v,
+                     const float *d1w, double *uo, double *vo, double *wo, const StepParams &p, const MeshDev &m,
+                     MeanState &ms, cudaStream_t st)
+{
+    if (nblocks(p) > ms.max_blocks) {
+        set_error("mean buffer too small");
+        return -1;
+    }
+    MeanRed r{ms.partial, ms.counter, ms.scalar, (double)p.nx, (double)p.ny, ms.vel_force};
+    k_rk2_mixed<<<point_grid(p), point_block(), 0, st>>>(u, v, w, d1u, d1v, d1w, uo, vo, wo, p, m, r);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
+int launch_rhs_mixed(const double *u, const double *v, const double *w, const double *pprev, float *r,
+                     double *plane_part, double *mode0, const StepParams &p, const MeshDev &m, const double *za,
+                     const double *zbt, const double *zc, double dxi2, double dyi2, int incremental, cudaStream_t st)
+{
+    ZOp z{za, zbt, zc};
+    k_rhs_mixed<<<point_grid(p), point_block(), 0, st>>>(u, v, w, pprev, r, plane_part, p, m, z, dxi2, dyi2,
+                                                          incremental);
+    PL_CHECK_LAUNCH();
+    dim3 g = point_grid(p);
+    k_plane_sums<<<(p.nz + 127) / 128, 128, 0, st>>>(plane_part, (int)(g.x * g.y), p.nz, mode0);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
+int launch_correct_mixed(const double *pprev, const float *dp, double *pnew, double *u, double *v, double *w,
+                         const StepParams &p, const MeshDev &m, int forced_x, const double *scalar, int incremental,
+                         cudaStream_t st)
+{
+    k_correct_mixed<<<point_grid(p), point_block(), 0, st>>>(pprev, dp, pnew, u, v, w, p, m, forced_x, scalar,
+                                                              incremental);
     PL_CHECK_LAUNCH();
     return 0;
 }

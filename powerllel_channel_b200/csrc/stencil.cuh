@@ -37,16 +37,34 @@ int launch_correct_fp64(const double *p_, double *u, double *v, double *w, const
 int launch_force_fp64(double *u, double *v, double *w, const StepParams &p, const int forced[3],
                       const double vel_force[3], ReduceBuf &rb, cudaStream_t st);
 
-// mixed-precision step kernels: u,v,w FP64; RK increments and p FP32
+// Mean_h of the RK2 output reduced inside the RK2 kernel (deterministic
+// last-block sum); scalar[3] = vel_force(1) - Mean_h, applied by the
+// correction kernel (forceVel)
+struct MeanState {
+    double *partial = nullptr;       // >= max_blocks
+    unsigned int *counter = nullptr; // zero-initialised once
+    double *scalar = nullptr;        // >= 4
+    int max_blocks = 0;
+    double vel_force = 0.0;
+};
+
+int launch_rk2m_fp64(double *u, double *v, double *w, const double *u1, const double *v1, const double *w1,
+                     const StepParams &p, const MeshDev &m, MeanState &ms, cudaStream_t st);
+int launch_correct_force_fp64(const double *p_, double *u, double *v, double *w, const StepParams &p,
+                              const MeshDev &m, int forced_x, const double *scalar, cudaStream_t st);
+
+// mixed precision: u, v, w, p in FP64; stage-1 increments and PPE in FP32
 int launch_rk1_mixed(const double *u, const double *v, const double *w, float *d1u, float *d1v, float *d1w,
                      const StepParams &p, const MeshDev &m, cudaStream_t st);
 int launch_rk2_mixed(const double *u, const double *v, const double *w, const float *d1u, const float *d1v,
                      const float *d1w, double *uo, double *vo, double *wo, const StepParams &p, const MeshDev &m,
-                     cudaStream_t st);
-int launch_calc_rhs_mixed(const double *u, const double *v, const double *w, float *rhs, double *rhs_mode0,
-                          const StepParams &p, const MeshDev &m, cudaStream_t st);
-int launch_correct_mixed(const float *p_, double *u, double *v, double *w, const StepParams &p, const MeshDev &m,
-                         const int forced[3], ReduceBuf &rb, cudaStream_t st);
+                     MeanState &ms, cudaStream_t st);
+int launch_rhs_mixed(const double *u, const double *v, const double *w, const double *pprev, float *r,
+                     double *plane_part, double *mode0, const StepParams &p, const MeshDev &m, const double *za,
+                     const double *zbt, const double *zc, double dxi2, double dyi2, int incremental, cudaStream_t st);
+int launch_correct_mixed(const double *pprev, const float *dp, double *pnew, double *u, double *v, double *w,
+                         const StepParams &p, const MeshDev &m, int forced_x, const double *scalar, int incremental,
+                         cudaStream_t st);
 
 // diagnostics: out[0] = max|div| , out[1] = max CFL (already * dt), out[2] =
 // NaN count over u,v,w (ghosts included); loc[0..2] ijk of the div max,

@@ -1,0 +1,77 @@
+"""CPU tests of the library's host logic: the tridiagonal tables of
+trid_tables.h (shared with the CUDA code) replayed with the kernels' column
+algorithm must reproduce the reference's golden PPE outputs; the half-complex
+transforms are taken from numpy here, so this isolates the table logic."""
+import ctypes as C
+import glob
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, ROOT
+
+_lib = None
+
+
+def host_lib():
+    global _lib
+    if _lib is None:
+        d = tempfile.mkdtemp(prefix="host_trid_")
+        so = os.path.join(d, "libhost_trid.so")
+        subprocess.run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-ffp-contract=off", "-o", so,
+                        os.path.join(ROOT, "tests", "host_trid.cpp")], check=True)
+        _lib = C.CDLL(so)
+        _lib.host_trid_solve.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                         C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double)]
+    return _lib
+
+
+def r2hc(x, axis):
+    n = x.shape[axis]
+    X = np.fft.rfft(x, axis=axis)
+    out = np.empty_like(x)
+    idx = [slice(None)] * x.ndim
+    for k in range(n // 2 + 1):
+        idx[axis] = k
+        out[tuple(idx)] = X.take(k, axis=axis).real
+    for k in range(1, (n + 1) // 2):
+        idx[axis] = n - k
+        out[tuple(idx)] = X.take(k, axis=axis).imag
+    return out
+
+
+def hc2r(h, axis):
+    n = h.shape[axis]
+    X = np.zeros(h.shape[:axis] + (n // 2 + 1,) + h.shape[axis + 1:], dtype=complex)
+    idx = [slice(None)] * h.ndim
+    for k in range(n // 2 + 1):
+        idx[axis] = k
+        re = h[tuple(idx)]
+        im = 0.0
+        if 0 < k < n - k:
+            j2 = list(idx)
+            j2[axis] = n - k
+            im = h[tuple(j2)]
+        X[tuple(idx)] = re + 1j * im
+    return np.fft.irfft(X, n=n, axis=axis) * n
+
+
+GOLDEN_PPE = sorted(glob.glob(os.path.join(GOLDEN, "ppe_*.npz")))
+
+
+@pytest.mark.parametrize("path", GOLDEN_PPE, ids=[os.path.basename(p)[:-4] for p in GOLDEN_PPE])
+def test_trid_tables_reproduce_reference(path):
+    d = np.load(path)
+    nx, ny, nz = int(d["nx"]), int(d["ny"]), int(d["nz"])
+    nparts = int(d["p_col"]) if int(d["pdd"]) else 0
+    x = np.ascontiguousarray(r2hc(r2hc(d["rhs"], 2), 1))
+    dzf = np.ascontiguousarray(d["dzf"])
+    host_lib().host_trid_solve(nx, ny, nz, float(d["dx"]), float(d["dy"]), dzf.ctypes.data_as(C.POINTER(C.c_double)),
+                               nparts, x.ctypes.data_as(C.POINTER(C.c_double)))
+    p = hc2r(hc2r(x, 1), 2) / (nx * ny)
+    ref = d["p"]
+    err = np.abs((p - p.mean()) - (ref - ref.mean())).max() / np.abs(ref - ref.mean()).max()
+    assert err < 1e-12, err

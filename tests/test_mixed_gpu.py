@@ -1,0 +1,82 @@
+"""GPU tests of the mixed-precision path against the FP64 oracle.
+
+The mixed path keeps u, v, w and p in FP64, evaluates the momentum stencils in
+FP32 (stage-1 increments stored in FP32), and solves for the pressure
+increment with FP32 FFTs around an FP64 tridiagonal elimination; the
+right-hand side of the increment (div u/dt - L p_prev) and the (0,0) mode are
+FP64.  Acceptance (north star): velocity relative L2 error <= 1e-5 against the
+FP64 oracle and max |div u| <= 1e-10."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l2(a, b):
+    a = a[1:-1, 1:-1, 1:-1]
+    b = b[1:-1, 1:-1, 1:-1]
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def rel_max(a, b):
+    a = a[1:-1, 1:-1, 1:-1]
+    b = b[1:-1, 1:-1, 1:-1]
+    return float(np.abs(a - b).max() / np.abs(b).max())
+
+
+@pytest.mark.parametrize("nx,ny,nz,nsteps", [(64, 64, 64, 20), (96, 72, 48, 10)])
+def test_mixed_vs_fp64_oracle(gpu, oracle_mod, nx, ny, nz, nsteps):
+    plb, O = gpu, oracle_mod
+    cfg = plb.ChannelConfig(nx=nx, ny=ny, nz=nz, stretch_ratio=1.5, re_tau=180.0, precision=plb.PL_MIXED)
+    ch = plb.Channel(cfg)
+    ch.init_flow(42, 0.1)
+    ch.step(nsteps)
+    gu, gv, gw, gp = ch.get_fields()
+    d = ch.diagnostics()
+    g = O.Grid(nx, ny, nz, stretch=1.5, re_tau=180.0)
+    u, v, w, p = g.init_flow(42, 0.1)
+    ppe = O.PPE(nx, ny, nz, g.g.dx, g.g.dy, g.dzf_global)
+    u1, v1, w1 = g.zeros(), g.zeros(), g.zeros()
+    for _ in range(nsteps):
+        g.step(ppe, u, v, w, u1, v1, w1, p)
+    errs = {n: (rel_l2(a, b), rel_max(a, b)) for n, a, b in (("u", gu, u), ("v", gv, v), ("w", gw, w))}
+    for n, (l2, mx) in errs.items():
+        assert l2 <= 1e-5, (n, l2, mx)
+    assert d["div_max"] <= 1e-10, d
+    assert d["nan_count"] == 0
+
+
+def test_mixed_phase_rk1_increment(gpu, oracle_mod):
+    """RK1 in FP32 arithmetic: u1 = u + d1 within FP32 round-off of dt*RHS."""
+    plb, O = gpu, oracle_mod
+    nx, ny, nz = 48, 36, 24
+    cfg = plb.ChannelConfig(nx=nx, ny=ny, nz=nz, stretch_ratio=1.5, re_tau=180.0, precision=plb.PL_MIXED)
+    ch = plb.Channel(cfg)
+    g = O.Grid(nx, ny, nz, stretch=1.5, re_tau=180.0)
+    u, v, w, _ = g.init_flow(7, 0.2)
+    ch.set_fields(u, v, w)
+    u1, v1, w1 = g.rk1(u, v, w)
+    g.bound_vel(u1, v1, w1)
+    ch.phase("rk1")
+    for which, ref, base in ((4, u1, u), (5, v1, v), (6, w1, w)):
+        got = ch.get_field(which)
+        inc = np.abs(ref - base).max()
+        assert np.abs(got - ref).max() <= 2e-5 * inc + 1e-15, which
+
+
+def test_mixed_full_size_accuracy(gpu):
+    """512x384x256 (the bench size), 100 steps: the mixed path against the
+    FP64 path of this library (itself pinned to the oracle at small sizes)."""
+    plb = gpu
+    res = {}
+    for prec in (plb.PL_FP64, plb.PL_MIXED):
+        cfg = plb.ChannelConfig(nx=512, ny=384, nz=256, stretch_ratio=2.0, re_tau=1000.0, precision=prec)
+        ch = plb.Channel(cfg)
+        ch.init_flow(11, 0.1)
+        ch.step(100)
+        res[prec] = (ch.get_field(0), ch.get_field(1), ch.get_field(2), ch.diagnostics())
+        ch.close()
+    for q in range(3):
+        assert rel_l2(res[plb.PL_MIXED][q], res[plb.PL_FP64][q]) <= 1e-5
+    assert res[plb.PL_MIXED][3]["div_max"] <= 1e-10
+    assert res[plb.PL_FP64][3]["div_max"] <= 1e-10

@@ -26,6 +26,31 @@ def relerr_modmean(a, b):
     return np.abs(a - b).max() / np.abs(b).max()
 
 
+def partitions(nz, nparts):
+    """z-partitions of decomp_2d.c:261-283 (0-based start, size)"""
+    size, nu = nz // nparts, nz % nparts
+    sz = [size if m < nparts - nu else size + 1 for m in range(nparts)]
+    return [(sum(sz[:m]), sz[m]) for m in range(nparts)]
+
+
+def relerr_pdd(a, b, nparts):
+    """PDD with two partitions has a single interface whose 2x2 reduced system
+    is the exact one, and for the (kx,ky) = (0,0) mode that system inherits
+    the singularity of the Neumann problem (det = w*v - 1 is round-off): the
+    reference's solution then carries an arbitrary constant per partition,
+    fixed by round-off.  Compare modulo one constant per partition there;
+    with P >= 3 the truncated interface systems are regular and one global
+    constant is the only freedom."""
+    if nparts != 2:
+        return relerr_modmean(a, b)
+    a = a.copy()
+    b = b.copy()
+    for k0, ke in partitions(a.shape[0], nparts):
+        a[k0:k0 + ke] -= a[k0:k0 + ke].mean()
+        b[k0:k0 + ke] -= b[k0:k0 + ke].mean()
+    return np.abs(a - b).max() / np.abs(b).max()
+
+
 GOLDEN_PPE = sorted(glob.glob(os.path.join(GOLDEN, "ppe_*.npz")))
 
 
@@ -41,7 +66,7 @@ def test_reference_abi_vs_golden(gpu, path):
     var[1:-1, 1:-1, 1:-1] = d["rhs"]
     with plb.PoissonSolver(nx, ny, nz, float(d["dx"]), float(d["dy"]), d["dzf"], nparts=nparts) as s:
         s.execute(var)
-    assert relerr_modmean(var[1:-1, 1:-1, 1:-1], d["p"]) < TOL64
+    assert relerr_pdd(var[1:-1, 1:-1, 1:-1], d["p"], nparts) < TOL64
     ghost = var.copy()
     ghost[1:-1, 1:-1, 1:-1] = 7.25
     assert np.all(ghost == 7.25)
@@ -58,7 +83,7 @@ def test_device_ppe_vs_golden(gpu, path):
     x = torch.tensor(d["rhs"], dtype=torch.float64, device="cuda").contiguous()
     s.solve(x)
     torch.cuda.synchronize()
-    assert relerr_modmean(x.cpu().numpy(), d["p"]) < TOL64
+    assert relerr_pdd(x.cpu().numpy(), d["p"], nparts) < TOL64
     # repeated solves are deterministic (no races in the kernels)
     y = torch.tensor(d["rhs"], dtype=torch.float64, device="cuda").contiguous()
     s.solve(y)
@@ -67,7 +92,7 @@ def test_device_ppe_vs_golden(gpu, path):
 
 
 @pytest.mark.parametrize("nx,ny,nz,nparts", [(64, 64, 64, 0), (128, 96, 48, 0), (256, 192, 32, 4),
-                                            (64, 48, 40, 8), (96, 72, 30, 4)])
+                                            (64, 48, 40, 8), (96, 72, 30, 4), (64, 48, 32, 2)])
 def test_ppe_vs_oracle_live(gpu, oracle_mod, nx, ny, nz, nparts):
     """Sizes beyond the fixtures (radix-3 lengths, uneven PDD partitions)."""
     import torch
@@ -84,14 +109,15 @@ def test_ppe_vs_oracle_live(gpu, oracle_mod, nx, ny, nz, nparts):
     x = torch.tensor(r, dtype=torch.float64, device="cuda").contiguous()
     s.solve(x)
     torch.cuda.synchronize()
-    assert relerr_modmean(x.cpu().numpy(), var[1:-1, 1:-1, 1:-1]) < TOL64
+    assert relerr_pdd(x.cpu().numpy(), var[1:-1, 1:-1, 1:-1], nparts) < TOL64
 
 
 @pytest.mark.parametrize("mx,my", [(1, 0), (0, 1), (3, 2), (16, 12), (32, 0)])
 def test_ppe_single_modes(gpu, oracle_mod, mx, my):
     """Manufactured solution: p = cos(2 pi mx x/Lx + 0.3) cos(2 pi my y/Ly),
     uniform in z, solves L p = lambda p exactly (lambda the discrete
-    eigenvalue, mod_fft_fftw.inc:180-183)."""
+    eigenvalue, mod_fft_fftw.inc:180-183).  Tolerance relative to the input
+    amplitude: high modes have |lambda| >> 1, so p is much smaller than f."""
     import torch
     plb, O = gpu, oracle_mod
     nx, ny, nz = 64, 48, 16
@@ -106,7 +132,7 @@ def test_ppe_single_modes(gpu, oracle_mod, mx, my):
     s.solve(t)
     torch.cuda.synchronize()
     got = t.cpu().numpy()
-    assert np.abs((got - got.mean()) - (f / lam - (f / lam).mean())).max() < 1e-12 * np.abs(f / lam).max()
+    assert np.abs((got - got.mean()) - (f / lam - (f / lam).mean())).max() < 1e-13 * np.abs(f).max()
 
 
 def test_ppe_linearity_full_size(gpu):

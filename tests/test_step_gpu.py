@@ -1,8 +1,8 @@
 """GPU parity of the RK2 projection step (FP64 path) against the oracle.
 
 Every phase is compared on the same input state; the whole step is compared
-after several steps.  Velocities are compared directly (max|diff| / max|u|),
-the pressure modulo its mean (the Neumann null mode, see test_ppe_gpu).
+after several steps.  Velocities are compared directly (max|diff| / max|u|), the pressure modulo its
+mean (the Neumann null mode, see test_ppe_gpu) relative to max|p|.
 FP64 tolerance 1e-12 relative."""
 import os
 
@@ -21,9 +21,13 @@ def rel(a, b):
 
 
 def rel_modmean(a, b):
+    """pressure: modulo the Neumann null mode (its mean), relative to the stored
+    field's magnitude -- the reference fixes the null-mode constant by
+    dividing round-off by the round-off last pivot, so digits below
+    eps*max|p| carry no information in either implementation"""
     a = a[1:-1, 1:-1, 1:-1]
     b = b[1:-1, 1:-1, 1:-1]
-    return rel(a - a.mean(), b - b.mean())
+    return np.abs((a - a.mean()) - (b - b.mean())).max() / max(np.abs(b).max(), 1e-300)
 
 
 def make_pair(plb, O, nx, ny, nz, stretch=1.5, re_tau=180.0, nparts=0, seed=42, noise=0.1, dt=1e-4):
@@ -82,7 +86,10 @@ def test_phase_rk2_rhs_ppe_correct(gpu, oracle_mod):
     g.calc_rhs(u, v, w, p)
     ch.phase("calc_rhs")
     got = ch.get_field(3)
-    assert rel(got[1:-1, 1:-1, 1:-1], p[1:-1, 1:-1, 1:-1]) < TOL64
+    # div(u)/dt cancels terms of size |u|/(dx dt): measure the error on that scale
+    scale = (np.abs(u).max() * g.g.dx_inv + np.abs(v).max() * g.g.dy_inv
+             + np.abs(w).max() * g.arr1d("dzf_inv").max()) / g.g.dt
+    assert np.abs(got[1:-1, 1:-1, 1:-1] - p[1:-1, 1:-1, 1:-1]).max() < 1e-14 * scale
     ppe.execute(p)
     g.bound_p(p)
     ch.phase("poisson")
@@ -114,7 +121,12 @@ def test_steps_match_oracle(gpu, oracle_mod, nparts):
     assert rel_modmean(gp, p) < 1e-10
     d = ch.diagnostics()
     div_o, ijk = g.max_div(u, v, w)
-    assert d["div_max"] < 1e-12 and div_o < 1e-12
+    if nparts == 0:
+        assert d["div_max"] < 1e-12 and div_o < 1e-12
+    else:
+        # PDD truncates the low-wavenumber systems (the reference's algorithm),
+        # so the projection leaves a divergence; it must be the reference's
+        assert abs(d["div_max"] - div_o) < 1e-9 * div_o and tuple(d["div_ijk"]) == ijk
     cfl_o, cijk = g.max_cfl(u, v, w)
     assert abs(d["cfl_max"] - cfl_o) < 1e-12 * cfl_o and tuple(d["cfl_ijk"]) == cijk
     assert d["nan_count"] == 0
@@ -168,6 +180,10 @@ def test_full_size_step_invariants(gpu):
         res.append(u)
         ch.close()
     assert np.array_equal(res[0], res[1])
-    g_dzf = None  # bulk velocity: dz-weighted mean of u (Mean_h) equals 1 after forceVel
+    # forceVel holds the dz-weighted bulk velocity (Mean_h) at vel_force = 1
+    nz = 256
+    zf = 0.5 * (1.0 + np.tanh((np.arange(nz + 1) / nz - 0.5) * 2.0) / np.tanh(1.0))
+    dzf = 2.0 * np.diff(zf)
     u = res[0][1:-1, 1:-1, 1:-1]
-    assert u.shape == (256, 384, 512)
+    bulk = (u.mean(axis=(1, 2)) * dzf / 2.0).sum()
+    assert abs(bulk - 1.0) < 1e-12
