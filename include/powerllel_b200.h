@@ -137,6 +137,8 @@ void *pl_channel_stream(pl_channel *c);
  * 4. Per-phase entries on the channel's device fields (one kernel each,
  *    asynchronous; the step calls them in this order)
  * ====================================================================== */
+int pl_phase_rk(pl_channel *c);         /* both stages in one kernel when nx % 32 == 0 and ny % 8 == 0
+                                           (what pl_channel_step runs), else rk1 then rk2 */
 int pl_phase_rk1(pl_channel *c);        /* timeIntVelRK1 + updateBoundVel(u1) */
 int pl_phase_rk2(pl_channel *c);        /* timeIntVelRK2 + updateBoundVel(u) */
 int pl_phase_calc_rhs(pl_channel *c);   /* calcRHS into p */

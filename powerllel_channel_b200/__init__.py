@@ -98,7 +98,7 @@ def lib():
     L.pl_channel_stream.argtypes = [C.c_void_p]
     L.pl_channel_stream.restype = C.c_void_p
     L.pl_channel_profile.argtypes = [C.c_void_p, C.c_int, _dp, C.c_char_p, C.c_int]
-    for name in ("pl_phase_rk1", "pl_phase_rk2", "pl_phase_calc_rhs", "pl_phase_poisson", "pl_phase_correct_force"):
+    for name in ("pl_phase_rk", "pl_phase_rk1", "pl_phase_rk2", "pl_phase_calc_rhs", "pl_phase_poisson", "pl_phase_correct_force"):
         getattr(L, name).argtypes = [C.c_void_p]
     _lib = L
     return L

@@ -191,10 +191,12 @@ struct pl_channel {
     double *u = nullptr, *v = nullptr, *w = nullptr;
     double *u1 = nullptr, *v1 = nullptr, *w1 = nullptr;
     double *p = nullptr;
-    double *ub = nullptr, *vb = nullptr, *wb = nullptr, *pb = nullptr;
+    double *ub = nullptr, *vb = nullptr, *wb = nullptr, *pb = nullptr, *pm = nullptr;
     float *d1u = nullptr, *d1v = nullptr, *d1w = nullptr, *r32 = nullptr;
     double *plane_part = nullptr, *mode0 = nullptr;
-    int incremental = 1;
+    int incremental = 1;   // mixed path: solve for a pressure increment (Thomas)
+    long long nsolve = 0;  // projections since the initial field (mixed prediction schedule)
+    bool fused_rk = false; // both RK stages in one kernel (rk_fused.cu)
     Ppe ppe;
     ReduceBuf rb;
     MeanState ms;
@@ -281,6 +283,7 @@ static void channel_free(pl_channel *c)
     cudaFree(c->vb);
     cudaFree(c->wb);
     cudaFree(c->pb);
+    cudaFree(c->pm);
     cudaFree(c->d1u);
     cudaFree(c->d1v);
     cudaFree(c->d1w);
@@ -357,13 +360,14 @@ extern "C" int pl_channel_create(pl_channel **out, const pl_channel_config *cfg)
         cudaMemset(*f, 0, sizeof(float) * n);
         return true;
     };
-    bool ok = dalloc(&c->u, c->nf) && dalloc(&c->v, c->nf) && dalloc(&c->w, c->nf) && dalloc(&c->p, c->np);
+    c->fused_rk = rk_fused_supported(c->sp);
+    bool ok = dalloc(&c->u, c->nf) && dalloc(&c->v, c->nf) && dalloc(&c->w, c->nf) && dalloc(&c->p, c->np) &&
+              dalloc(&c->ub, c->nf) && dalloc(&c->vb, c->nf) && dalloc(&c->wb, c->nf);
     if (ok && !mixed) ok = dalloc(&c->u1, c->nf) && dalloc(&c->v1, c->nf) && dalloc(&c->w1, c->nf);
     if (ok && mixed)
-        ok = dalloc(&c->ub, c->nf) && dalloc(&c->vb, c->nf) && dalloc(&c->wb, c->nf) && dalloc(&c->pb, c->np) &&
-             falloc(&c->d1u, c->nf) && falloc(&c->d1v, c->nf) && falloc(&c->d1w, c->nf) && falloc(&c->r32, c->np) &&
-             dalloc(&c->mode0, c->nz) &&
-             dalloc(&c->plane_part, (size_t)((c->nx + 63) / 64) * ((c->ny + 3) / 4) * c->nz);
+        ok = dalloc(&c->pb, c->np) && dalloc(&c->pm, c->np) && falloc(&c->d1u, c->nf) && falloc(&c->d1v, c->nf) &&
+             falloc(&c->d1w, c->nf) && falloc(&c->r32, c->np) && dalloc(&c->mode0, c->nz) &&
+             dalloc(&c->plane_part, (size_t)warp_partials_per_plane(c->sp) * c->nz);
     if (!ok) {
         set_error("pl_channel_create: out of device memory for the fields");
         return fail();
@@ -376,6 +380,7 @@ extern "C" int pl_channel_create(pl_channel **out, const pl_channel_config *cfg)
                    mixed ? PREC_MIXED : PREC_FP64))
         return fail();
     c->max_blocks = ((c->nx + 63) / 64) * ((c->ny + 3) / 4) * c->nz;
+    if (c->fused_rk && rk_fused_blocks(c->sp) > c->max_blocks) c->max_blocks = rk_fused_blocks(c->sp);
     c->rb.max_blocks = c->max_blocks;
     if (cudaMalloc(&c->rb.partial, sizeof(double) * 3 * c->max_blocks) != cudaSuccess ||
         cudaMalloc(&c->rb.scalar, sizeof(double) * 8) != cudaSuccess ||
@@ -424,6 +429,8 @@ extern "C" int pl_channel_init_flow(pl_channel *c, uint64_t seed, double noise)
     PL_CUDA_TRY(cudaMemsetAsync(c->w, 0, sizeof(double) * c->nf, c->stream));
     PL_CUDA_TRY(cudaMemsetAsync(c->p, 0, sizeof(double) * c->np, c->stream));
     if (c->pb) PL_CUDA_TRY(cudaMemsetAsync(c->pb, 0, sizeof(double) * c->np, c->stream));
+    if (c->pm) PL_CUDA_TRY(cudaMemsetAsync(c->pm, 0, sizeof(double) * c->np, c->stream));
+    c->nsolve = 0;
     int rc = launch_init_fill(c->u, c->v, c->w, dprof, seed, noise, c->sp, c->stream);
     if (!rc) rc = launch_mean_sum(c->u, c->sp, c->m, c->rb, 0, c->stream);
     if (!rc) rc = launch_init_finish(c->u, c->v, c->w, c->sp, c->cfg.u_ref, c->rb, c->stream);
@@ -458,13 +465,28 @@ extern "C" int pl_phase_rk2(pl_channel *c)
     return rc;
 }
 
+// mixed path pressure prediction: the first two projections after the
+// initial field solve for the full pressure (the first one removes the
+// initial divergence, an outlier in time); then the increment over p_n, and
+// from the fourth on over the extrapolation 2 p_n - p_{n-1}
+static int mixed_mode(const pl_channel *c, const double **pn, const double **pnm1)
+{
+    *pn = c->p;
+    *pnm1 = c->p;
+    if (!c->incremental || c->nsolve < 2) return 0;
+    if (c->nsolve >= 3) *pnm1 = c->pm;
+    return 1;
+}
+
 extern "C" int pl_phase_calc_rhs(pl_channel *c)
 {
     int rc;
     if (is_mixed(c)) {
         const double dx = c->cfg.lx / c->nx, dy = c->cfg.ly / c->ny;
-        rc = launch_rhs_mixed(c->u, c->v, c->w, c->p, c->r32, c->plane_part, c->mode0, c->sp, c->m, c->ppe.d_a,
-                              c->ppe.d_bt, c->ppe.d_c, 1.0 / (dx * dx), 1.0 / (dy * dy), c->incremental, c->stream);
+        const double *pn, *pnm1;
+        const int inc = mixed_mode(c, &pn, &pnm1);
+        rc = launch_rhs_mixed(c->u, c->v, c->w, pn, pnm1, c->r32, c->plane_part, c->mode0, c->sp, c->m, c->ppe.d_a,
+                              c->ppe.d_bt, c->ppe.d_c, 1.0 / (dx * dx), 1.0 / (dy * dy), inc, c->stream);
     } else {
         rc = launch_calc_rhs_fp64(c->u, c->v, c->w, c->p, c->sp, c->m, c->stream);
     }
@@ -474,7 +496,7 @@ extern "C" int pl_phase_calc_rhs(pl_channel *c)
 
 extern "C" int pl_phase_poisson(pl_channel *c)
 {
-    if (is_mixed(c)) return ppe_solve_fp32(&c->ppe, c->r32, c->incremental ? c->mode0 : nullptr, c->stream);
+    if (is_mixed(c)) return ppe_solve_fp32(&c->ppe, c->r32, c->mode0, c->stream);
     return ppe_solve_fp64(&c->ppe, c->p, c->stream);
 }
 
@@ -482,14 +504,39 @@ extern "C" int pl_phase_correct_force(pl_channel *c)
 {
     int rc;
     if (is_mixed(c)) {
-        rc = launch_correct_mixed(c->p, c->r32, c->pb, c->u, c->v, c->w, c->sp, c->m, c->cfg.is_forced[0],
-                                  c->ms.scalar, c->incremental, c->stream);
-        std::swap(c->p, c->pb);
+        const double *pn, *pnm1;
+        const int inc = mixed_mode(c, &pn, &pnm1);
+        rc = launch_correct_mixed(pn, pnm1, c->r32, c->pb, c->u, c->v, c->w, c->sp, c->m, c->cfg.is_forced[0],
+                                  c->ms.scalar, inc, c->stream);
+        // rotate: p_{n-1} <- p_n, p_n <- p_new
+        double *old_pm = c->pm;
+        c->pm = c->p;
+        c->p = c->pb;
+        c->pb = old_pm;
+        c->nsolve++;
     } else {
         rc = launch_correct_force_fp64(c->p, c->u, c->v, c->w, c->sp, c->m, c->cfg.is_forced[0], c->ms.scalar,
                                        c->stream);
     }
     channel_mark(c, "correct_force");
+    return rc;
+}
+
+// both RK stages in one kernel (out of place), when the grid tiles by 32 x 8
+extern "C" int pl_phase_rk(pl_channel *c)
+{
+    int rc;
+    if (!c->fused_rk) {
+        rc = pl_phase_rk1(c);
+        if (!rc) rc = pl_phase_rk2(c);
+        return rc;
+    }
+    rc = is_mixed(c) ? launch_rk_fused_mixed(c->u, c->v, c->w, c->ub, c->vb, c->wb, c->sp, c->m, c->ms, c->stream)
+                     : launch_rk_fused_fp64(c->u, c->v, c->w, c->ub, c->vb, c->wb, c->sp, c->m, c->ms, c->stream);
+    std::swap(c->u, c->ub);
+    std::swap(c->v, c->vb);
+    std::swap(c->w, c->wb);
+    channel_mark(c, "rk_fused");
     return rc;
 }
 
@@ -540,9 +587,7 @@ extern "C" int pl_channel_profile(pl_channel *c, int nsteps, double *ms, char *n
 extern "C" int pl_channel_step(pl_channel *c, int nsteps)
 {
     for (int s = 0; s < nsteps; s++) {
-        if (pl_phase_rk1(c) || pl_phase_rk2(c) || pl_phase_calc_rhs(c) || pl_phase_poisson(c) ||
-            pl_phase_correct_force(c))
-            return -1;
+        if (pl_phase_rk(c) || pl_phase_calc_rhs(c) || pl_phase_poisson(c) || pl_phase_correct_force(c)) return -1;
     }
     return 0;
 }
@@ -645,6 +690,7 @@ extern "C" int pl_channel_get_field(pl_channel *c, int which, double *host)
 extern "C" int pl_channel_set_fields(pl_channel *c, const double *u, const double *v, const double *w)
 {
     PL_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->nsolve = 0; // a new state: the pressure history no longer applies
     const int nx = c->nx, ny = c->ny, nz = c->nz;
     const size_t gx = nx + 2, gxy = gx * (ny + 2);
     std::vector<double> tmp(c->nf);

@@ -195,12 +195,32 @@ __device__ __forceinline__ void thomas_column(const T *xin, double *xs, T *xout,
 }
 
 template <typename T>
-__global__ void __launch_bounds__(128) k_thomas(const T *xin, double *xs, T *xout, TridDev t)
+__global__ void __launch_bounds__(128) k_thomas(const T *xin, double *xs, T *xout, TridDev t, const double *mode0)
 {
     const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y;
     if (px >= t.nx) return;
     const size_t col = (size_t)px + (size_t)t.nx * py, stride = (size_t)t.nx * t.ny;
     const size_t cls = trid_class(px, py, t), cstride = (size_t)t.ncx * t.ncy;
+    if (mode0 != nullptr && col == 0) {
+        // Mixed path, (kx,ky) = (0,0): the Neumann system is singular (its
+        // last pivot is round-off), so its FP32-transformed right-hand side
+        // is not consistent to the precision the division needs.  Solve it in
+        // FP64 from the FP64 plane sums of the right-hand side, with the
+        // gauge x[nz-1] = 0 fixing the free constant.
+        double xp = mode0[0];
+        xs[0] = xp;
+        for (int k = 1; k < t.nz; k++) {
+            xp = mode0[k] - __ldg(t.mult + (size_t)k * cstride) * xp;
+            xs[(size_t)k * stride] = xp;
+        }
+        double xn = 0.0;
+        xout[(size_t)(t.nz - 1) * stride] = (T)0;
+        for (int k = t.nz - 2; k >= 0; k--) {
+            xn = (xs[(size_t)k * stride] - __ldg(t.c + k) * xn) * __ldg(t.rb + (size_t)k * cstride);
+            xout[(size_t)k * stride] = (T)xn;
+        }
+        return;
+    }
     thomas_column<T>(xin, xs, xout, col, cls, stride, cstride, 0, t.nz, t);
 }
 
@@ -247,30 +267,6 @@ __global__ void __launch_bounds__(128) k_pdd(double *xs, T *xout, TridDev t, Pdd
             xout[g] = (T)(xs[g] - __ldg(p.v + gc) * y1 - __ldg(p.w + gc) * y2);
         }
         y1 = y3;
-    }
-}
-
-// Mixed path, (kx,ky) = (0,0): the Neumann system is singular (its last pivot
-// is round-off), so its FP32-transformed right-hand side cannot be trusted to
-// the consistency the division needs.  Solve it in FP64 from the FP64 plane
-// sums with the gauge x[nz-1] = 0 (fixes the free constant) and store the
-// result in the transformed array.  One thread; nz sequential rows.
-__global__ void k_mode0(float *x, double *xs, const double *__restrict__ mode0, TridDev t)
-{
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    // class 0 and column 0 are the (0,0) slot; xs is the FP64 sweep buffer
-    const size_t stride = (size_t)t.nx * t.ny, cstride = (size_t)t.ncx * t.ncy;
-    double xp = mode0[0];
-    xs[0] = xp;
-    for (int k = 1; k < t.nz; k++) {
-        xp = mode0[k] - __ldg(t.mult + (size_t)k * cstride) * xp;
-        xs[(size_t)k * stride] = xp;
-    }
-    double xn = 0.0; // gauge: x[nz-1] = 0 instead of dividing by the round-off pivot
-    x[(size_t)(t.nz - 1) * stride] = 0.0f;
-    for (int k = t.nz - 2; k >= 0; k--) {
-        xn = (xs[(size_t)k * stride] - __ldg(t.c + k) * xn) * __ldg(t.rb + (size_t)k * cstride);
-        x[(size_t)k * stride] = (float)xn;
     }
 }
 
@@ -477,13 +473,13 @@ template <typename T> static int launch_y(const Ppe *s, bool fwd, T *data, cudaS
     return 0;
 }
 
-template <typename T> static int launch_trid(Ppe *s, T *x, cudaStream_t st)
+template <typename T> static int launch_trid(Ppe *s, T *x, cudaStream_t st, const double *mode0 = nullptr)
 {
     TridDev t{s->nx, s->ny, s->nz, s->ncx, s->ncy, s->d_mult, s->d_rb, s->d_c};
     dim3 grid((s->nx + 127) / 128, s->ny);
     double *xs = (sizeof(T) == 8 && s->nparts == 0) ? reinterpret_cast<double *>(x) : s->d_scratch;
     if (s->nparts == 0) {
-        k_thomas<T><<<grid, 128, 0, st>>>(x, xs, x, t);
+        k_thomas<T><<<grid, 128, 0, st>>>(x, xs, x, t, mode0);
     } else {
         if (sizeof(T) == 4) {
             k_widen<<<1184, 256, 0, st>>>(reinterpret_cast<const float *>(x), xs, s->scratch_elems);
@@ -541,12 +537,7 @@ int ppe_solve_fp32(Ppe *s, float *d_var, const double *mode0, cudaStream_t st)
     mark(s, "ppe_xfft_fwd");
     if (launch_y<float>(s, true, d_var, st)) return -1;
     mark(s, "ppe_yfft_fwd");
-    if (launch_trid<float>(s, d_var, st)) return -1;
-    if (mode0 && s->nparts == 0) {
-        TridDev t{s->nx, s->ny, s->nz, s->ncx, s->ncy, s->d_mult, s->d_rb, s->d_c};
-        k_mode0<<<1, 32, 0, st>>>(d_var, s->d_scratch, mode0, t);
-        PL_CHECK_LAUNCH();
-    }
+    if (launch_trid<float>(s, d_var, st, s->nparts == 0 ? mode0 : nullptr)) return -1;
     mark(s, s->nparts ? "ppe_pdd" : "ppe_thomas");
     if (launch_y<float>(s, false, d_var, st)) return -1;
     mark(s, "ppe_yfft_bwd");

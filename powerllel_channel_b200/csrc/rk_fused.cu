@@ -1,0 +1,252 @@
+// rk_fused.cu -- both RK2 stages of timeIntVelRK1 / timeIntVelRK2
+// (mod_calcVel.f90:52-146, 240-334) with their wall fills in one kernel.
+//
+// 2.5D blocking: a CTA owns a 32 x 8 tile of (i, j) and marches up a chunk of
+// k-planes.  Shared-memory rings hold the last planes of u (halo 2 in x, y)
+// and of the stage-1 field (halo 1): each plane of u is read from HBM once,
+// the stage-1 field u1 = u + dt*RHS(u) never leaves the SM, and the stage-2
+// update is written once.  HBM traffic per point: read u, v, w and write the
+// new u, v, w, instead of writing and re-reading u1, v1, w1 between two
+// kernels.
+//
+// FP64 path: the rings hold u and u1 in double, the expressions are the
+// reference's.  Mixed path: the rings hold u in float and the stage-1
+// increment d1 = dt*RHS(u) in float (u1 = u + d1 for the stencils, FP32
+// arithmetic); the update u_new = (u1 + dt*RHS(u1) + u)/2 uses the FP64 u of
+// the centre and is stored in FP64.
+#include "stencil.cuh"
+#include "stencil_rhs.cuh"
+
+namespace pl {
+
+constexpr int FX = 32, FY = 8;          // tile
+constexpr int UW = FX + 4, UH = FY + 4; // ring plane with a halo of 2
+constexpr int UPS = UW * UH;            // 432 values per plane
+
+template <bool MIXED> struct RkTraits;
+template <> struct RkTraits<false> {
+    using R = double;       // ring and stencil arithmetic type
+    static constexpr int NS = 3; // planes per ring
+};
+template <> struct RkTraits<true> {
+    using R = float;
+    static constexpr int NS = 4;
+};
+
+template <typename R> struct RingLoad {
+    const R *a;
+    __device__ __forceinline__ R operator()(size_t q) const { return a[q]; }
+};
+
+// mixed path: u1 = u + d1 on the ring
+struct RingSum {
+    const float *a, *d;
+    __device__ __forceinline__ float operator()(size_t q) const { return a[q] + d[q]; }
+};
+
+__device__ __forceinline__ Nb ring_nb(int x, int y, int s0, int sm, int sp)
+{
+    Nb n;
+    const size_t xy = (size_t)y * UW + x;
+    n.c = (size_t)s0 * UPS + xy;
+    n.xm = n.c - 1;
+    n.xp = n.c + 1;
+    n.ym = n.c - UW;
+    n.yp = n.c + UW;
+    n.zm = (size_t)sm * UPS + xy;
+    n.zp = (size_t)sp * UPS + xy;
+    n.xpym = n.c + 1 - UW;
+    n.xmyp = n.c - 1 + UW;
+    n.xpzm = n.zm + 1;
+    n.xmzp = n.zp - 1;
+    n.ypzm = n.zm + UW;
+    n.ymzp = n.zp - UW;
+    return n;
+}
+
+template <bool MIXED>
+__global__ void __launch_bounds__(FX *FY) k_rk_fused(const double *__restrict__ u, const double *__restrict__ v,
+                                                     const double *__restrict__ w, double *__restrict__ uo,
+                                                     double *__restrict__ vo, double *__restrict__ wo, StepParams p,
+                                                     MeshDev m, MeanRed red, int kchunk)
+{
+    using R = typename RkTraits<MIXED>::R;
+    constexpr int NS = RkTraits<MIXED>::NS;
+    constexpr int FS = NS * UPS; // ring size per field
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R *ur = reinterpret_cast<R *>(smem_raw); // u, v, w rings
+    R *qr = ur + 3 * FS;                     // u1 (FP64) or d1 (mixed) rings
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + ty * FX, nthr = FX * FY;
+    const int i0 = blockIdx.x * FX, j0 = blockIdx.y * FY;
+    const int kbeg = blockIdx.z * kchunk + 1, kend = min(kbeg + kchunk - 1, p.nz);
+    const size_t sk = (size_t)p.nx * p.ny;
+    const R dt = (R)p.dt;
+    const R bcu = (R)(0.0 - p.u_crf);
+
+    auto load_u_plane = [&](int kq) { // kq in [0, nz+1]; periodic x, y halo
+        const int s = kq % NS;
+        for (int q = tid; q < UPS; q += nthr) {
+            const int lx = q % UW, ly = q / UW;
+            int gi = i0 - 2 + lx, gj = j0 - 2 + ly;
+            gi += (gi < 0) ? p.nx : 0;
+            gi -= (gi >= p.nx) ? p.nx : 0;
+            gj += (gj < 0) ? p.ny : 0;
+            gj -= (gj >= p.ny) ? p.ny : 0;
+            const size_t g = (size_t)gi + (size_t)p.nx * gj + sk * kq;
+            ur[0 * FS + s * UPS + q] = (R)__ldg(u + g);
+            ur[1 * FS + s * UPS + q] = (R)__ldg(v + g);
+            ur[2 * FS + s * UPS + q] = (R)__ldg(w + g);
+        }
+    };
+
+    // stage 1 on the halo-1 region of plane mq (1 <= mq <= nz)
+    auto produce = [&](int mq) {
+        const int s0 = mq % NS, sm = (mq - 1) % NS, sp = (mq + 1) % NS;
+        for (int q = tid; q < (FX + 2) * (FY + 2); q += nthr) {
+            const int x = q % (FX + 2) + 1, y = q / (FX + 2) + 1;
+            const Nb n = ring_nb(x, y, s0, sm, sp);
+            R ru, rv, rw;
+            momentum_rhs<R>(RingLoad<R>{ur}, RingLoad<R>{ur + FS}, RingLoad<R>{ur + 2 * FS}, n, mq, p, m, ru, rv,
+                            rw);
+            if (MIXED) { // increments
+                qr[n.c] = dt * ru;
+                qr[FS + n.c] = dt * rv;
+                qr[2 * FS + n.c] = (mq == p.nz) ? (R)0 : dt * rw; // w1(nz) = 0 = w(nz)
+            } else {      // u1 = u + dt*(visc - conv)
+                qr[n.c] = ur[n.c] + dt * ru;
+                qr[FS + n.c] = ur[FS + n.c] + dt * rv;
+                qr[2 * FS + n.c] = (mq == p.nz) ? (R)0 : ur[2 * FS + n.c] + dt * rw;
+            }
+        }
+    };
+
+    // imposeNoSlipBC on the stage-1 field: plane kg from plane ki (0 <- 1, nz+1 <- nz)
+    auto wall = [&](int kg, int ki) {
+        const int sg = kg % NS, si = ki % NS;
+        for (int q = tid; q < (FX + 2) * (FY + 2); q += nthr) {
+            const int x = q % (FX + 2) + 1, y = q / (FX + 2) + 1;
+            const size_t xy = (size_t)y * UW + x;
+            if (MIXED) { // u1(g) = 2bc - u1(i) and u(g) = 2bc - u(i)  =>  d1(g) = -d1(i)
+                qr[sg * UPS + xy] = -qr[si * UPS + xy];
+                qr[FS + sg * UPS + xy] = -qr[FS + si * UPS + xy];
+            } else {
+                qr[sg * UPS + xy] = (R)2 * bcu - qr[si * UPS + xy];
+                qr[FS + sg * UPS + xy] = -qr[FS + si * UPS + xy];
+            }
+            qr[2 * FS + sg * UPS + xy] = (R)0;
+        }
+    };
+
+    double su = 0.0;
+    // stage 2 at interior plane kq from the stage-1 planes kq-1, kq, kq+1
+    auto stage2 = [&](int kq) {
+        const int s0 = kq % NS, sm = (kq - 1) % NS, sp = (kq + 1) % NS;
+        const Nb n = ring_nb(tx + 2, ty + 2, s0, sm, sp);
+        R ru, rv, rw;
+        if (MIXED)
+            momentum_rhs<R>(RingSum{(const float *)ur, (const float *)qr},
+                            RingSum{(const float *)ur + FS, (const float *)qr + FS},
+                            RingSum{(const float *)ur + 2 * FS, (const float *)qr + 2 * FS}, n, kq, p, m, ru, rv, rw);
+        else
+            momentum_rhs<R>(RingLoad<R>{qr}, RingLoad<R>{qr + FS}, RingLoad<R>{qr + 2 * FS}, n, kq, p, m, ru, rv,
+                            rw);
+        const size_t g = (size_t)(i0 + tx) + (size_t)p.nx * (j0 + ty) + sk * kq;
+        const double uc = __ldg(u + g), vc = __ldg(v + g), wc = __ldg(w + g);
+        double nu, nv, nw;
+        if (MIXED) {
+            nu = ((uc + (double)qr[n.c]) + (double)(dt * ru) + uc) * 0.5;
+            nv = ((vc + (double)qr[FS + n.c]) + (double)(dt * rv) + vc) * 0.5;
+            nw = ((wc + (double)qr[2 * FS + n.c]) + (double)(dt * rw) + wc) * 0.5;
+        } else {
+            nu = ((double)qr[n.c] + p.dt * (double)ru + uc) * 0.5;
+            nv = ((double)qr[FS + n.c] + p.dt * (double)rv + vc) * 0.5;
+            nw = ((double)qr[2 * FS + n.c] + p.dt * (double)rw + wc) * 0.5;
+        }
+        uo[g] = nu;
+        vo[g] = nv;
+        if (kq != p.nz) wo[g] = nw;
+        wall_fill<double>(uo, vo, wo, g, kq, sk, p.nz, 0.0 - p.u_crf, nu, nv);
+        su += nu * __ldg(m.dzflzi + kq);
+    };
+
+    const int mstart = max(kbeg - 1, 1), mend = min(kend + 1, p.nz);
+    load_u_plane(mstart - 1);
+    load_u_plane(mstart);
+    for (int mq = mstart; mq <= mend; mq++) {
+        load_u_plane(mq + 1);
+        __syncthreads();
+        produce(mq);
+        __syncthreads();
+        if (mq == 1) {
+            wall(0, 1);
+            __syncthreads();
+        }
+        if (mq - 1 >= kbeg && mq - 1 <= kend) stage2(mq - 1);
+        if (mq == p.nz) {
+            // the top wall plane reuses the ring slot of u1(nz-2), which
+            // stage2(nz-1) above has just consumed
+            __syncthreads();
+            wall(p.nz + 1, p.nz);
+            __syncthreads();
+            if (p.nz >= kbeg && p.nz <= kend) stage2(p.nz);
+        }
+        __syncthreads();
+    }
+    mean_reduce(su, red);
+}
+
+static int fused_chunks(const StepParams &p)
+{
+    const int tiles = (p.nx / FX) * (p.ny / FY);
+    int nch = (1184 + tiles - 1) / tiles;
+    const int maxch = p.nz / 16 > 1 ? p.nz / 16 : 1;
+    if (nch > maxch) nch = maxch;
+    if (nch < 1) nch = 1;
+    return nch;
+}
+
+bool rk_fused_supported(const StepParams &p) { return p.nx % FX == 0 && p.ny % FY == 0 && p.nz >= 2; }
+
+int rk_fused_blocks(const StepParams &p) { return (p.nx / FX) * (p.ny / FY) * fused_chunks(p); }
+
+template <bool MIXED>
+static int launch_rk_fused_t(const double *u, const double *v, const double *w, double *uo, double *vo, double *wo,
+                             const StepParams &p, const MeshDev &m, MeanState &ms, cudaStream_t st)
+{
+    if (!rk_fused_supported(p)) {
+        set_error("fused RK kernel needs nx % 32 == 0 and ny % 8 == 0");
+        return -1;
+    }
+    const int nch = fused_chunks(p);
+    const int kchunk = (p.nz + nch - 1) / nch;
+    dim3 grid(p.nx / FX, p.ny / FY, (p.nz + kchunk - 1) / kchunk);
+    if ((int)(grid.x * grid.y * grid.z) > ms.max_blocks) {
+        set_error("mean buffer too small for the fused RK kernel");
+        return -1;
+    }
+    using R = typename RkTraits<MIXED>::R;
+    const size_t shm = sizeof(R) * 6 * RkTraits<MIXED>::NS * UPS;
+    static bool attr_set = false;
+    if (!attr_set) {
+        PL_CUDA_TRY(cudaFuncSetAttribute(k_rk_fused<MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        attr_set = true;
+    }
+    MeanRed r{ms.partial, ms.counter, ms.scalar, (double)p.nx, (double)p.ny, ms.vel_force};
+    k_rk_fused<MIXED><<<grid, dim3(FX, FY), shm, st>>>(u, v, w, uo, vo, wo, p, m, r, kchunk);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
+int launch_rk_fused_fp64(const double *u, const double *v, const double *w, double *uo, double *vo, double *wo,
+                         const StepParams &p, const MeshDev &m, MeanState &ms, cudaStream_t st)
+{
+    return launch_rk_fused_t<false>(u, v, w, uo, vo, wo, p, m, ms, st);
+}
+
+int launch_rk_fused_mixed(const double *u, const double *v, const double *w, double *uo, double *vo, double *wo,
+                          const StepParams &p, const MeshDev &m, MeanState &ms, cudaStream_t st)
+{
+    return launch_rk_fused_t<true>(u, v, w, uo, vo, wo, p, m, ms, st);
+}
+
+} // namespace pl

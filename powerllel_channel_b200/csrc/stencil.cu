@@ -8,139 +8,9 @@
 // which reproduces imposeNoSlipBC (mod_updateBound.f90:312-368) applied after
 // the periodic fills.
 #include "stencil.cuh"
+#include "stencil_rhs.cuh"
 
 namespace pl {
-
-// ------------------------------------------------------------------------
-// momentum right-hand side (timeIntVelRK1_kernel, mod_calcVel.f90:74-138;
-// timeIntVelRK2_kernel evaluates the same expressions on u1, :262-326)
-// ------------------------------------------------------------------------
-struct Nb {
-    size_t c, xm, xp, ym, yp, zm, zp, xpym, xmyp, xpzm, xmzp, ypzm, ymzp;
-};
-
-__device__ __forceinline__ Nb neighbours(int i, int j, int k, int nx, int ny)
-{
-    const int im = (i == 0) ? nx - 1 : i - 1, ip = (i == nx - 1) ? 0 : i + 1;
-    const int jm = (j == 0) ? ny - 1 : j - 1, jp = (j == ny - 1) ? 0 : j + 1;
-    const size_t sk = (size_t)nx * ny;
-    const size_t row = (size_t)nx * j + sk * k, rowm = (size_t)nx * jm + sk * k, rowp = (size_t)nx * jp + sk * k;
-    Nb n;
-    n.c = row + i;
-    n.xm = row + im;
-    n.xp = row + ip;
-    n.ym = rowm + i;
-    n.yp = rowp + i;
-    n.zm = n.c - sk;
-    n.zp = n.c + sk;
-    n.xpym = rowm + ip; // (i+1, j-1)
-    n.xmyp = rowp + im; // (i-1, j+1)
-    n.xpzm = n.xp - sk; // (i+1, k-1)
-    n.xmzp = n.xm + sk; // (i-1, k+1)
-    n.ypzm = n.yp - sk; // (j+1, k-1)
-    n.ymzp = n.ym + sk; // (j-1, k+1)
-    return n;
-}
-
-// Field accessor: plain load converted to the compute type.
-template <typename TS, typename TC> struct LoadF {
-    const TS *__restrict__ a;
-    __device__ __forceinline__ TC operator()(size_t q) const { return (TC)__ldg(a + q); }
-};
-
-// Accessor of the mixed path's stage-1 field u1 = u + d1 (u FP64, d1 FP32),
-// rounded to FP32 for the FP32 stencil arithmetic.
-struct LoadSum {
-    const double *__restrict__ a;
-    const float *__restrict__ d;
-    __device__ __forceinline__ float operator()(size_t q) const
-    {
-        return (float)(__ldg(a + q) + (double)__ldg(d + q));
-    }
-};
-
-template <typename TC, typename AU, typename AV, typename AW>
-__device__ __forceinline__ void momentum_rhs(const AU &u, const AV &v, const AW &w, const Nb &n, int k,
-                                             const StepParams &p, const MeshDev &m, TC &ru, TC &rv, TC &rw)
-{
-    const TC dx_inv = (TC)p.dx_inv, dy_inv = (TC)p.dy_inv, re_inv = (TC)p.re_inv, u_crf = (TC)p.u_crf;
-    const TC dzf_k = (TC)__ldg(m.dzf + k), dzf_kp = (TC)__ldg(m.dzf + k + 1), dzf_km = (TC)__ldg(m.dzf + k - 1);
-    const TC dzci_k = (TC)__ldg(m.dzc_inv + k), dzci_km = (TC)__ldg(m.dzc_inv + k - 1);
-    const TC dzfi_k = (TC)__ldg(m.dzf_inv + k), dzfi_kp = (TC)__ldg(m.dzf_inv + k + 1);
-    const TC h = (TC)0.25, half = (TC)0.5;
-
-    const TC uc = u(n.c), uxp = u(n.xp), uxm = u(n.xm), uyp = u(n.yp), uym = u(n.ym), uzp = u(n.zp), uzm = u(n.zm);
-    const TC vc = v(n.c), vxp = v(n.xp), vxm = v(n.xm), vyp = v(n.yp), vym = v(n.ym), vzp = v(n.zp), vzm = v(n.zm);
-    const TC wc = w(n.c), wxp = w(n.xp), wxm = w(n.xm), wyp = w(n.yp), wym = w(n.ym), wzp = w(n.zp), wzm = w(n.zm);
-    TC ue, uw, un, us, ut, ub, vn, vs, wt, wb, ve, vw, vt, vb, we, ww, wn, ws;
-    TC dqe, dqw, dqn, dqs, dqt, dqb, conv, visc;
-
-    // u-equation (:74-94)
-    ue = (uc + uxp);
-    uw = (uxm + uc);
-    un = (uc + uyp);
-    us = (uym + uc);
-    ut = (uc * dzf_kp + uzp * dzf_k) * dzci_k;
-    ub = (uc * dzf_km + uzm * dzf_k) * dzci_km;
-    vn = (vc + vxp);
-    vs = (vym + v(n.xpym));
-    wt = (wc + wxp);
-    wb = (wzm + w(n.xpzm));
-    dqe = (uxp - uc) * dx_inv;
-    dqw = (uc - uxm) * dx_inv;
-    dqn = (uyp - uc) * dy_inv;
-    dqs = (uc - uym) * dy_inv;
-    dqt = (uzp - uc) * dzci_k;
-    dqb = (uc - uzm) * dzci_km;
-    conv = h * ((ue * ue - uw * uw) * dx_inv + (un * vn - us * vs) * dy_inv + (ut * wt - ub * wb) * dzfi_k);
-    conv = conv + half * u_crf * (ue - uw) * dx_inv;
-    visc = ((dqe - dqw) * dx_inv + (dqn - dqs) * dy_inv + (dqt - dqb) * dzfi_k) * re_inv;
-    ru = visc - conv;
-
-    // v-equation (:96-116)
-    ve = (vc + vxp);
-    vw = (vxm + vc);
-    vn = (vc + vyp);
-    vs = (vym + vc);
-    vt = (vc * dzf_kp + vzp * dzf_k) * dzci_k;
-    vb = (vc * dzf_km + vzm * dzf_k) * dzci_km;
-    ue = (uc + uyp);
-    uw = (uxm + u(n.xmyp));
-    wt = (wc + wyp);
-    wb = (wzm + w(n.ypzm));
-    dqe = (vxp - vc) * dx_inv;
-    dqw = (vc - vxm) * dx_inv;
-    dqn = (vyp - vc) * dy_inv;
-    dqs = (vc - vym) * dy_inv;
-    dqt = (vzp - vc) * dzci_k;
-    dqb = (vc - vzm) * dzci_km;
-    conv = h * ((ue * ve - uw * vw) * dx_inv + (vn * vn - vs * vs) * dy_inv + (wt * vt - wb * vb) * dzfi_k);
-    conv = conv + half * u_crf * (ve - vw) * dx_inv;
-    visc = ((dqe - dqw) * dx_inv + (dqn - dqs) * dy_inv + (dqt - dqb) * dzfi_k) * re_inv;
-    rv = visc - conv;
-
-    // w-equation (:118-138)
-    we = (wc + wxp);
-    ww = (wxm + wc);
-    wn = (wc + wyp);
-    ws = (wym + wc);
-    wt = (wc + wzp);
-    wb = (wc + wzm);
-    ue = (uc * dzf_kp + uzp * dzf_k) * dzci_k;
-    uw = (uxm * dzf_kp + u(n.xmzp) * dzf_k) * dzci_k;
-    vn = (vc * dzf_kp + vzp * dzf_k) * dzci_k;
-    vs = (vym * dzf_kp + v(n.ymzp) * dzf_k) * dzci_k;
-    dqe = (wxp - wc) * dx_inv;
-    dqw = (wc - wxm) * dx_inv;
-    dqn = (wyp - wc) * dy_inv;
-    dqs = (wc - wym) * dy_inv;
-    dqt = (wzp - wc) * dzfi_kp;
-    dqb = (wc - wzm) * dzfi_k;
-    conv = h * ((ue * we - uw * ww) * dx_inv + (vn * wn - vs * ws) * dy_inv + (wt * wt - wb * wb) * dzci_k);
-    conv = conv + half * u_crf * (we - ww) * dx_inv;
-    visc = ((dqe - dqw) * dx_inv + (dqn - dqs) * dy_inv + (dqt - dqb) * dzci_k) * re_inv;
-    rw = visc - conv;
-}
 
 #define PL_POINT_INDEX()                                                                   \
     const int i = blockIdx.x * blockDim.x + threadIdx.x;                                   \
@@ -148,24 +18,6 @@ __device__ __forceinline__ void momentum_rhs(const AU &u, const AV &v, const AW 
     const int k = blockIdx.z + 1;                                                          \
     if (i >= p.nx || j >= p.ny) return;                                                    \
     const size_t sk = (size_t)p.nx * p.ny;
-
-// wall fills of imposeNoSlipBC for the plane just written (k == 1 or nz)
-template <typename T>
-__device__ __forceinline__ void wall_fill(T *u, T *v, T *w, size_t c, int k, size_t sk, int nz, T bcu, T uval,
-                                          T vval)
-{
-    if (k == 1) {
-        u[c - sk] = (T)2.0 * bcu - uval;
-        v[c - sk] = -vval;
-        w[c - sk] = (T)0;
-    }
-    if (k == nz) {
-        u[c + sk] = (T)2.0 * bcu - uval;
-        v[c + sk] = -vval;
-        w[c] = (T)0;
-        w[c + sk] = (T)0;
-    }
-}
 
 // RK1: u1 = u + dt*(visc - conv) (mod_calcVel.f90:94,116,138) + wall fill
 __global__ void __launch_bounds__(256) k_rk1_fp64(const double *__restrict__ u, const double *__restrict__ v,
@@ -215,36 +67,6 @@ __global__ void __launch_bounds__(256) k_calc_rhs_fp64(const double *__restrict_
     const double dti = 1.0 / p.dt, dtidxi = dti * p.dx_inv, dtidyi = dti * p.dy_inv;
     rhs[n.c - sk] = (__ldg(u + n.c) - __ldg(u + n.xm)) * dtidxi + (__ldg(v + n.c) - __ldg(v + n.ym)) * dtidyi +
                     (__ldg(w + n.c) - __ldg(w + n.zm)) * dti * __ldg(m.dzf_inv + k);
-}
-
-// block-wide sum of three values; result valid in thread 0
-__device__ __forceinline__ void block_sum3(double &a, double &b, double &c)
-{
-    __shared__ double sh[3][32];
-    const int lane = (threadIdx.x + threadIdx.y * blockDim.x) & 31;
-    const int wid = (threadIdx.x + threadIdx.y * blockDim.x) >> 5;
-    const int nw = (blockDim.x * blockDim.y + 31) >> 5;
-    for (int o = 16; o > 0; o >>= 1) {
-        a += __shfl_down_sync(0xffffffffu, a, o);
-        b += __shfl_down_sync(0xffffffffu, b, o);
-        c += __shfl_down_sync(0xffffffffu, c, o);
-    }
-    if (lane == 0) {
-        sh[0][wid] = a;
-        sh[1][wid] = b;
-        sh[2][wid] = c;
-    }
-    __syncthreads();
-    if (wid == 0) {
-        a = lane < nw ? sh[0][lane] : 0.0;
-        b = lane < nw ? sh[1][lane] : 0.0;
-        c = lane < nw ? sh[2][lane] : 0.0;
-        for (int o = 16; o > 0; o >>= 1) {
-            a += __shfl_down_sync(0xffffffffu, a, o);
-            b += __shfl_down_sync(0xffffffffu, b, o);
-            c += __shfl_down_sync(0xffffffffu, c, o);
-        }
-    }
 }
 
 // correctVel (mod_calcVel.f90:436-450) + dz-weighted sums for Mean_h
@@ -520,53 +342,6 @@ __global__ void __launch_bounds__(256) k_fill_bc(double *u, double *v, double *w
     w[cn + sk] = 0.0;
 }
 
-// ------------------------------------------------------------------------
-// Mean_h of the new streamwise velocity, fused into the RK2 kernels.
-// forceVel (mod_calcVel.f90:463-476) shifts u by vel_force - Mean_h(u) after
-// correctVel.  correctVel changes sum_i u by -dt/dx * sum_i (p_{i+1} - p_i),
-// which telescopes to zero on the periodic x lines, so Mean_h of the
-// corrected u equals Mean_h of the RK2 output (up to round-off): the shift is
-// computed here and applied by the correction kernel, saving a pass.
-// Block partials are summed by the last block in a fixed order
-// (deterministic).
-// ------------------------------------------------------------------------
-struct MeanRed {
-    double *partial;        // one per block
-    unsigned int *counter;  // zero between launches
-    double *scalar;         // [0] = Mean_h, [3] = vel_force - Mean_h
-    double dnx, dny, vel_force;
-};
-
-__device__ __forceinline__ void mean_reduce(double su, const MeanRed &r)
-{
-    double z0 = 0.0, z1 = 0.0;
-    block_sum3(su, z0, z1);
-    __shared__ bool last;
-    const int t = threadIdx.x + threadIdx.y * blockDim.x;
-    const unsigned int nb = gridDim.x * gridDim.y * gridDim.z;
-    if (t == 0) {
-        const size_t b = blockIdx.x + (size_t)gridDim.x * (blockIdx.y + (size_t)gridDim.y * blockIdx.z);
-        r.partial[b] = su;
-        __threadfence();
-        last = (atomicAdd(r.counter, 1u) == nb - 1);
-    }
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    const int nthr = blockDim.x * blockDim.y;
-    double s = 0.0;
-    for (unsigned int q = t; q < nb; q += nthr) s += __ldcg(r.partial + q);
-    z0 = z1 = 0.0;
-    __syncthreads();
-    block_sum3(s, z0, z1);
-    if (t == 0) {
-        const double mean = s / r.dnx / r.dny;
-        r.scalar[0] = mean;
-        r.scalar[3] = r.vel_force - mean;
-        *r.counter = 0u;
-    }
-}
-
 // RK2 (FP64) with the fused Mean_h of the new u
 __global__ void __launch_bounds__(256) k_rk2m_fp64(double *u, double *v, double *w, const double *__restrict__ u1,
                                                    const double *__restrict__ v1, const double *__restrict__ w1,
@@ -679,20 +454,27 @@ __global__ void __launch_bounds__(256) k_rk2_mixed(const double *__restrict__ u,
     mean_reduce(su, red);
 }
 
-// Incremental pressure residual: r = div(u)/dt - L p_prev in FP64, stored in
+// Incremental pressure residual: r = div(u)/dt - L p_pred in FP64, stored in
 // FP32 (it is the small increment's right-hand side), with the FP64 plane
 // sums of r (the (kx,ky) = (0,0) right-hand side, solved in FP64).
+// p_pred = 2 p_n - p_{n-1} is the linear extrapolation of the pressure in
+// time: every FP32 error of the increment solve scales with |r|, and the
+// extrapolation makes r the second difference of p in time.
 // L is exactly the operator the PPE inverts: periodic second differences
-// over dx^2, dy^2 and the partition's tridiagonal row a, bt, c in z.
+// over dx^2, dy^2 and the tridiagonal row a, bt, c in z.
 struct ZOp {
     const double *a, *bt, *c; // per k (0-based interior), set_trid_coeff rows
 };
 
+struct PPred {
+    const double *__restrict__ pn, *__restrict__ pnm1;
+    __device__ __forceinline__ double operator()(size_t q) const { return 2.0 * __ldg(pn + q) - __ldg(pnm1 + q); }
+};
+
 __global__ void __launch_bounds__(256) k_rhs_mixed(const double *__restrict__ u, const double *__restrict__ v,
-                                                   const double *__restrict__ w, const double *__restrict__ pp,
-                                                   float *__restrict__ r, double *__restrict__ plane_part,
-                                                   StepParams p, MeshDev m, ZOp z, double dxi2, double dyi2,
-                                                   int incremental)
+                                                   const double *__restrict__ w, PPred pp, float *__restrict__ r,
+                                                   double *__restrict__ warp_part, StepParams p, MeshDev m, ZOp z,
+                                                   double dxi2, double dyi2, int incremental)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -706,37 +488,47 @@ __global__ void __launch_bounds__(256) k_rhs_mixed(const double *__restrict__ u,
                      (__ldg(w + n.c) - __ldg(w + n.zm)) * dti * __ldg(m.dzf_inv + k);
         if (incremental) {
             const size_t pc = n.c - sk;
-            const double p0 = __ldg(pp + pc);
-            double lp = (__ldg(pp + n.xp - sk) - 2.0 * p0 + __ldg(pp + n.xm - sk)) * dxi2 +
-                        (__ldg(pp + n.yp - sk) - 2.0 * p0 + __ldg(pp + n.ym - sk)) * dyi2;
+            const double p0 = pp(pc);
+            double lp = (pp(n.xp - sk) - 2.0 * p0 + pp(n.xm - sk)) * dxi2 + (pp(n.yp - sk) - 2.0 * p0 + pp(n.ym - sk)) * dyi2;
             const int kk = k - 1;
             lp += __ldg(z.bt + kk) * p0;
-            if (kk > 0) lp += __ldg(z.a + kk) * __ldg(pp + pc - sk);
-            if (kk < p.nz - 1) lp += __ldg(z.c + kk) * __ldg(pp + pc + sk);
+            if (kk > 0) lp += __ldg(z.a + kk) * pp(pc - sk);
+            if (kk < p.nz - 1) lp += __ldg(z.c + kk) * pp(pc + sk);
             rhs -= lp;
         }
         r[n.c - sk] = (float)rhs;
         val = rhs;
     }
-    double z0 = 0.0, z1 = 0.0;
-    block_sum3(val, z0, z1);
-    if (threadIdx.x == 0 && threadIdx.y == 0)
-        plane_part[(size_t)blockIdx.z * gridDim.x * gridDim.y + blockIdx.x + (size_t)gridDim.x * blockIdx.y] = val;
+    // warp partials (no block barrier); summed per plane in a fixed order
+    for (int o = 16; o > 0; o >>= 1) val += __shfl_down_sync(0xffffffffu, val, o);
+    const int t = threadIdx.x + threadIdx.y * blockDim.x;
+    if ((t & 31) == 0) {
+        const int wpb = (blockDim.x * blockDim.y) >> 5;
+        const size_t b = blockIdx.x + (size_t)gridDim.x * blockIdx.y;
+        warp_part[((size_t)blockIdx.z * gridDim.x * gridDim.y + b) * wpb + (t >> 5)] = val;
+    }
 }
 
-// per-plane sums of the block partials (fixed order): mode0[k] = sum_ij r
-__global__ void k_plane_sums(const double *plane_part, int nbxy, int nz, double *mode0)
+// per-plane sums of the warp partials (fixed order): mode0[k] = sum_ij r
+__global__ void k_plane_sums(const double *part, int nper, int nz, double *mode0)
 {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.x;
     if (k >= nz) return;
     double s = 0.0;
-    for (int b = 0; b < nbxy; b++) s += plane_part[(size_t)k * nbxy + b];
-    mode0[k] = s;
+    for (int b = threadIdx.x; b < nper; b += blockDim.x) s += part[(size_t)k * nper + b];
+    __shared__ double sh[256];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) mode0[k] = sh[0];
 }
 
-// correctVel with p = p_prev + dp (FP64 + FP32 increment), the new p stored
-// in FP64 in the other buffer, + forceVel shift + wall fill
-__global__ void __launch_bounds__(256) k_correct_mixed(const double *__restrict__ pprev, const float *__restrict__ dp,
+// correctVel with p = p_pred + dp (FP64 prediction + FP32 increment), the new
+// p stored in FP64 in a third buffer, + forceVel shift + wall fill
+__global__ void __launch_bounds__(256) k_correct_mixed(PPred pp, const float *__restrict__ dp,
                                                        double *__restrict__ pnew, double *u, double *v, double *w,
                                                        StepParams p, MeshDev m, int forced_x, const double *scalar,
                                                        int incremental)
@@ -744,7 +536,7 @@ __global__ void __launch_bounds__(256) k_correct_mixed(const double *__restrict_
     PL_POINT_INDEX();
     const Nb n = neighbours(i, j, k, p.nx, p.ny);
     const size_t pc = n.c - sk;
-    auto P = [&](size_t q) { return (incremental ? __ldg(pprev + q) : 0.0) + (double)__ldg(dp + q); };
+    auto P = [&](size_t q) { return (incremental ? pp(q) : 0.0) + (double)__ldg(dp + q); };
     const double dt = p.dt, dtdxi = dt * p.dx_inv, dtdyi = dt * p.dy_inv;
     const double p0 = P(pc);
     const double pxp = P(n.xp - sk), pyp = P(n.yp - sk);
@@ -928,28 +720,36 @@ int launch_rk2_mixed(const double *u, const double *v, const double *w, const fl
     return 0;
 }
 
-int launch_rhs_mixed(const double *u, const double *v, const double *w, const double *pprev, float *r,
-                     double *plane_part, double *mode0, const StepParams &p, const MeshDev &m, const double *za,
-                     const double *zbt, const double *zc, double dxi2, double dyi2, int incremental, cudaStream_t st)
+int launch_rhs_mixed(const double *u, const double *v, const double *w, const double *pn, const double *pnm1,
+                     float *r, double *warp_part, double *mode0, const StepParams &p, const MeshDev &m,
+                     const double *za, const double *zbt, const double *zc, double dxi2, double dyi2, int incremental,
+                     cudaStream_t st)
 {
     ZOp z{za, zbt, zc};
-    k_rhs_mixed<<<point_grid(p), point_block(), 0, st>>>(u, v, w, pprev, r, plane_part, p, m, z, dxi2, dyi2,
+    k_rhs_mixed<<<point_grid(p), point_block(), 0, st>>>(u, v, w, PPred{pn, pnm1}, r, warp_part, p, m, z, dxi2, dyi2,
                                                           incremental);
     PL_CHECK_LAUNCH();
     dim3 g = point_grid(p);
-    k_plane_sums<<<(p.nz + 127) / 128, 128, 0, st>>>(plane_part, (int)(g.x * g.y), p.nz, mode0);
+    const int nper = (int)(g.x * g.y) * (int)((point_block().x * point_block().y) / 32);
+    k_plane_sums<<<p.nz, 256, 0, st>>>(warp_part, nper, p.nz, mode0);
     PL_CHECK_LAUNCH();
     return 0;
 }
 
-int launch_correct_mixed(const double *pprev, const float *dp, double *pnew, double *u, double *v, double *w,
-                         const StepParams &p, const MeshDev &m, int forced_x, const double *scalar, int incremental,
-                         cudaStream_t st)
+int launch_correct_mixed(const double *pn, const double *pnm1, const float *dp, double *pnew, double *u, double *v,
+                         double *w, const StepParams &p, const MeshDev &m, int forced_x, const double *scalar,
+                         int incremental, cudaStream_t st)
 {
-    k_correct_mixed<<<point_grid(p), point_block(), 0, st>>>(pprev, dp, pnew, u, v, w, p, m, forced_x, scalar,
-                                                              incremental);
+    k_correct_mixed<<<point_grid(p), point_block(), 0, st>>>(PPred{pn, pnm1}, dp, pnew, u, v, w, p, m, forced_x,
+                                                              scalar, incremental);
     PL_CHECK_LAUNCH();
     return 0;
+}
+
+int warp_partials_per_plane(const StepParams &p)
+{
+    dim3 g = point_grid(p);
+    return (int)(g.x * g.y) * (int)((point_block().x * point_block().y) / 32);
 }
 
 } // namespace pl

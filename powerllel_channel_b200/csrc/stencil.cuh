@@ -48,6 +48,14 @@ struct MeanState {
     double vel_force = 0.0;
 };
 
+// fused RK1 + RK2 (rk_fused.cu): u -> (uo, vo, wo) out of place
+bool rk_fused_supported(const StepParams &p);
+int rk_fused_blocks(const StepParams &p);
+int launch_rk_fused_fp64(const double *u, const double *v, const double *w, double *uo, double *vo, double *wo,
+                         const StepParams &p, const MeshDev &m, MeanState &ms, cudaStream_t st);
+int launch_rk_fused_mixed(const double *u, const double *v, const double *w, double *uo, double *vo, double *wo,
+                          const StepParams &p, const MeshDev &m, MeanState &ms, cudaStream_t st);
+
 int launch_rk2m_fp64(double *u, double *v, double *w, const double *u1, const double *v1, const double *w1,
                      const StepParams &p, const MeshDev &m, MeanState &ms, cudaStream_t st);
 int launch_correct_force_fp64(const double *p_, double *u, double *v, double *w, const StepParams &p,
@@ -59,12 +67,14 @@ int launch_rk1_mixed(const double *u, const double *v, const double *w, float *d
 int launch_rk2_mixed(const double *u, const double *v, const double *w, const float *d1u, const float *d1v,
                      const float *d1w, double *uo, double *vo, double *wo, const StepParams &p, const MeshDev &m,
                      MeanState &ms, cudaStream_t st);
-int launch_rhs_mixed(const double *u, const double *v, const double *w, const double *pprev, float *r,
-                     double *plane_part, double *mode0, const StepParams &p, const MeshDev &m, const double *za,
-                     const double *zbt, const double *zc, double dxi2, double dyi2, int incremental, cudaStream_t st);
-int launch_correct_mixed(const double *pprev, const float *dp, double *pnew, double *u, double *v, double *w,
-                         const StepParams &p, const MeshDev &m, int forced_x, const double *scalar, int incremental,
-                         cudaStream_t st);
+int launch_rhs_mixed(const double *u, const double *v, const double *w, const double *pn, const double *pnm1,
+                     float *r, double *warp_part, double *mode0, const StepParams &p, const MeshDev &m,
+                     const double *za, const double *zbt, const double *zc, double dxi2, double dyi2, int incremental,
+                     cudaStream_t st);
+int launch_correct_mixed(const double *pn, const double *pnm1, const float *dp, double *pnew, double *u, double *v,
+                         double *w, const StepParams &p, const MeshDev &m, int forced_x, const double *scalar,
+                         int incremental, cudaStream_t st);
+int warp_partials_per_plane(const StepParams &p);
 
 // diagnostics: out[0] = max|div| , out[1] = max CFL (already * dt), out[2] =
 // NaN count over u,v,w (ghosts included); loc[0..2] ijk of the div max,
