@@ -12,7 +12,8 @@
 //
 // The complex FFT is a Stockham autosort decimation-in-time transform over a
 // batch held in shared memory, ping-ponging between two buffers, with radix
-// 4, 2 and 3 passes.  Twiddles exp(-2 pi i t / n) come from a table computed on
+// 8, 6, 4, 3 and 2 passes (each thread keeps one butterfly in registers).
+// Twiddles exp(-2 pi i t / n) come from a table computed on
 // the host in long double.
 #pragma once
 
@@ -82,6 +83,66 @@ template <typename V, bool FWD> __device__ __forceinline__ void dft3(V &a0, V &a
     a2 = csub(t, u);
 }
 
+// 8-point DFT: two 4-point DFTs (even, odd samples) and the w8^k combination
+template <typename V, bool FWD> __device__ __forceinline__ void dft8(V *a)
+{
+    using T = decltype(a[0].x);
+    const T h = T(0.70710678118654752440084436210484904);
+    V e0 = a[0], e1 = a[2], e2 = a[4], e3 = a[6];
+    V o0 = a[1], o1 = a[3], o2 = a[5], o3 = a[7];
+    dft4<V, FWD>(e0, e1, e2, e3);
+    dft4<V, FWD>(o0, o1, o2, o3);
+    // w8^1 o1, w8^2 o2, w8^3 o3 with w8 = exp(-+ i pi/4)
+    V t1, t2, t3;
+    if (FWD) {
+        t1.x = h * (o1.x + o1.y);
+        t1.y = h * (o1.y - o1.x);
+        t2.x = o2.y;
+        t2.y = -o2.x;
+        t3.x = h * (o3.y - o3.x);
+        t3.y = -h * (o3.x + o3.y);
+    } else {
+        t1.x = h * (o1.x - o1.y);
+        t1.y = h * (o1.x + o1.y);
+        t2.x = -o2.y;
+        t2.y = o2.x;
+        t3.x = -h * (o3.x + o3.y);
+        t3.y = h * (o3.x - o3.y);
+    }
+    a[0] = cadd(e0, o0);
+    a[4] = csub(e0, o0);
+    a[1] = cadd(e1, t1);
+    a[5] = csub(e1, t1);
+    a[2] = cadd(e2, t2);
+    a[6] = csub(e2, t2);
+    a[3] = cadd(e3, t3);
+    a[7] = csub(e3, t3);
+}
+
+// 6-point DFT: two 3-point DFTs (even, odd samples) and the w6^k combination
+template <typename V, bool FWD> __device__ __forceinline__ void dft6(V *a)
+{
+    using T = decltype(a[0].x);
+    const T s3 = T(0.86602540378443864676372317075293618);
+    V e0 = a[0], e1 = a[2], e2 = a[4];
+    V o0 = a[1], o1 = a[3], o2 = a[5];
+    dft3<V, FWD>(e0, e1, e2);
+    dft3<V, FWD>(o0, o1, o2);
+    // w6 = exp(-+ i pi/3) = (1/2, -+ s3), w6^2 = (-1/2, -+ s3)
+    const T sg = FWD ? -s3 : s3;
+    V t1, t2;
+    t1.x = T(0.5) * o1.x - sg * o1.y;
+    t1.y = T(0.5) * o1.y + sg * o1.x;
+    t2.x = T(-0.5) * o2.x - sg * o2.y;
+    t2.y = T(-0.5) * o2.y + sg * o2.x;
+    a[0] = cadd(e0, o0);
+    a[3] = csub(e0, o0);
+    a[1] = cadd(e1, t1);
+    a[4] = csub(e1, t1);
+    a[2] = cadd(e2, t2);
+    a[5] = csub(e2, t2);
+}
+
 // One Stockham stage over a batch of `nb` sequences of length n.
 // Element (m, b) of a buffer lives at buf[m * sm + b * sb].
 // BATCH_FAST: consecutive threads take consecutive b (use when sb == 1).
@@ -105,7 +166,24 @@ __device__ __forceinline__ void fft_stage(const V *__restrict__ src, V *__restri
         V *d = dst + (size_t)b * sb;
         const int jm = j % Ns;
         const int idxD = (j / Ns) * Ns * R + jm;
-        if (R == 4) {
+        if (R == 8 || R == 6) {
+            V a[8];
+#pragma unroll
+            for (int r = 0; r < 8; r++)
+                if (r < R) a[r] = s[(j + r * nbf) * sm];
+            if (Ns > 1) {
+#pragma unroll
+                for (int r = 1; r < 8; r++)
+                    if (r < R) a[r] = cmul(a[r], twiddle<V, FWD>(tw, r * jm * tstep));
+            }
+            if (R == 8)
+                dft8<V, FWD>(a);
+            else
+                dft6<V, FWD>(a);
+#pragma unroll
+            for (int r = 0; r < 8; r++)
+                if (r < R) d[(idxD + r * Ns) * sm] = a[r];
+        } else if (R == 4) {
             V a0 = s[(j)*sm], a1 = s[(j + nbf) * sm], a2 = s[(j + 2 * nbf) * sm], a3 = s[(j + 3 * nbf) * sm];
             if (Ns > 1) {
                 a1 = cmul(a1, twiddle<V, FWD>(tw, jm * tstep));

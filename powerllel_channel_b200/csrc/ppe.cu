@@ -281,22 +281,36 @@ __global__ void k_widen(const float *__restrict__ in, double *__restrict__ out, 
 // Host plan
 // ------------------------------------------------------------------------
 
+// radix plan: 8s first, then one 4 or 2, then 3s (a leftover 2 merged with a
+// 3 into a 6): few stages, so few shared-memory round trips
 static int factor_radices(int n, int *radix, int *nstages)
 {
     int s = 0, m = n;
-    while (m % 4 == 0 && s < FFT_MAX_STAGES) {
+    while (m % 8 == 0 && s < FFT_MAX_STAGES) {
+        radix[s++] = 8;
+        m /= 8;
+    }
+    int two = 0;
+    if (m % 4 == 0) {
         radix[s++] = 4;
         m /= 4;
-    }
-    if (m % 2 == 0 && s < FFT_MAX_STAGES) {
-        radix[s++] = 2;
+    } else if (m % 2 == 0) {
+        two = 1;
         m /= 2;
     }
-    while (m % 3 == 0 && s < FFT_MAX_STAGES) {
-        radix[s++] = 3;
+    int threes = 0;
+    while (m % 3 == 0) {
+        threes++;
         m /= 3;
     }
     if (m != 1) return -1;
+    if (two && threes) {
+        radix[s++] = 6;
+        threes--;
+    } else if (two) {
+        radix[s++] = 2;
+    }
+    while (threes-- > 0 && s < FFT_MAX_STAGES) radix[s++] = 3;
     *nstages = s;
     return 0;
 }
