@@ -82,6 +82,7 @@ def lib():
                                 C.c_int, C.c_int]
     L.pl_ppe_solve.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
     L.pl_ppe_destroy.argtypes = [C.c_void_p]
+    L.pl_ppe_solve_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
     L.pl_channel_create.argtypes = [C.POINTER(C.c_void_p), C.POINTER(_Config)]
     L.pl_channel_destroy.argtypes = [C.c_void_p]
     L.pl_channel_init_flow.argtypes = [C.c_void_p, C.c_uint64, C.c_double]

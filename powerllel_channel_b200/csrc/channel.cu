@@ -131,10 +131,6 @@ extern "C" void free_poisson_solver(void)
 // ------------------------------------------------------------------------
 // 2. Device-resident PPE
 // ------------------------------------------------------------------------
-struct pl_ppe {
-    Ppe s;
-};
-
 extern "C" int pl_ppe_create(pl_ppe **out, int nx, int ny, int nz, double dx, double dy, const double *dzf_global,
                              int nparts, int precision)
 {

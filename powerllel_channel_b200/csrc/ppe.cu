@@ -14,6 +14,8 @@
 // (ix <= nx/2, jy <= ny/2): a quarter of the reference's b array.
 #include <cmath>
 #include <cstring>
+#include <mutex>
+#include <string>
 
 #include "ppe.cuh"
 #include "trid_tables.h"
@@ -561,3 +563,85 @@ int ppe_solve_fp32(Ppe *s, float *d_var, const double *mode0, cudaStream_t st)
 }
 
 } // namespace pl
+
+// ------------------------------------------------------------------------
+// Allocation-free solve (pl_ppe_solve_noalloc in include/powerllel_b200.h).
+//
+// Some callers cannot call cudaMalloc while they solve: a driver that records
+// its time loop into a CUDA graph (allocation is not permitted while a stream
+// is being captured), or a host program whose device memory is owned by
+// another allocator.  For them the mixed-precision Thomas solve takes its FP64
+// forward-sweep scratch from this fixed device array instead of the buffer
+// pl_ppe_create allocates.  The array is file-scope device memory: every GPU
+// that loads the library holds it (16 MiB) until the process exits.
+// ------------------------------------------------------------------------
+namespace pl {
+
+constexpr size_t NOALLOC_SCRATCH_DOUBLES = (size_t)1 << 21; // 16 MiB: nx*ny*nz <= 2,097,152
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_SCRATCH_DOUBLES];
+
+// device address of g_noalloc_scratch, looked up once per device: in host
+// code the symbol names a host-side stand-in, not device memory
+static std::mutex g_noalloc_mu;
+static double *g_noalloc_ptr[64] = {nullptr};
+
+static int noalloc_scratch(double **out)
+{
+    int dev = -1;
+    PL_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) {
+        set_error("pl_ppe_solve_noalloc: device ordinal out of range");
+        return -1;
+    }
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void *ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || ptr == nullptr) {
+            set_error(std::string("pl_ppe_solve_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
+            return -1;
+        }
+        g_noalloc_ptr[dev] = static_cast<double *>(ptr);
+    }
+    *out = g_noalloc_ptr[dev];
+    return 0;
+}
+
+static int ppe_solve_fp32_noalloc(Ppe *s, float *d_var, cudaStream_t st)
+{
+    if (s->prec != PREC_MIXED || s->nparts != 0) {
+        set_error("pl_ppe_solve_noalloc: the plan must be PL_MIXED with Thomas (nparts = 0)");
+        return -1;
+    }
+    const size_t n = (size_t)s->nx * s->ny * s->nz;
+    if (n > NOALLOC_SCRATCH_DOUBLES) {
+        set_error("pl_ppe_solve_noalloc: nx*ny*nz = " + std::to_string(n) + " exceeds the fixed scratch of " +
+                  std::to_string(NOALLOC_SCRATCH_DOUBLES) + " values; use pl_ppe_solve");
+        return -1;
+    }
+    double *xs = nullptr;
+    if (noalloc_scratch(&xs)) return -1;
+    const size_t nxl = s->nx, nxy = (size_t)s->nx * s->ny;
+    if (launch_x<float>(s, true, d_var, 0, nxl, nxy, d_var, 0, nxl, nxy, 1.0f, st)) return -1;
+    if (launch_y<float>(s, true, d_var, st)) return -1;
+    // every value of the scratch is written by the forward sweep before the
+    // backward sweep reads it, so nothing needs clearing between calls
+    TridDev t{s->nx, s->ny, s->nz, s->ncx, s->ncy, s->d_mult, s->d_rb, s->d_c};
+    dim3 grid((s->nx + 127) / 128, s->ny);
+    k_thomas<float><<<grid, 128, 0, st>>>(d_var, xs, d_var, t, nullptr);
+    PL_CHECK_LAUNCH();
+    if (launch_y<float>(s, false, d_var, st)) return -1;
+    if (launch_x<float>(s, false, d_var, 0, nxl, nxy, d_var, 0, nxl, nxy, (float)s->norm, st)) return -1;
+    return 0;
+}
+
+} // namespace pl
+
+extern "C" int pl_ppe_solve_noalloc(pl_ppe *p, void *d_var, void *stream)
+{
+    if (!p || !d_var) {
+        pl::set_error("pl_ppe_solve_noalloc: null argument");
+        return -1;
+    }
+    return pl::ppe_solve_fp32_noalloc(&p->s, (float *)d_var, (cudaStream_t)stream);
+}

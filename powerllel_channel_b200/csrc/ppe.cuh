@@ -68,3 +68,8 @@ int ppe_solve_fp64_strided(Ppe *s, const double *in, double *out, size_t off, si
                            double *d_work, cudaStream_t st);
 
 } // namespace pl
+
+// the C ABI's opaque PPE handle (include/powerllel_b200.h)
+struct pl_ppe {
+    pl::Ppe s;
+};
