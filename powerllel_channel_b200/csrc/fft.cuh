@@ -32,6 +32,15 @@ template <typename V> struct FftPlanDev {
     const V *tw; // exp(-2 pi i t / n), t < n
 };
 
+// Shared-memory index padding: one unused slot after every 128 bytes (8
+// double2 or 16 float2), so the strided writes of a Stockham stage (stride R
+// elements when Ns = 1) spread over all banks instead of a few.
+template <typename V> __host__ __device__ __forceinline__ int fpad(int i)
+{
+    return i + (i >> (sizeof(V) == 16 ? 3 : 4));
+}
+template <typename V> __host__ __device__ __forceinline__ int fpad_elems(int n) { return fpad<V>(n) + 1; }
+
 template <typename V, bool FWD>
 __device__ __forceinline__ V twiddle(const V *tw, int t)
 {
@@ -144,7 +153,7 @@ template <typename V, bool FWD> __device__ __forceinline__ void dft6(V *a)
 }
 
 // One Stockham stage over a batch of `nb` sequences of length n.
-// Element (m, b) of a buffer lives at buf[m * sm + b * sb].
+// Element (m, b) of a buffer lives at buf[fpad(m * sm + b * sb)].
 // BATCH_FAST: consecutive threads take consecutive b (use when sb == 1).
 template <typename V, bool FWD, bool BATCH_FAST>
 __device__ __forceinline__ void fft_stage(const V *__restrict__ src, V *__restrict__ dst, int n, int nb, int sm,
@@ -162,15 +171,14 @@ __device__ __forceinline__ void fft_stage(const V *__restrict__ src, V *__restri
             j = q % nbf;
             b = q / nbf;
         }
-        const V *s = src + (size_t)b * sb;
-        V *d = dst + (size_t)b * sb;
+        const int base = b * sb;
         const int jm = j % Ns;
         const int idxD = (j / Ns) * Ns * R + jm;
         if (R == 8 || R == 6) {
             V a[8];
 #pragma unroll
             for (int r = 0; r < 8; r++)
-                if (r < R) a[r] = s[(j + r * nbf) * sm];
+                if (r < R) a[r] = src[fpad<V>(base + (j + r * nbf) * sm)];
             if (Ns > 1) {
 #pragma unroll
                 for (int r = 1; r < 8; r++)
@@ -182,35 +190,35 @@ __device__ __forceinline__ void fft_stage(const V *__restrict__ src, V *__restri
                 dft6<V, FWD>(a);
 #pragma unroll
             for (int r = 0; r < 8; r++)
-                if (r < R) d[(idxD + r * Ns) * sm] = a[r];
+                if (r < R) dst[fpad<V>(base + (idxD + r * Ns) * sm)] = a[r];
         } else if (R == 4) {
-            V a0 = s[(j)*sm], a1 = s[(j + nbf) * sm], a2 = s[(j + 2 * nbf) * sm], a3 = s[(j + 3 * nbf) * sm];
+            V a0 = src[fpad<V>(base + j * sm)], a1 = src[fpad<V>(base + (j + nbf) * sm)], a2 = src[fpad<V>(base + (j + 2 * nbf) * sm)], a3 = src[fpad<V>(base + (j + 3 * nbf) * sm)];
             if (Ns > 1) {
                 a1 = cmul(a1, twiddle<V, FWD>(tw, jm * tstep));
                 a2 = cmul(a2, twiddle<V, FWD>(tw, 2 * jm * tstep));
                 a3 = cmul(a3, twiddle<V, FWD>(tw, 3 * jm * tstep));
             }
             dft4<V, FWD>(a0, a1, a2, a3);
-            d[(idxD)*sm] = a0;
-            d[(idxD + Ns) * sm] = a1;
-            d[(idxD + 2 * Ns) * sm] = a2;
-            d[(idxD + 3 * Ns) * sm] = a3;
+            dst[fpad<V>(base + idxD * sm)] = a0;
+            dst[fpad<V>(base + (idxD + Ns) * sm)] = a1;
+            dst[fpad<V>(base + (idxD + 2 * Ns) * sm)] = a2;
+            dst[fpad<V>(base + (idxD + 3 * Ns) * sm)] = a3;
         } else if (R == 2) {
-            V a0 = s[(j)*sm], a1 = s[(j + nbf) * sm];
+            V a0 = src[fpad<V>(base + j * sm)], a1 = src[fpad<V>(base + (j + nbf) * sm)];
             if (Ns > 1) a1 = cmul(a1, twiddle<V, FWD>(tw, jm * tstep));
             dft2<V, FWD>(a0, a1);
-            d[(idxD)*sm] = a0;
-            d[(idxD + Ns) * sm] = a1;
+            dst[fpad<V>(base + idxD * sm)] = a0;
+            dst[fpad<V>(base + (idxD + Ns) * sm)] = a1;
         } else { // R == 3
-            V a0 = s[(j)*sm], a1 = s[(j + nbf) * sm], a2 = s[(j + 2 * nbf) * sm];
+            V a0 = src[fpad<V>(base + j * sm)], a1 = src[fpad<V>(base + (j + nbf) * sm)], a2 = src[fpad<V>(base + (j + 2 * nbf) * sm)];
             if (Ns > 1) {
                 a1 = cmul(a1, twiddle<V, FWD>(tw, jm * tstep));
                 a2 = cmul(a2, twiddle<V, FWD>(tw, 2 * jm * tstep));
             }
             dft3<V, FWD>(a0, a1, a2);
-            d[(idxD)*sm] = a0;
-            d[(idxD + Ns) * sm] = a1;
-            d[(idxD + 2 * Ns) * sm] = a2;
+            dst[fpad<V>(base + idxD * sm)] = a0;
+            dst[fpad<V>(base + (idxD + Ns) * sm)] = a1;
+            dst[fpad<V>(base + (idxD + 2 * Ns) * sm)] = a2;
         }
     }
 }

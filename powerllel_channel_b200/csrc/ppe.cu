@@ -38,7 +38,7 @@ __global__ void __launch_bounds__(256) k_xfft(const T *__restrict__ in, size_t i
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int n = plan.n; // = nx
     V *buf0 = reinterpret_cast<V *>(smem_raw);
-    V *buf1 = buf0 + (size_t)pb * n;
+    V *buf1 = buf0 + fpad_elems<V>(pb * n);
     const int k = blockIdx.y;
     const int p0 = blockIdx.x * pb;
     const int nb = min(pb, ny / 2 - p0);
@@ -48,14 +48,14 @@ __global__ void __launch_bounds__(256) k_xfft(const T *__restrict__ in, size_t i
         const int m = e % n, r = (e / n) & 1, b = e / (2 * n);
         const int j = 2 * (p0 + b) + r;
         T val = in[in_off + (size_t)m + (size_t)j * in_sj + (size_t)k * in_sk];
-        reinterpret_cast<T *>(&buf0[(size_t)b * n + m])[r] = val;
+        reinterpret_cast<T *>(&buf0[fpad<V>(b * n + m)])[r] = val;
     }
     __syncthreads();
     if (FWD) {
         V *res = fft_batch<V, true, false>(buf0, buf1, plan, nb, 1, n, tid, nthr);
         for (int e = tid; e < nb * n; e += nthr) {
             const int m = e % n, b = e / n;
-            V A = res[(size_t)b * n + m], Bc = res[(size_t)b * n + (m == 0 ? 0 : n - m)];
+            V A = res[fpad<V>(b * n + m)], Bc = res[fpad<V>(b * n + (m == 0 ? 0 : n - m))];
             V h = split_hc(A, Bc, m, n);
             const int j = 2 * (p0 + b);
             out[out_off + (size_t)m + (size_t)j * out_sj + (size_t)k * out_sk] = h.x;
@@ -64,14 +64,14 @@ __global__ void __launch_bounds__(256) k_xfft(const T *__restrict__ in, size_t i
     } else {
         for (int e = tid; e < nb * n; e += nthr) {
             const int m = e % n, b = e / n;
-            V P = buf0[(size_t)b * n + m], Q = buf0[(size_t)b * n + (m == 0 ? 0 : n - m)];
-            buf1[(size_t)b * n + m] = merge_hc(P, Q, m, n);
+            V P = buf0[fpad<V>(b * n + m)], Q = buf0[fpad<V>(b * n + (m == 0 ? 0 : n - m))];
+            buf1[fpad<V>(b * n + m)] = merge_hc(P, Q, m, n);
         }
         __syncthreads();
         V *res = fft_batch<V, false, false>(buf1, buf0, plan, nb, 1, n, tid, nthr);
         for (int e = tid; e < nb * n; e += nthr) {
             const int m = e % n, b = e / n;
-            V z = res[(size_t)b * n + m];
+            V z = res[fpad<V>(b * n + m)];
             const int j = 2 * (p0 + b);
             out[out_off + (size_t)m + (size_t)j * out_sj + (size_t)k * out_sk] = z.x * scale;
             out[out_off + (size_t)m + (size_t)(j + 1) * out_sj + (size_t)k * out_sk] = z.y * scale;
@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(256) k_yfft(T *__restrict__ data, FftPlanDev<t
     const int n = plan.n; // = ny
     const int ncol = nx / 2;
     V *buf0 = reinterpret_cast<V *>(smem_raw);
-    V *buf1 = buf0 + (size_t)w * n;
+    V *buf1 = buf0 + fpad_elems<V>(w * n);
     const int k = blockIdx.y;
     const int c0 = blockIdx.x * w;
     const int nb = min(w, ncol - c0);
@@ -100,27 +100,27 @@ __global__ void __launch_bounds__(256) k_yfft(T *__restrict__ data, FftPlanDev<t
 
     for (int e = tid; e < nb * n; e += nthr) {
         const int c = e % nb, m = e / nb;
-        buf0[(size_t)m * w + c] = plane[(size_t)m * ncol + c0 + c];
+        buf0[fpad<V>(m * w + c)] = plane[(size_t)m * ncol + c0 + c];
     }
     __syncthreads();
     if (FWD) {
         V *res = fft_batch<V, true, true>(buf0, buf1, plan, nb, w, 1, tid, nthr);
         for (int e = tid; e < nb * n; e += nthr) {
             const int c = e % nb, m = e / nb;
-            V A = res[(size_t)m * w + c], Bc = res[(size_t)(m == 0 ? 0 : n - m) * w + c];
+            V A = res[fpad<V>(m * w + c)], Bc = res[fpad<V>((m == 0 ? 0 : n - m) * w + c)];
             plane[(size_t)m * ncol + c0 + c] = split_hc(A, Bc, m, n);
         }
     } else {
         for (int e = tid; e < nb * n; e += nthr) {
             const int c = e % nb, m = e / nb;
-            V P = buf0[(size_t)m * w + c], Q = buf0[(size_t)(m == 0 ? 0 : n - m) * w + c];
-            buf1[(size_t)m * w + c] = merge_hc(P, Q, m, n);
+            V P = buf0[fpad<V>(m * w + c)], Q = buf0[fpad<V>((m == 0 ? 0 : n - m) * w + c)];
+            buf1[fpad<V>(m * w + c)] = merge_hc(P, Q, m, n);
         }
         __syncthreads();
         V *res = fft_batch<V, false, true>(buf1, buf0, plan, nb, w, 1, tid, nthr);
         for (int e = tid; e < nb * n; e += nthr) {
             const int c = e % nb, m = e / nb;
-            plane[(size_t)m * ncol + c0 + c] = res[(size_t)m * w + c];
+            plane[(size_t)m * ncol + c0 + c] = res[fpad<V>(m * w + c)];
         }
     }
 }
@@ -460,7 +460,7 @@ static int launch_x(const Ppe *s, bool fwd, const T *in, size_t in_off, size_t i
     using V = typename cplx_of<T>::type;
     const int pb = x_pairs_per_cta(s->nx, s->ny);
     dim3 grid((s->ny / 2 + pb - 1) / pb, s->nz);
-    const size_t shm = 2 * sizeof(V) * (size_t)pb * s->nx;
+    const size_t shm = 2 * sizeof(V) * (size_t)fpad_elems<V>(pb * s->nx);
     const FftPlanDev<V> &plan = *reinterpret_cast<const FftPlanDev<V> *>(
         sizeof(T) == 8 ? (const void *)&s->px64 : (const void *)&s->px32);
     if (fwd)
@@ -478,7 +478,7 @@ template <typename T> static int launch_y(const Ppe *s, bool fwd, T *data, cudaS
     using V = typename cplx_of<T>::type;
     const int w = y_cols_per_cta(s->nx, s->ny);
     dim3 grid((s->nx / 2 + w - 1) / w, s->nz);
-    const size_t shm = 2 * sizeof(V) * (size_t)w * s->ny;
+    const size_t shm = 2 * sizeof(V) * (size_t)fpad_elems<V>(w * s->ny);
     const FftPlanDev<V> &plan = *reinterpret_cast<const FftPlanDev<V> *>(
         sizeof(T) == 8 ? (const void *)&s->py64 : (const void *)&s->py32);
     if (fwd)

@@ -10,10 +10,10 @@
 // kernels.
 //
 // FP64 path: the rings hold u and u1 in double, the expressions are the
-// reference's.  Mixed path: the rings hold u in float and the stage-1
-// increment d1 = dt*RHS(u) in float (u1 = u + d1 for the stencils, FP32
-// arithmetic); the update u_new = (u1 + dt*RHS(u1) + u)/2 uses the FP64 u of
-// the centre and is stored in FP64.
+// reference's.  Mixed path: the rings hold u, the stage-1 increment
+// d1 = dt*RHS(u) and u1 = u + d1, all in float (FP32 stencil arithmetic); the
+// update u_new = ((u + d1) + dt*RHS(u1) + u)/2 uses the FP64 u of the centre
+// and is stored in FP64.
 #include "stencil.cuh"
 #include "stencil_rhs.cuh"
 
@@ -30,31 +30,25 @@ template <> struct RkTraits<false> {
 };
 template <> struct RkTraits<true> {
     using R = float;
-    static constexpr int NS = 4;
+    static constexpr int NS = 3;
 };
 
 template <typename R> struct RingLoad {
     const R *a;
-    __device__ __forceinline__ R operator()(size_t q) const { return a[q]; }
+    __device__ __forceinline__ R operator()(int q) const { return a[q]; }
 };
 
-// mixed path: u1 = u + d1 on the ring
-struct RingSum {
-    const float *a, *d;
-    __device__ __forceinline__ float operator()(size_t q) const { return a[q] + d[q]; }
-};
-
-__device__ __forceinline__ Nb ring_nb(int x, int y, int s0, int sm, int sp)
+__device__ __forceinline__ Nb32 ring_nb(int x, int y, int s0, int sm, int sp)
 {
-    Nb n;
-    const size_t xy = (size_t)y * UW + x;
-    n.c = (size_t)s0 * UPS + xy;
+    Nb32 n;
+    const int xy = y * UW + x;
+    n.c = s0 * UPS + xy;
     n.xm = n.c - 1;
     n.xp = n.c + 1;
     n.ym = n.c - UW;
     n.yp = n.c + UW;
-    n.zm = (size_t)sm * UPS + xy;
-    n.zp = (size_t)sp * UPS + xy;
+    n.zm = sm * UPS + xy;
+    n.zp = sp * UPS + xy;
     n.xpym = n.c + 1 - UW;
     n.xmyp = n.c - 1 + UW;
     n.xpzm = n.zm + 1;
@@ -76,6 +70,7 @@ __global__ void __launch_bounds__(FX *FY) k_rk_fused(const double *__restrict__ 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R *ur = reinterpret_cast<R *>(smem_raw); // u, v, w rings
     R *qr = ur + 3 * FS;                     // u1 (FP64) or d1 (mixed) rings
+    R *sr = qr + 3 * FS;                     // mixed: u1 = u + d1 in FP32 (the stage-2 stencil input)
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + ty * FX, nthr = FX * FY;
     const int i0 = blockIdx.x * FX, j0 = blockIdx.y * FY;
     const int kbeg = blockIdx.z * kchunk + 1, kend = min(kbeg + kchunk - 1, p.nz);
@@ -104,14 +99,18 @@ __global__ void __launch_bounds__(FX *FY) k_rk_fused(const double *__restrict__ 
         const int s0 = mq % NS, sm = (mq - 1) % NS, sp = (mq + 1) % NS;
         for (int q = tid; q < (FX + 2) * (FY + 2); q += nthr) {
             const int x = q % (FX + 2) + 1, y = q / (FX + 2) + 1;
-            const Nb n = ring_nb(x, y, s0, sm, sp);
+            const Nb32 n = ring_nb(x, y, s0, sm, sp);
             R ru, rv, rw;
             momentum_rhs<R>(RingLoad<R>{ur}, RingLoad<R>{ur + FS}, RingLoad<R>{ur + 2 * FS}, n, mq, p, m, ru, rv,
                             rw);
-            if (MIXED) { // increments
-                qr[n.c] = dt * ru;
-                qr[FS + n.c] = dt * rv;
-                qr[2 * FS + n.c] = (mq == p.nz) ? (R)0 : dt * rw; // w1(nz) = 0 = w(nz)
+            if (MIXED) { // increments, and u1 = u + d1 for the stage-2 stencils
+                const R du = dt * ru, dv = dt * rv, dw = (mq == p.nz) ? (R)0 : dt * rw; // w1(nz) = 0 = w(nz)
+                qr[n.c] = du;
+                qr[FS + n.c] = dv;
+                qr[2 * FS + n.c] = dw;
+                sr[n.c] = ur[n.c] + du;
+                sr[FS + n.c] = ur[FS + n.c] + dv;
+                sr[2 * FS + n.c] = ur[2 * FS + n.c] + dw;
             } else {      // u1 = u + dt*(visc - conv)
                 qr[n.c] = ur[n.c] + dt * ru;
                 qr[FS + n.c] = ur[FS + n.c] + dt * rv;
@@ -125,15 +124,20 @@ __global__ void __launch_bounds__(FX *FY) k_rk_fused(const double *__restrict__ 
         const int sg = kg % NS, si = ki % NS;
         for (int q = tid; q < (FX + 2) * (FY + 2); q += nthr) {
             const int x = q % (FX + 2) + 1, y = q / (FX + 2) + 1;
-            const size_t xy = (size_t)y * UW + x;
+            const int xy = y * UW + x;
             if (MIXED) { // u1(g) = 2bc - u1(i) and u(g) = 2bc - u(i)  =>  d1(g) = -d1(i)
-                qr[sg * UPS + xy] = -qr[si * UPS + xy];
-                qr[FS + sg * UPS + xy] = -qr[FS + si * UPS + xy];
+                const R du = -qr[si * UPS + xy], dv = -qr[FS + si * UPS + xy];
+                qr[sg * UPS + xy] = du;
+                qr[FS + sg * UPS + xy] = dv;
+                qr[2 * FS + sg * UPS + xy] = (R)0;
+                sr[sg * UPS + xy] = ur[sg * UPS + xy] + du;
+                sr[FS + sg * UPS + xy] = ur[FS + sg * UPS + xy] + dv;
+                sr[2 * FS + sg * UPS + xy] = ur[2 * FS + sg * UPS + xy];
             } else {
                 qr[sg * UPS + xy] = (R)2 * bcu - qr[si * UPS + xy];
                 qr[FS + sg * UPS + xy] = -qr[FS + si * UPS + xy];
+                qr[2 * FS + sg * UPS + xy] = (R)0;
             }
-            qr[2 * FS + sg * UPS + xy] = (R)0;
         }
     };
 
@@ -141,12 +145,10 @@ __global__ void __launch_bounds__(FX *FY) k_rk_fused(const double *__restrict__ 
     // stage 2 at interior plane kq from the stage-1 planes kq-1, kq, kq+1
     auto stage2 = [&](int kq) {
         const int s0 = kq % NS, sm = (kq - 1) % NS, sp = (kq + 1) % NS;
-        const Nb n = ring_nb(tx + 2, ty + 2, s0, sm, sp);
+        const Nb32 n = ring_nb(tx + 2, ty + 2, s0, sm, sp);
         R ru, rv, rw;
         if (MIXED)
-            momentum_rhs<R>(RingSum{(const float *)ur, (const float *)qr},
-                            RingSum{(const float *)ur + FS, (const float *)qr + FS},
-                            RingSum{(const float *)ur + 2 * FS, (const float *)qr + 2 * FS}, n, kq, p, m, ru, rv, rw);
+            momentum_rhs<R>(RingLoad<R>{sr}, RingLoad<R>{sr + FS}, RingLoad<R>{sr + 2 * FS}, n, kq, p, m, ru, rv, rw);
         else
             momentum_rhs<R>(RingLoad<R>{qr}, RingLoad<R>{qr + FS}, RingLoad<R>{qr + 2 * FS}, n, kq, p, m, ru, rv,
                             rw);
@@ -225,10 +227,13 @@ static int launch_rk_fused_t(const double *u, const double *v, const double *w, 
         return -1;
     }
     using R = typename RkTraits<MIXED>::R;
-    const size_t shm = sizeof(R) * 6 * RkTraits<MIXED>::NS * UPS;
+    const size_t shm = sizeof(R) * (MIXED ? 9 : 6) * RkTraits<MIXED>::NS * UPS;
     static bool attr_set = false;
     if (!attr_set) {
         PL_CUDA_TRY(cudaFuncSetAttribute(k_rk_fused<MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        // prefer the largest shared-memory carve-out: several CTAs per SM
+        PL_CUDA_TRY(cudaFuncSetAttribute(k_rk_fused<MIXED>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                         (int)cudaSharedmemCarveoutMaxShared));
         attr_set = true;
     }
     MeanRed r{ms.partial, ms.counter, ms.scalar, (double)p.nx, (double)p.ny, ms.vel_force};

@@ -57,8 +57,13 @@ struct LoadSum {
     }
 };
 
-template <typename TC, typename AU, typename AV, typename AW>
-__device__ __forceinline__ void momentum_rhs(const AU &u, const AV &v, const AW &w, const Nb &n, int k,
+// shared-memory ring offsets fit in 32 bits
+struct Nb32 {
+    int c, xm, xp, ym, yp, zm, zp, xpym, xmyp, xpzm, xmzp, ypzm, ymzp;
+};
+
+template <typename TC, typename AU, typename AV, typename AW, typename NB = Nb>
+__device__ __forceinline__ void momentum_rhs(const AU &u, const AV &v, const AW &w, const NB &n, int k,
                                              const StepParams &p, const MeshDev &m, TC &ru, TC &rv, TC &rw)
 {
     const TC dx_inv = (TC)p.dx_inv, dy_inv = (TC)p.dy_inv, re_inv = (TC)p.re_inv, u_crf = (TC)p.u_crf;
