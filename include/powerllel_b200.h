@@ -167,6 +167,30 @@ int pl_phase_correct_force(pl_channel *c); /* updateBoundP, correctVel, forceVel
  * name to names (nslots*32 bytes, NUL-padded).  Returns the slot count, or -1. */
 int pl_channel_profile(pl_channel *c, int nsteps, double *ms, char *names, int max_slots);
 
+
+/* ======================================================================
+ * 5. Discrete adjoint (FP64 path, Thomas PPE).  No counterpart in the
+ *    reference: the reference has neither a body force nor an adjoint.
+ * ====================================================================== */
+/* Uniform body force f added to the momentum right-hand side of both RK
+ * stages: u1 = u + dt (RHS(u) + f), u = (u1 + dt (RHS(u1) + f) + u) / 2.
+ * Zero by default (the reference's step).  FP64 path only; forceVel stays on. */
+int pl_channel_set_body_force(pl_channel *c, const double f[3]);
+/* J = 1/2 dx dy [ sum_{k=1..nz} dzf_k sum_ij (u^2 + v^2) + sum_{k=1..nz-1} dzc_k sum_ij w^2 ]
+ * of the current fields (kinetic energy over the staggered cells). */
+int pl_channel_kinetic_energy(pl_channel *c, double *ke);
+/* Gradient of J after nsteps steps from the current fields x0, by the
+ * hand-written discrete adjoint with a checkpoint every `every` steps
+ * (segments recomputed forward).  Writes J(x_nsteps) to *ke, dJ/du0, dJ/dv0,
+ * dJ/dw0 to the device arrays d_gu, d_gv, d_gw (device layout nx*ny*(nz+2),
+ * wall planes and w's level nz zero) and dJ/df to grad_f (host).  The
+ * gradient is with respect to the degrees of freedom: u, v on levels 1..nz,
+ * w on levels 1..nz-1.  On return u, v, w hold x0 again; p and the stage-1
+ * fields are overwritten.  Device memory: (ceil(nsteps/every) + every + 9)
+ * fields.  Errors: mixed precision, PDD (trid_parts > 1), nsteps < 0, every < 1. */
+int pl_adjoint_ke_gradient(pl_channel *c, int nsteps, int every, double *ke, double *d_gu, double *d_gv,
+                           double *d_gw, double grad_f[3]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -99,6 +99,9 @@ def lib():
     L.pl_channel_stream.argtypes = [C.c_void_p]
     L.pl_channel_stream.restype = C.c_void_p
     L.pl_channel_profile.argtypes = [C.c_void_p, C.c_int, _dp, C.c_char_p, C.c_int]
+    L.pl_channel_set_body_force.argtypes = [C.c_void_p, _dp]
+    L.pl_channel_kinetic_energy.argtypes = [C.c_void_p, _dp]
+    L.pl_adjoint_ke_gradient.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp, C.c_void_p, C.c_void_p, C.c_void_p, _dp]
     for name in ("pl_phase_rk", "pl_phase_rk1", "pl_phase_rk2", "pl_phase_calc_rhs", "pl_phase_poisson", "pl_phase_correct_force"):
         getattr(L, name).argtypes = [C.c_void_p]
     _lib = L
@@ -293,6 +296,27 @@ class Channel:
 
     def download_compact(self, host_ptr: int) -> None:
         _check(lib().pl_channel_download_compact(self._h, C.c_void_p(host_ptr)), "pl_channel_download_compact")
+
+    def set_body_force(self, f) -> None:
+        """Uniform body force added to both RK stages (FP64 path)."""
+        fa = np.ascontiguousarray(f, dtype=np.float64)
+        _check(lib().pl_channel_set_body_force(self._h, _ptr(fa)), "pl_channel_set_body_force")
+
+    def kinetic_energy(self) -> float:
+        ke = np.zeros(1)
+        _check(lib().pl_channel_kinetic_energy(self._h, _ptr(ke)), "pl_channel_kinetic_energy")
+        return float(ke[0])
+
+    def adjoint_ke_gradient(self, nsteps: int, every: int, d_gu: int, d_gv: int, d_gw: int):
+        """Gradient of the kinetic energy after nsteps steps (hand-written
+        adjoint, checkpoint every `every` steps) w.r.t. the current fields and
+        the body force. d_g*: device pointers of nx*ny*(nz+2) doubles.
+        Returns (J, dJ/df)."""
+        ke = np.zeros(1)
+        gf = np.zeros(3)
+        _check(lib().pl_adjoint_ke_gradient(self._h, int(nsteps), int(every), _ptr(ke), C.c_void_p(d_gu),
+                                            C.c_void_p(d_gv), C.c_void_p(d_gw), _ptr(gf)), "pl_adjoint_ke_gradient")
+        return float(ke[0]), gf
 
     def field_ptr(self, which: int) -> int:
         return lib().pl_channel_field(self._h, which)

@@ -1,0 +1,46 @@
+// channel.cuh -- the device-resident channel object behind the pl_channel_*
+// entry points, shared by the step (channel.cu) and its adjoint (adjoint.cu).
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "../../include/powerllel_b200.h"
+#include "ppe.cuh"
+#include "stencil.cuh"
+
+struct pl_channel {
+    pl_channel_config cfg{};
+    int nx = 0, ny = 0, nz = 0;
+    size_t nf = 0;  // elements of a velocity-like field, nx*ny*(nz+2)
+    size_t np = 0;  // elements of p, nx*ny*nz
+    pl::StepParams sp{};
+    std::vector<double> dzf_global, zc_global, dzf, dzf_inv, dzc, dzc_inv, dzflzi, prof;
+    double *d_mesh = nullptr;
+    pl::MeshDev m{};
+    // FP64 path: u,v,w = ua,va,wa; stage-1 fields u1,v1,w1; p
+    // mixed path: u,v,w ping-pong between (ua,va,wa) and (ub,vb,wb); stage-1
+    // increments d1u,d1v,d1w (FP32); p ping-pong between p and pb (FP64); the
+    // PPE works in place on r32 (FP32)
+    double *u = nullptr, *v = nullptr, *w = nullptr;
+    double *u1 = nullptr, *v1 = nullptr, *w1 = nullptr;
+    double *p = nullptr;
+    double *ub = nullptr, *vb = nullptr, *wb = nullptr, *pb = nullptr, *pm = nullptr;
+    float *d1u = nullptr, *d1v = nullptr, *d1w = nullptr, *r32 = nullptr;
+    double *plane_part = nullptr, *mode0 = nullptr;
+    int incremental = 1;   // mixed path: solve for a pressure increment (Thomas)
+    long long nsolve = 0;  // projections since the initial field (mixed prediction schedule)
+    bool fused_rk = false; // both RK stages in one kernel (rk_fused.cu)
+    pl::Ppe ppe;
+    pl::ReduceBuf rb;
+    pl::MeanState ms;
+    double *d_diag = nullptr;
+    int *d_loc = nullptr;
+    double *d_dpart = nullptr;
+    long long *d_dipart = nullptr;
+    int max_blocks = 0;
+    cudaStream_t stream = nullptr;
+    // profiling marks (pl_channel_profile)
+    std::vector<cudaEvent_t> *prof_events = nullptr;
+    std::vector<std::string> *prof_names = nullptr;
+};

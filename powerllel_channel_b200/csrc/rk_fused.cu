@@ -112,9 +112,9 @@ __global__ void __launch_bounds__(FX *FY) k_rk_fused(const double *__restrict__ 
                 sr[FS + n.c] = ur[FS + n.c] + dv;
                 sr[2 * FS + n.c] = ur[2 * FS + n.c] + dw;
             } else {      // u1 = u + dt*(visc - conv)
-                qr[n.c] = ur[n.c] + dt * ru;
-                qr[FS + n.c] = ur[FS + n.c] + dt * rv;
-                qr[2 * FS + n.c] = (mq == p.nz) ? (R)0 : ur[2 * FS + n.c] + dt * rw;
+                qr[n.c] = ur[n.c] + dt * (ru + (R)p.fb[0]);
+                qr[FS + n.c] = ur[FS + n.c] + dt * (rv + (R)p.fb[1]);
+                qr[2 * FS + n.c] = (mq == p.nz) ? (R)0 : ur[2 * FS + n.c] + dt * (rw + (R)p.fb[2]);
             }
         }
     };
@@ -160,9 +160,9 @@ __global__ void __launch_bounds__(FX *FY) k_rk_fused(const double *__restrict__ 
             nv = ((vc + (double)qr[FS + n.c]) + (double)(dt * rv) + vc) * 0.5;
             nw = ((wc + (double)qr[2 * FS + n.c]) + (double)(dt * rw) + wc) * 0.5;
         } else {
-            nu = ((double)qr[n.c] + p.dt * (double)ru + uc) * 0.5;
-            nv = ((double)qr[FS + n.c] + p.dt * (double)rv + vc) * 0.5;
-            nw = ((double)qr[2 * FS + n.c] + p.dt * (double)rw + wc) * 0.5;
+            nu = ((double)qr[n.c] + p.dt * ((double)ru + p.fb[0]) + uc) * 0.5;
+            nv = ((double)qr[FS + n.c] + p.dt * ((double)rv + p.fb[1]) + vc) * 0.5;
+            nw = ((double)qr[2 * FS + n.c] + p.dt * ((double)rw + p.fb[2]) + wc) * 0.5;
         }
         uo[g] = nu;
         vo[g] = nv;

@@ -30,11 +30,11 @@ __global__ void __launch_bounds__(256) k_rk1_fp64(const double *__restrict__ u, 
     double ru, rv, rw;
     momentum_rhs<double>(LoadF<double, double>{u}, LoadF<double, double>{v}, LoadF<double, double>{w}, n, k, p, m,
                          ru, rv, rw);
-    const double nu = __ldg(u + n.c) + p.dt * ru;
-    const double nv = __ldg(v + n.c) + p.dt * rv;
+    const double nu = __ldg(u + n.c) + p.dt * (ru + p.fb[0]);
+    const double nv = __ldg(v + n.c) + p.dt * (rv + p.fb[1]);
     u1[n.c] = nu;
     v1[n.c] = nv;
-    if (k != p.nz) w1[n.c] = __ldg(w + n.c) + p.dt * rw;
+    if (k != p.nz) w1[n.c] = __ldg(w + n.c) + p.dt * (rw + p.fb[2]);
     wall_fill<double>(u1, v1, w1, n.c, k, sk, p.nz, 0.0 - p.u_crf, nu, nv);
 }
 
@@ -49,11 +49,11 @@ __global__ void __launch_bounds__(256) k_rk2_fp64(double *u, double *v, double *
     double ru, rv, rw;
     momentum_rhs<double>(LoadF<double, double>{u1}, LoadF<double, double>{v1}, LoadF<double, double>{w1}, n, k, p,
                          m, ru, rv, rw);
-    const double nu = (__ldg(u1 + n.c) + p.dt * ru + u[n.c]) * 0.5;
-    const double nv = (__ldg(v1 + n.c) + p.dt * rv + v[n.c]) * 0.5;
+    const double nu = (__ldg(u1 + n.c) + p.dt * (ru + p.fb[0]) + u[n.c]) * 0.5;
+    const double nv = (__ldg(v1 + n.c) + p.dt * (rv + p.fb[1]) + v[n.c]) * 0.5;
     u[n.c] = nu;
     v[n.c] = nv;
-    if (k != p.nz) w[n.c] = (__ldg(w1 + n.c) + p.dt * rw + w[n.c]) * 0.5;
+    if (k != p.nz) w[n.c] = (__ldg(w1 + n.c) + p.dt * (rw + p.fb[2]) + w[n.c]) * 0.5;
     wall_fill<double>(u, v, w, n.c, k, sk, p.nz, 0.0 - p.u_crf, nu, nv);
 }
 
@@ -357,11 +357,11 @@ __global__ void __launch_bounds__(256) k_rk2m_fp64(double *u, double *v, double 
         double ru, rv, rw;
         momentum_rhs<double>(LoadF<double, double>{u1}, LoadF<double, double>{v1}, LoadF<double, double>{w1}, n, k,
                              p, m, ru, rv, rw);
-        const double nu = (__ldg(u1 + n.c) + p.dt * ru + u[n.c]) * 0.5;
-        const double nv = (__ldg(v1 + n.c) + p.dt * rv + v[n.c]) * 0.5;
+        const double nu = (__ldg(u1 + n.c) + p.dt * (ru + p.fb[0]) + u[n.c]) * 0.5;
+        const double nv = (__ldg(v1 + n.c) + p.dt * (rv + p.fb[1]) + v[n.c]) * 0.5;
         u[n.c] = nu;
         v[n.c] = nv;
-        if (k != p.nz) w[n.c] = (__ldg(w1 + n.c) + p.dt * rw + w[n.c]) * 0.5;
+        if (k != p.nz) w[n.c] = (__ldg(w1 + n.c) + p.dt * (rw + p.fb[2]) + w[n.c]) * 0.5;
         wall_fill<double>(u, v, w, n.c, k, sk, p.nz, 0.0 - p.u_crf, nu, nv);
         su = nu * __ldg(m.dzflzi + k);
     }

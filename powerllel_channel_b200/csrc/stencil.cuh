@@ -14,6 +14,7 @@ struct MeshDev {
 struct StepParams {
     int nx, ny, nz;
     double dx_inv, dy_inv, re_inv, dt, u_crf;
+    double fb[3]; // uniform body force added to both RK stages (FP64 path; zero in the reference's step)
 };
 
 // Reduction scratch: per-block partial results and the final scalars.
