@@ -35,11 +35,11 @@ template <typename V> struct FftPlanDev {
 // Shared-memory index padding: one unused slot after every 128 bytes (8
 // double2 or 16 float2), so the strided writes of a Stockham stage (stride R
 // elements when Ns = 1) spread over all banks instead of a few.
-template <typename V> __host__ __device__ __forceinline__ int fpad(int i)
+template <typename V> __host__ __device__ constexpr int fpad(int i)
 {
     return i + (i >> (sizeof(V) == 16 ? 3 : 4));
 }
-template <typename V> __host__ __device__ __forceinline__ int fpad_elems(int n) { return fpad<V>(n) + 1; }
+template <typename V> __host__ __device__ constexpr int fpad_elems(int n) { return fpad<V>(n) + 1; }
 
 template <typename V, bool FWD>
 __device__ __forceinline__ V twiddle(const V *tw, int t)
@@ -240,6 +240,127 @@ __device__ V *fft_batch(V *buf0, V *buf1, const FftPlanDev<V> &p, int nb, int sm
         dst = t;
     }
     return src;
+}
+
+// ---------------------------------------------------------------------------
+// Compile-time sizes.  For the common line lengths the transform length, the
+// radix sequence, the batch geometry and every index divisor are template
+// constants, so a stage costs its butterfly arithmetic plus two shared-memory
+// accesses per element; twiddles are read from a shared-memory copy of the
+// table.  The radix sequence and the operations are those of the runtime
+// engine above, so both give bitwise identical results.
+// ---------------------------------------------------------------------------
+
+// radix of stage s for length n (0 past the last stage): 8s first, then 4, or
+// a 2 merged with one 3 into a 6, then 3s (the host's factor_radices order)
+__host__ __device__ constexpr int ct_radix(int n, int s)
+{
+    int m = n, idx = 0;
+    while (m % 8 == 0) {
+        if (idx == s) return 8;
+        idx++;
+        m /= 8;
+    }
+    int two = 0;
+    if (m % 4 == 0) {
+        if (idx == s) return 4;
+        idx++;
+        m /= 4;
+    } else if (m % 2 == 0) {
+        two = 1;
+        m /= 2;
+    }
+    int threes = 0;
+    while (m % 3 == 0) {
+        threes++;
+        m /= 3;
+    }
+    if (two && threes) {
+        if (idx == s) return 6;
+        idx++;
+        threes--;
+    } else if (two) {
+        if (idx == s) return 2;
+        idx++;
+    }
+    while (threes-- > 0) {
+        if (idx == s) return 3;
+        idx++;
+    }
+    return 0;
+}
+
+// product of the radices of the stages before s (Stockham's Ns)
+__host__ __device__ constexpr int ct_ns(int n, int s)
+{
+    int p = 1;
+    for (int q = 0; q < s; q++) p *= ct_radix(n, q);
+    return p;
+}
+
+template <typename V, bool FWD, int R> __device__ __forceinline__ void dft_r(V *a)
+{
+    if constexpr (R == 8)
+        dft8<V, FWD>(a);
+    else if constexpr (R == 6)
+        dft6<V, FWD>(a);
+    else if constexpr (R == 4)
+        dft4<V, FWD>(a[0], a[1], a[2], a[3]);
+    else if constexpr (R == 3)
+        dft3<V, FWD>(a[0], a[1], a[2]);
+    else
+        dft2<V, FWD>(a[0], a[1]);
+}
+
+// One stage over NB sequences (nb <= NB present) of length N; element (m, b)
+// at buf[fpad(m * SM + b * SB)]; BF: consecutive threads take consecutive b.
+template <typename V, bool FWD, bool BF, int N, int R, int NS, int NB, int SM, int SB, int NTHR>
+__device__ __forceinline__ void ct_stage(const V *__restrict__ src, V *__restrict__ dst, int nb,
+                                         const V *__restrict__ tw, int tid)
+{
+    constexpr int NBF = N / R, TSTEP = N / (NS * R), TOTAL = NBF * NB;
+    constexpr int ITERS = (TOTAL + NTHR - 1) / NTHR;
+#pragma unroll
+    for (int it = 0; it < ITERS; it++) {
+        const int q = tid + it * NTHR;
+        if (TOTAL % NTHR == 0 || q < TOTAL) {
+            const int b = BF ? q % NB : q / NBF;
+            const int j = BF ? q / NB : q % NBF;
+            if (b < nb) {
+                const int jm = j % NS;
+                const int idxD = (j / NS) * NS * R + jm;
+                const int base = b * SB;
+                V a[R];
+#pragma unroll
+                for (int r = 0; r < R; r++) a[r] = src[fpad<V>(base + (j + r * NBF) * SM)];
+                if (NS > 1) {
+#pragma unroll
+                    for (int r = 1; r < R; r++) {
+                        V w = tw[r * jm * TSTEP];
+                        if (!FWD) w.y = -w.y;
+                        a[r] = cmul(a[r], w);
+                    }
+                }
+                dft_r<V, FWD, R>(a);
+#pragma unroll
+                for (int r = 0; r < R; r++) dst[fpad<V>(base + (idxD + r * NS) * SM)] = a[r];
+            }
+        }
+    }
+}
+
+// All stages from S on; returns the buffer holding the result.  Ends with a
+// __syncthreads().
+template <typename V, bool FWD, bool BF, int N, int NB, int SM, int SB, int NTHR, int S = 0>
+__device__ __forceinline__ V *ct_batch(V *src, V *dst, int nb, const V *tw, int tid)
+{
+    if constexpr (ct_radix(N, S) == 0) {
+        return src;
+    } else {
+        ct_stage<V, FWD, BF, N, ct_radix(N, S), ct_ns(N, S), NB, SM, SB, NTHR>(src, dst, nb, tw, tid);
+        __syncthreads();
+        return ct_batch<V, FWD, BF, N, NB, SM, SB, NTHR, S + 1>(dst, src, nb, tw, tid);
+    }
 }
 
 // Split the spectrum Z of z = a + i b (length n, even) into the two FFTW

@@ -12,6 +12,7 @@
 // lambda_x(ix) + lambda_y(jy), and slots p and n-p of a half-complex array
 // share the eigenvalue, so they are stored once per class
 // (ix <= nx/2, jy <= ny/2): a quarter of the reference's b array.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -122,6 +123,216 @@ __global__ void __launch_bounds__(256) k_yfft(T *__restrict__ data, FftPlanDev<t
             const int c = e % nb, m = e / nb;
             plane[(size_t)m * ncol + c0 + c] = res[fpad<V>(m * w + c)];
         }
+    }
+}
+
+// Compile-time-length version of k_xfft (same layout, same arithmetic): N is
+// the line length, the batch per CTA is a constant, and the twiddle table is
+// staged in shared memory.  Used for the strided (ghosted) layout of the
+// host-pointer drop-in.
+template <int N> __host__ __device__ constexpr int ct_x_lines() { return N >= 1024 ? 1 : 1024 / N; }
+
+template <typename T, int N, bool FWD>
+__global__ void __launch_bounds__(256) k_xfft_ct(const T *__restrict__ in, size_t in_off, size_t in_sj, size_t in_sk,
+                                                 T *__restrict__ out, size_t out_off, size_t out_sj, size_t out_sk,
+                                                 const typename cplx_of<T>::type *__restrict__ twg, int ny, T scale)
+{
+    using V = typename cplx_of<T>::type;
+    constexpr int NB = ct_x_lines<N>(), BUF = fpad_elems<V>(NB * N);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *buf0 = reinterpret_cast<V *>(smem_raw);
+    V *buf1 = buf0 + BUF;
+    V *tw = buf1 + BUF;
+    const int k = blockIdx.y;
+    const int p0 = blockIdx.x * NB;
+    const int nb = min(NB, ny / 2 - p0);
+    const int tid = threadIdx.x;
+    for (int t = tid; t < N; t += 256) tw[t] = __ldg(twg + t);
+    for (int e = tid; e < nb * 2 * N; e += 256) {
+        const int m = e % N, r = (e / N) & 1, b = e / (2 * N);
+        const int j = 2 * (p0 + b) + r;
+        T val = in[in_off + (size_t)m + (size_t)j * in_sj + (size_t)k * in_sk];
+        reinterpret_cast<T *>(&buf0[fpad<V>(b * N + m)])[r] = val;
+    }
+    __syncthreads();
+    if (FWD) {
+        V *res = ct_batch<V, true, false, N, NB, 1, N, 256>(buf0, buf1, nb, tw, tid);
+        for (int e = tid; e < nb * N; e += 256) {
+            const int m = e % N, b = e / N;
+            V A = res[fpad<V>(b * N + m)], Bc = res[fpad<V>(b * N + (m == 0 ? 0 : N - m))];
+            V h = split_hc(A, Bc, m, N);
+            const int j = 2 * (p0 + b);
+            out[out_off + (size_t)m + (size_t)j * out_sj + (size_t)k * out_sk] = h.x;
+            out[out_off + (size_t)m + (size_t)(j + 1) * out_sj + (size_t)k * out_sk] = h.y;
+        }
+    } else {
+        for (int e = tid; e < nb * N; e += 256) {
+            const int m = e % N, b = e / N;
+            V P = buf0[fpad<V>(b * N + m)], Q = buf0[fpad<V>(b * N + (m == 0 ? 0 : N - m))];
+            buf1[fpad<V>(b * N + m)] = merge_hc(P, Q, m, N);
+        }
+        __syncthreads();
+        V *res = ct_batch<V, false, false, N, NB, 1, N, 256>(buf1, buf0, nb, tw, tid);
+        for (int e = tid; e < nb * N; e += 256) {
+            const int m = e % N, b = e / N;
+            V z = res[fpad<V>(b * N + m)];
+            const int j = 2 * (p0 + b);
+            out[out_off + (size_t)m + (size_t)j * out_sj + (size_t)k * out_sk] = z.x * scale;
+            out[out_off + (size_t)m + (size_t)(j + 1) * out_sj + (size_t)k * out_sk] = z.y * scale;
+        }
+    }
+}
+
+// Persistent versions on the compact layout [k][j][i] (the device solves):
+// each CTA walks line groups g = blockIdx.x, + gridDim.x, ...; the loads of
+// group g + gridDim.x are issued into registers before group g's transform
+// runs, so their latency overlaps the butterflies.  The y kernel moves whole
+// 32-byte sectors: W column pairs of V = 8 (FP32) or 4 (FP64) per row.
+template <typename V, int N> __host__ __device__ constexpr int pf_y_cols()
+{
+    return sizeof(V) == 8 ? ((3072 / N) >= 8 ? 8 : ((3072 / N) >= 4 ? 4 : 2))
+                          : ((1536 / N) >= 4 ? 4 : ((1536 / N) >= 2 ? 2 : 1));
+}
+
+// threads per CTA of the persistent x kernel, and line pairs per group: one
+// radix-8 stage of a group is one butterfly per thread
+template <typename T> __host__ __device__ constexpr int pf_x_threads() { return sizeof(T) == 8 ? 128 : 256; }
+template <typename T, int N> __host__ __device__ constexpr int pf_x_lines()
+{
+    return (pf_x_threads<T>() * 8 / N) < 1 ? 1 : pf_x_threads<T>() * 8 / N;
+}
+
+template <typename T, int N, bool FWD>
+__global__ void __launch_bounds__(pf_x_threads<T>()) k_xfft_pf(const T *__restrict__ in, T *__restrict__ out,
+                                                               const typename cplx_of<T>::type *__restrict__ twg,
+                                                               int ny, int total, T scale)
+{
+    using V = typename cplx_of<T>::type;
+    constexpr int NT = pf_x_threads<T>();
+    constexpr int NB = pf_x_lines<T, N>(), BUF = fpad_elems<V>(NB * N), E = (2 * NB * N + NT - 1) / NT;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *buf0 = reinterpret_cast<V *>(smem_raw);
+    V *buf1 = buf0 + BUF;
+    V *tw = buf1 + BUF;
+    const int tid = threadIdx.x;
+    const int gpk = (ny / 2 + NB - 1) / NB; // groups per k-plane
+    for (int t = tid; t < N; t += NT) tw[t] = __ldg(twg + t);
+    T pre[E];
+    auto fetch = [&](int g) {
+        const int k = g / gpk, p0 = (g % gpk) * NB, cnt = min(NB, ny / 2 - p0) * 2 * N;
+        const T *src = in + (size_t)k * N * ny + (size_t)2 * p0 * N; // rows 2 p0 .. 2 p0 + 2 nb - 1
+#pragma unroll
+        for (int i = 0; i < E; i++) {
+            const int e = tid + NT * i;
+            if (e < cnt) pre[i] = src[e];
+        }
+    };
+    int g = blockIdx.x;
+    if (g < total) fetch(g);
+    for (; g < total; g += gridDim.x) {
+        const int k = g / gpk, p0 = (g % gpk) * NB, nb = min(NB, ny / 2 - p0);
+#pragma unroll
+        for (int i = 0; i < E; i++) {
+            const int e = tid + NT * i;
+            if (e < nb * 2 * N) {
+                const int m = e % N, r = (e / N) & 1, b = e / (2 * N);
+                reinterpret_cast<T *>(&buf0[fpad<V>(b * N + m)])[r] = pre[i];
+            }
+        }
+        __syncthreads();
+        if (g + (int)gridDim.x < total) fetch(g + gridDim.x);
+        T *dst = out + (size_t)k * N * ny + (size_t)2 * p0 * N;
+        if (FWD) {
+            V *res = ct_batch<V, true, false, N, NB, 1, N, NT>(buf0, buf1, nb, tw, tid);
+            for (int e = tid; e < nb * N; e += NT) {
+                const int m = e % N, b = e / N;
+                V A = res[fpad<V>(b * N + m)], Bc = res[fpad<V>(b * N + (m == 0 ? 0 : N - m))];
+                V h = split_hc(A, Bc, m, N);
+                dst[(size_t)2 * b * N + m] = h.x;
+                dst[(size_t)(2 * b + 1) * N + m] = h.y;
+            }
+        } else {
+            for (int e = tid; e < nb * N; e += NT) {
+                const int m = e % N, b = e / N;
+                V P = buf0[fpad<V>(b * N + m)], Q = buf0[fpad<V>(b * N + (m == 0 ? 0 : N - m))];
+                buf1[fpad<V>(b * N + m)] = merge_hc(P, Q, m, N);
+            }
+            __syncthreads();
+            V *res = ct_batch<V, false, false, N, NB, 1, N, NT>(buf1, buf0, nb, tw, tid);
+            for (int e = tid; e < nb * N; e += NT) {
+                const int m = e % N, b = e / N;
+                V z = res[fpad<V>(b * N + m)];
+                dst[(size_t)2 * b * N + m] = z.x * scale;
+                dst[(size_t)(2 * b + 1) * N + m] = z.y * scale;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T, int N, bool FWD>
+__global__ void __launch_bounds__(256) k_yfft_pf(T *__restrict__ data, const typename cplx_of<T>::type *__restrict__ twg,
+                                                 int nx, int total)
+{
+    using V = typename cplx_of<T>::type;
+    constexpr int W = pf_y_cols<V, N>(), BUF = fpad_elems<V>(W * N), E = (W * N + 255) / 256;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int ncol = nx / 2;
+    V *buf0 = reinterpret_cast<V *>(smem_raw);
+    V *buf1 = buf0 + BUF;
+    V *tw = buf1 + BUF;
+    const int tid = threadIdx.x;
+    const int gpk = (ncol + W - 1) / W;
+    for (int t = tid; t < N; t += 256) tw[t] = __ldg(twg + t);
+    V pre[E];
+    auto fetch = [&](int g) {
+        const int k = g / gpk, c0 = (g % gpk) * W, nb = min(W, ncol - c0);
+        const V *plane = reinterpret_cast<const V *>(data) + (size_t)k * N * ncol;
+#pragma unroll
+        for (int i = 0; i < E; i++) {
+            const int e = tid + 256 * i, c = e % W, m = e / W;
+            if ((W * N) % 256 == 0 || e < W * N)
+                if (c < nb) pre[i] = plane[(size_t)m * ncol + c0 + c];
+        }
+    };
+    int g = blockIdx.x;
+    if (g < total) fetch(g);
+    for (; g < total; g += gridDim.x) {
+        const int k = g / gpk, c0 = (g % gpk) * W, nb = min(W, ncol - c0);
+        V *plane = reinterpret_cast<V *>(data) + (size_t)k * N * ncol;
+#pragma unroll
+        for (int i = 0; i < E; i++) {
+            const int e = tid + 256 * i, c = e % W, m = e / W;
+            if ((W * N) % 256 == 0 || e < W * N)
+                if (c < nb) buf0[fpad<V>(m * W + c)] = pre[i];
+        }
+        __syncthreads();
+        if (g + (int)gridDim.x < total) fetch(g + gridDim.x);
+        if (FWD) {
+            V *res = ct_batch<V, true, true, N, W, W, 1, 256>(buf0, buf1, nb, tw, tid);
+            for (int e = tid; e < W * N; e += 256) {
+                const int c = e % W, m = e / W;
+                if (c < nb) {
+                    V A = res[fpad<V>(m * W + c)], Bc = res[fpad<V>((m == 0 ? 0 : N - m) * W + c)];
+                    plane[(size_t)m * ncol + c0 + c] = split_hc(A, Bc, m, N);
+                }
+            }
+        } else {
+            for (int e = tid; e < W * N; e += 256) {
+                const int c = e % W, m = e / W;
+                if (c < nb) {
+                    V P = buf0[fpad<V>(m * W + c)], Q = buf0[fpad<V>((m == 0 ? 0 : N - m) * W + c)];
+                    buf1[fpad<V>(m * W + c)] = merge_hc(P, Q, m, N);
+                }
+            }
+            __syncthreads();
+            V *res = ct_batch<V, false, true, N, W, W, 1, 256>(buf1, buf0, nb, tw, tid);
+            for (int e = tid; e < W * N; e += 256) {
+                const int c = e % W, m = e / W;
+                if (c < nb) plane[(size_t)m * ncol + c0 + c] = res[fpad<V>(m * W + c)];
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -453,11 +664,89 @@ static int y_cols_per_cta(int nx, int ny)
     return w;
 }
 
+static int sm_count()
+{
+    static int n = 0;
+    if (n == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 1;
+    }
+    return n;
+}
+
+template <typename K> static int persistent_grid(K kernel, size_t shm, int total, int threads = 256)
+{
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, shm) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    return std::max(1, std::min(total, per_sm * sm_count()));
+}
+
+template <typename T, int N, bool FWD>
+static int launch_x_ct(const Ppe *s, const T *in, size_t in_off, size_t in_sj, size_t in_sk, T *out, size_t out_off,
+                       size_t out_sj, size_t out_sk, T scale, cudaStream_t st)
+{
+    using V = typename cplx_of<T>::type;
+    constexpr int NB = ct_x_lines<N>();
+    const size_t shm = sizeof(V) * (2 * (size_t)fpad_elems<V>(NB * N) + N);
+    const V *tw = reinterpret_cast<const V *>(sizeof(T) == 8 ? (const void *)s->d_twx64 : (const void *)s->d_twx32);
+    const size_t sk = (size_t)N * s->ny;
+    if (in_off == 0 && out_off == 0 && in_sj == (size_t)N && out_sj == (size_t)N && in_sk == sk && out_sk == sk) {
+        constexpr int NBP = pf_x_lines<T, N>(), NT = pf_x_threads<T>();
+        const size_t shmp = sizeof(V) * (2 * (size_t)fpad_elems<V>(NBP * N) + N);
+        if (shmp > 48 * 1024)
+            PL_CUDA_TRY(
+                cudaFuncSetAttribute(k_xfft_pf<T, N, FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmp));
+        const int total = ((s->ny / 2 + NBP - 1) / NBP) * s->nz;
+        k_xfft_pf<T, N, FWD><<<persistent_grid(k_xfft_pf<T, N, FWD>, shmp, total, NT), NT, shmp, st>>>(
+            in, out, tw, s->ny, total, scale);
+        PL_CHECK_LAUNCH();
+        return 0;
+    }
+    if (shm > 48 * 1024)
+        PL_CUDA_TRY(cudaFuncSetAttribute(k_xfft_ct<T, N, FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+    dim3 grid((s->ny / 2 + NB - 1) / NB, s->nz);
+    k_xfft_ct<T, N, FWD><<<grid, 256, shm, st>>>(in, in_off, in_sj, in_sk, out, out_off, out_sj, out_sk, tw, s->ny,
+                                                 scale);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
+template <typename T, int N, bool FWD> static int launch_y_ct(const Ppe *s, T *data, cudaStream_t st)
+{
+    using V = typename cplx_of<T>::type;
+    constexpr int W = pf_y_cols<V, N>();
+    const size_t shm = sizeof(V) * (2 * (size_t)fpad_elems<V>(W * N) + N);
+    if (shm > 48 * 1024)
+        PL_CUDA_TRY(cudaFuncSetAttribute(k_yfft_pf<T, N, FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+    const V *tw = reinterpret_cast<const V *>(sizeof(T) == 8 ? (const void *)s->d_twy64 : (const void *)s->d_twy32);
+    const int total = ((s->nx / 2 + W - 1) / W) * s->nz;
+    k_yfft_pf<T, N, FWD><<<persistent_grid(k_yfft_pf<T, N, FWD>, shm, total), 256, shm, st>>>(data, tw, s->nx, total);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
+// line lengths with compile-time kernels; other 2^a 3^b lengths use the
+// runtime-length kernels
+#define PL_FFT_CT_SIZES(X) X(64) X(128) X(192) X(256) X(384) X(512) X(768) X(1024)
+
 template <typename T>
 static int launch_x(const Ppe *s, bool fwd, const T *in, size_t in_off, size_t in_sj, size_t in_sk, T *out,
                     size_t out_off, size_t out_sj, size_t out_sk, T scale, cudaStream_t st)
 {
     using V = typename cplx_of<T>::type;
+    switch (s->nx) {
+#define PL_X_CASE(n)                                                                                               \
+    case n:                                                                                                        \
+        return fwd ? launch_x_ct<T, n, true>(s, in, in_off, in_sj, in_sk, out, out_off, out_sj, out_sk, scale, st)  \
+                   : launch_x_ct<T, n, false>(s, in, in_off, in_sj, in_sk, out, out_off, out_sj, out_sk, scale, st);
+        PL_FFT_CT_SIZES(PL_X_CASE)
+#undef PL_X_CASE
+    default:
+        break;
+    }
     const int pb = x_pairs_per_cta(s->nx, s->ny);
     dim3 grid((s->ny / 2 + pb - 1) / pb, s->nz);
     const size_t shm = 2 * sizeof(V) * (size_t)fpad_elems<V>(pb * s->nx);
@@ -476,6 +765,15 @@ static int launch_x(const Ppe *s, bool fwd, const T *in, size_t in_off, size_t i
 template <typename T> static int launch_y(const Ppe *s, bool fwd, T *data, cudaStream_t st)
 {
     using V = typename cplx_of<T>::type;
+    switch (s->ny) {
+#define PL_Y_CASE(n)                                                                                               \
+    case n:                                                                                                        \
+        return fwd ? launch_y_ct<T, n, true>(s, data, st) : launch_y_ct<T, n, false>(s, data, st);
+        PL_FFT_CT_SIZES(PL_Y_CASE)
+#undef PL_Y_CASE
+    default:
+        break;
+    }
     const int w = y_cols_per_cta(s->nx, s->ny);
     dim3 grid((s->nx / 2 + w - 1) / w, s->nz);
     const size_t shm = 2 * sizeof(V) * (size_t)fpad_elems<V>(w * s->ny);
