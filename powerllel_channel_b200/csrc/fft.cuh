@@ -312,13 +312,43 @@ template <typename V, bool FWD, int R> __device__ __forceinline__ void dft_r(V *
         dft2<V, FWD>(a[0], a[1]);
 }
 
+// Offset of stage s's twiddle block in the per-stage table: stage s (s >= 1)
+// holds w^(r jm N/(NS R)) at [(r-1) NS + jm], r = 1..R-1, jm < NS, so the
+// threads of a warp (consecutive jm) read consecutive entries.  The blocks
+// add up to N - 1 entries.
+__host__ __device__ constexpr int ct_twoff(int n, int s)
+{
+    int off = 0;
+    for (int q = 1; q < s; q++) off += ct_ns(n, q) * (ct_radix(n, q) - 1);
+    return off;
+}
+
+// Gather the per-stage twiddle table of length-N transforms from the global
+// table tw[t] = exp(-2 pi i t / N) (same values, reordered).
+template <typename V, int N, int NTHR>
+__device__ __forceinline__ void ct_build_twiddles(const V *__restrict__ twg, V *__restrict__ tws, int tid)
+{
+    int s = 1;
+    int off = 0;
+#pragma unroll 1
+    for (; ct_radix(N, s) != 0; s++) {
+        const int R = ct_radix(N, s), NS = ct_ns(N, s), tstep = N / (NS * R);
+        for (int idx = tid; idx < NS * (R - 1); idx += NTHR) {
+            const int r = idx / NS + 1, jm = idx % NS;
+            tws[off + idx] = __ldg(twg + r * jm * tstep);
+        }
+        off += NS * (R - 1);
+    }
+}
+
 // One stage over NB sequences (nb <= NB present) of length N; element (m, b)
 // at buf[fpad(m * SM + b * SB)]; BF: consecutive threads take consecutive b.
+// tws: this stage's block of the per-stage twiddle table.
 template <typename V, bool FWD, bool BF, int N, int R, int NS, int NB, int SM, int SB, int NTHR>
 __device__ __forceinline__ void ct_stage(const V *__restrict__ src, V *__restrict__ dst, int nb,
-                                         const V *__restrict__ tw, int tid)
+                                         const V *__restrict__ tws, int tid)
 {
-    constexpr int NBF = N / R, TSTEP = N / (NS * R), TOTAL = NBF * NB;
+    constexpr int NBF = N / R, TOTAL = NBF * NB;
     constexpr int ITERS = (TOTAL + NTHR - 1) / NTHR;
 #pragma unroll
     for (int it = 0; it < ITERS; it++) {
@@ -336,7 +366,7 @@ __device__ __forceinline__ void ct_stage(const V *__restrict__ src, V *__restric
                 if (NS > 1) {
 #pragma unroll
                     for (int r = 1; r < R; r++) {
-                        V w = tw[r * jm * TSTEP];
+                        V w = tws[(r - 1) * NS + jm];
                         if (!FWD) w.y = -w.y;
                         a[r] = cmul(a[r], w);
                     }
@@ -349,18 +379,101 @@ __device__ __forceinline__ void ct_stage(const V *__restrict__ src, V *__restric
     }
 }
 
-// All stages from S on; returns the buffer holding the result.  Ends with a
+// All stages from S on; tws is the per-stage twiddle table
+// (ct_build_twiddles).  Returns the buffer holding the result.  Ends with a
 // __syncthreads().
 template <typename V, bool FWD, bool BF, int N, int NB, int SM, int SB, int NTHR, int S = 0>
-__device__ __forceinline__ V *ct_batch(V *src, V *dst, int nb, const V *tw, int tid)
+__device__ __forceinline__ V *ct_batch(V *src, V *dst, int nb, const V *tws, int tid)
 {
     if constexpr (ct_radix(N, S) == 0) {
         return src;
     } else {
-        ct_stage<V, FWD, BF, N, ct_radix(N, S), ct_ns(N, S), NB, SM, SB, NTHR>(src, dst, nb, tw, tid);
+        ct_stage<V, FWD, BF, N, ct_radix(N, S), ct_ns(N, S), NB, SM, SB, NTHR>(src, dst, nb,
+                                                                              tws + (S > 0 ? ct_twoff(N, S) : 0), tid);
         __syncthreads();
-        return ct_batch<V, FWD, BF, N, NB, SM, SB, NTHR, S + 1>(dst, src, nb, tw, tid);
+        return ct_batch<V, FWD, BF, N, NB, SM, SB, NTHR, S + 1>(dst, src, nb, tws, tid);
     }
+}
+
+// In-place variant of ct_stage: every thread first loads, twiddles and
+// transforms all of its butterflies in registers, then (after a barrier that
+// the caller's previous stage ends with and one here) stores them over the
+// same buffer.  Halves the shared memory of the ping-pong form.
+template <typename V, bool FWD, bool BF, int N, int R, int NS, int NB, int SM, int SB, int NTHR>
+__device__ __forceinline__ void ct_stage_ip(V *buf, int nb, const V *__restrict__ tws, int tid)
+{
+    constexpr int NBF = N / R, TOTAL = NBF * NB;
+    constexpr int ITERS = (TOTAL + NTHR - 1) / NTHR;
+    V a[ITERS][R];
+#pragma unroll
+    for (int it = 0; it < ITERS; it++) {
+        const int q = tid + it * NTHR;
+        if (TOTAL % NTHR == 0 || q < TOTAL) {
+            const int b = BF ? q % NB : q / NBF;
+            const int j = BF ? q / NB : q % NBF;
+            if (b < nb) {
+                const int jm = j % NS;
+                const int base = b * SB;
+#pragma unroll
+                for (int r = 0; r < R; r++) a[it][r] = buf[fpad<V>(base + (j + r * NBF) * SM)];
+                if (NS > 1) {
+#pragma unroll
+                    for (int r = 1; r < R; r++) {
+                        V w = tws[(r - 1) * NS + jm];
+                        if (!FWD) w.y = -w.y;
+                        a[it][r] = cmul(a[it][r], w);
+                    }
+                }
+                dft_r<V, FWD, R>(a[it]);
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < ITERS; it++) {
+        const int q = tid + it * NTHR;
+        if (TOTAL % NTHR == 0 || q < TOTAL) {
+            const int b = BF ? q % NB : q / NBF;
+            const int j = BF ? q / NB : q % NBF;
+            if (b < nb) {
+                const int jm = j % NS;
+                const int idxD = (j / NS) * NS * R + jm;
+                const int base = b * SB;
+#pragma unroll
+                for (int r = 0; r < R; r++) buf[fpad<V>(base + (idxD + r * NS) * SM)] = a[it][r];
+            }
+        }
+    }
+}
+
+// All stages from S on, in place in buf.  Ends with a __syncthreads().
+template <typename V, bool FWD, bool BF, int N, int NB, int SM, int SB, int NTHR, int S = 0>
+__device__ __forceinline__ void ct_batch_ip(V *buf, int nb, const V *tws, int tid)
+{
+    if constexpr (ct_radix(N, S) != 0) {
+        ct_stage_ip<V, FWD, BF, N, ct_radix(N, S), ct_ns(N, S), NB, SM, SB, NTHR>(
+            buf, nb, tws + (S > 0 ? ct_twoff(N, S) : 0), tid);
+        __syncthreads();
+        ct_batch_ip<V, FWD, BF, N, NB, SM, SB, NTHR, S + 1>(buf, nb, tws, tid);
+    }
+}
+
+// Asynchronous global -> shared copies (cp.async; completion is awaited with
+// cp.async.wait_group, a hardware wait on this thread's own copies).
+__device__ __forceinline__ void cp_async_8(void *smem, const void *gmem)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_16(void *smem, const void *gmem)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int PENDING> __device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(PENDING) : "memory");
 }
 
 // Split the spectrum Z of z = a + i b (length n, even) into the two FFTW

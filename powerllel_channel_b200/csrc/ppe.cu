@@ -13,6 +13,7 @@
 // share the eigenvalue, so they are stored once per class
 // (ix <= nx/2, jy <= ny/2): a quarter of the reference's b array.
 #include <algorithm>
+#include <cstdint>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -147,7 +148,7 @@ __global__ void __launch_bounds__(256) k_xfft_ct(const T *__restrict__ in, size_
     const int p0 = blockIdx.x * NB;
     const int nb = min(NB, ny / 2 - p0);
     const int tid = threadIdx.x;
-    for (int t = tid; t < N; t += 256) tw[t] = __ldg(twg + t);
+    ct_build_twiddles<V, N, 256>(twg, tw, tid);
     for (int e = tid; e < nb * 2 * N; e += 256) {
         const int m = e % N, r = (e / N) & 1, b = e / (2 * N);
         const int j = 2 * (p0 + b) + r;
@@ -183,11 +184,15 @@ __global__ void __launch_bounds__(256) k_xfft_ct(const T *__restrict__ in, size_
     }
 }
 
-// Persistent versions on the compact layout [k][j][i] (the device solves):
-// each CTA walks line groups g = blockIdx.x, + gridDim.x, ...; the loads of
-// group g + gridDim.x are issued into registers before group g's transform
-// runs, so their latency overlaps the butterflies.  The y kernel moves whole
-// 32-byte sectors: W column pairs of V = 8 (FP32) or 4 (FP64) per row.
+// Persistent versions on the compact layout [k][j][i] (the device solves).
+// Each CTA walks line groups g = blockIdx.x, + gridDim.x, ...  The raw data
+// of the next group is copied global -> shared with cp.async into a staging
+// buffer while the current group is transformed in place in the work
+// buffer, so load latency overlaps the butterflies without holding the data
+// in registers.  The staging copy into the work buffer pairs the two real
+// lines into complex values (and, for the inverse, merges the half-complex
+// spectra).  The y kernel moves whole 32-byte sectors: W column pairs of V
+// per row (W * sizeof(V) = 64 bytes when N allows).
 template <typename V, int N> __host__ __device__ constexpr int pf_y_cols()
 {
     return sizeof(V) == 8 ? ((3072 / N) >= 8 ? 8 : ((3072 / N) >= 4 ? 4 : 2))
@@ -201,6 +206,18 @@ template <typename T, int N> __host__ __device__ constexpr int pf_x_lines()
 {
     return (pf_x_threads<T>() * 8 / N) < 1 ? 1 : pf_x_threads<T>() * 8 / N;
 }
+// shared memory of the persistent kernels, in V elements: work buffer,
+// staging buffer (rounded to an even count), per-stage twiddle table
+template <typename T, int N> __host__ __device__ constexpr int pf_x_smem_elems()
+{
+    using V = typename cplx_of<T>::type;
+    return (fpad_elems<V>(pf_x_lines<T, N>() * N) + 1) / 2 * 2 + pf_x_lines<T, N>() * N + N;
+}
+template <typename T, int N> __host__ __device__ constexpr int pf_y_smem_elems()
+{
+    using V = typename cplx_of<T>::type;
+    return (fpad_elems<V>(pf_y_cols<V, N>() * N) + 1) / 2 * 2 + pf_y_cols<V, N>() * N + N;
+}
 
 template <typename T, int N, bool FWD>
 __global__ void __launch_bounds__(pf_x_threads<T>()) k_xfft_pf(const T *__restrict__ in, T *__restrict__ out,
@@ -209,65 +226,64 @@ __global__ void __launch_bounds__(pf_x_threads<T>()) k_xfft_pf(const T *__restri
 {
     using V = typename cplx_of<T>::type;
     constexpr int NT = pf_x_threads<T>();
-    constexpr int NB = pf_x_lines<T, N>(), BUF = fpad_elems<V>(NB * N), E = (2 * NB * N + NT - 1) / NT;
+    constexpr int NB = pf_x_lines<T, N>(), BUF = (fpad_elems<V>(NB * N) + 1) / 2 * 2;
+    constexpr int CH = 16 / sizeof(T); // T values per 16-byte copy
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    V *buf0 = reinterpret_cast<V *>(smem_raw);
-    V *buf1 = buf0 + BUF;
-    V *tw = buf1 + BUF;
+    V *buf = reinterpret_cast<V *>(smem_raw);
+    T *stage = reinterpret_cast<T *>(buf + BUF); // 2 NB rows of N values, 16-byte aligned
+    V *tw = reinterpret_cast<V *>(stage + 2 * NB * N);
     const int tid = threadIdx.x;
     const int gpk = (ny / 2 + NB - 1) / NB; // groups per k-plane
-    for (int t = tid; t < N; t += NT) tw[t] = __ldg(twg + t);
-    T pre[E];
+    ct_build_twiddles<V, N, NT>(twg, tw, tid);
+    // rows 2 p0 .. 2 p0 + 2 nb - 1 of plane k are one contiguous run
     auto fetch = [&](int g) {
         const int k = g / gpk, p0 = (g % gpk) * NB, cnt = min(NB, ny / 2 - p0) * 2 * N;
-        const T *src = in + (size_t)k * N * ny + (size_t)2 * p0 * N; // rows 2 p0 .. 2 p0 + 2 nb - 1
-#pragma unroll
-        for (int i = 0; i < E; i++) {
-            const int e = tid + NT * i;
-            if (e < cnt) pre[i] = src[e];
-        }
+        const T *src = in + (size_t)k * N * ny + (size_t)2 * p0 * N;
+        for (int e = tid * CH; e < cnt; e += NT * CH) cp_async_16(stage + e, src + e);
+        cp_async_commit();
     };
-    int g = blockIdx.x;
-    if (g < total) fetch(g);
-    for (; g < total; g += gridDim.x) {
+    if (blockIdx.x < total) fetch(blockIdx.x);
+    for (int g = blockIdx.x; g < total; g += gridDim.x) {
         const int k = g / gpk, p0 = (g % gpk) * NB, nb = min(NB, ny / 2 - p0);
-#pragma unroll
-        for (int i = 0; i < E; i++) {
-            const int e = tid + NT * i;
-            if (e < nb * 2 * N) {
-                const int m = e % N, r = (e / N) & 1, b = e / (2 * N);
-                reinterpret_cast<T *>(&buf0[fpad<V>(b * N + m)])[r] = pre[i];
+        cp_async_wait<0>(); // this thread's copies of group g have landed
+        __syncthreads();    // ... and everyone's; the previous group is done with buf
+        for (int e = tid; e < nb * N; e += NT) {
+            const int m = e % N, b = e / N;
+            const T *r0 = stage + 2 * b * N, *r1 = r0 + N;
+            V z;
+            if (FWD) {
+                z.x = r0[m];
+                z.y = r1[m];
+            } else {
+                const int mc = (m == 0) ? 0 : N - m;
+                V P, Q;
+                P.x = r0[m];
+                P.y = r1[m];
+                Q.x = r0[mc];
+                Q.y = r1[mc];
+                z = merge_hc(P, Q, m, N);
             }
+            buf[fpad<V>(b * N + m)] = z;
         }
         __syncthreads();
         if (g + (int)gridDim.x < total) fetch(g + gridDim.x);
+        ct_batch_ip<V, FWD, false, N, NB, 1, N, NT>(buf, nb, tw, tid);
         T *dst = out + (size_t)k * N * ny + (size_t)2 * p0 * N;
-        if (FWD) {
-            V *res = ct_batch<V, true, false, N, NB, 1, N, NT>(buf0, buf1, nb, tw, tid);
-            for (int e = tid; e < nb * N; e += NT) {
-                const int m = e % N, b = e / N;
-                V A = res[fpad<V>(b * N + m)], Bc = res[fpad<V>(b * N + (m == 0 ? 0 : N - m))];
+        for (int e = tid; e < nb * N; e += NT) {
+            const int m = e % N, b = e / N;
+            if (FWD) {
+                V A = buf[fpad<V>(b * N + m)], Bc = buf[fpad<V>(b * N + (m == 0 ? 0 : N - m))];
                 V h = split_hc(A, Bc, m, N);
                 dst[(size_t)2 * b * N + m] = h.x;
                 dst[(size_t)(2 * b + 1) * N + m] = h.y;
-            }
-        } else {
-            for (int e = tid; e < nb * N; e += NT) {
-                const int m = e % N, b = e / N;
-                V P = buf0[fpad<V>(b * N + m)], Q = buf0[fpad<V>(b * N + (m == 0 ? 0 : N - m))];
-                buf1[fpad<V>(b * N + m)] = merge_hc(P, Q, m, N);
-            }
-            __syncthreads();
-            V *res = ct_batch<V, false, false, N, NB, 1, N, NT>(buf1, buf0, nb, tw, tid);
-            for (int e = tid; e < nb * N; e += NT) {
-                const int m = e % N, b = e / N;
-                V z = res[fpad<V>(b * N + m)];
+            } else {
+                V z = buf[fpad<V>(b * N + m)];
                 dst[(size_t)2 * b * N + m] = z.x * scale;
                 dst[(size_t)(2 * b + 1) * N + m] = z.y * scale;
             }
         }
-        __syncthreads();
     }
+    cp_async_wait<0>();
 }
 
 template <typename T, int N, bool FWD>
@@ -275,67 +291,61 @@ __global__ void __launch_bounds__(256) k_yfft_pf(T *__restrict__ data, const typ
                                                  int nx, int total)
 {
     using V = typename cplx_of<T>::type;
-    constexpr int W = pf_y_cols<V, N>(), BUF = fpad_elems<V>(W * N), E = (W * N + 255) / 256;
+    constexpr int W = pf_y_cols<V, N>(), BUF = (fpad_elems<V>(W * N) + 1) / 2 * 2, RAW = W * N;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int ncol = nx / 2;
-    V *buf0 = reinterpret_cast<V *>(smem_raw);
-    V *buf1 = buf0 + BUF;
-    V *tw = buf1 + BUF;
+    V *buf = reinterpret_cast<V *>(smem_raw);
+    V *stage = buf + BUF; // [m][c], dense
+    V *tw = stage + RAW;
     const int tid = threadIdx.x;
     const int gpk = (ncol + W - 1) / W;
-    for (int t = tid; t < N; t += 256) tw[t] = __ldg(twg + t);
-    V pre[E];
+    ct_build_twiddles<V, N, 256>(twg, tw, tid);
     auto fetch = [&](int g) {
         const int k = g / gpk, c0 = (g % gpk) * W, nb = min(W, ncol - c0);
         const V *plane = reinterpret_cast<const V *>(data) + (size_t)k * N * ncol;
-#pragma unroll
-        for (int i = 0; i < E; i++) {
-            const int e = tid + 256 * i, c = e % W, m = e / W;
-            if ((W * N) % 256 == 0 || e < W * N)
-                if (c < nb) pre[i] = plane[(size_t)m * ncol + c0 + c];
+        for (int e = tid; e < RAW; e += 256) {
+            const int c = e % W, m = e / W;
+            if (c < nb) {
+                if (sizeof(V) == 16)
+                    cp_async_16(stage + e, plane + (size_t)m * ncol + c0 + c);
+                else
+                    cp_async_8(stage + e, plane + (size_t)m * ncol + c0 + c);
+            }
         }
+        cp_async_commit();
     };
-    int g = blockIdx.x;
-    if (g < total) fetch(g);
-    for (; g < total; g += gridDim.x) {
+    if (blockIdx.x < total) fetch(blockIdx.x);
+    for (int g = blockIdx.x; g < total; g += gridDim.x) {
         const int k = g / gpk, c0 = (g % gpk) * W, nb = min(W, ncol - c0);
         V *plane = reinterpret_cast<V *>(data) + (size_t)k * N * ncol;
-#pragma unroll
-        for (int i = 0; i < E; i++) {
-            const int e = tid + 256 * i, c = e % W, m = e / W;
-            if ((W * N) % 256 == 0 || e < W * N)
-                if (c < nb) buf0[fpad<V>(m * W + c)] = pre[i];
+        cp_async_wait<0>();
+        __syncthreads();
+        for (int e = tid; e < RAW; e += 256) {
+            const int c = e % W, m = e / W;
+            if (c < nb) {
+                if (FWD)
+                    buf[fpad<V>(m * W + c)] = stage[e];
+                else
+                    buf[fpad<V>(m * W + c)] = merge_hc(stage[e], stage[(m == 0 ? 0 : N - m) * W + c], m, N);
+            }
         }
         __syncthreads();
         if (g + (int)gridDim.x < total) fetch(g + gridDim.x);
-        if (FWD) {
-            V *res = ct_batch<V, true, true, N, W, W, 1, 256>(buf0, buf1, nb, tw, tid);
-            for (int e = tid; e < W * N; e += 256) {
-                const int c = e % W, m = e / W;
-                if (c < nb) {
-                    V A = res[fpad<V>(m * W + c)], Bc = res[fpad<V>((m == 0 ? 0 : N - m) * W + c)];
+        ct_batch_ip<V, FWD, true, N, W, W, 1, 256>(buf, nb, tw, tid);
+        for (int e = tid; e < RAW; e += 256) {
+            const int c = e % W, m = e / W;
+            if (c < nb) {
+                if (FWD) {
+                    V A = buf[fpad<V>(m * W + c)], Bc = buf[fpad<V>((m == 0 ? 0 : N - m) * W + c)];
                     plane[(size_t)m * ncol + c0 + c] = split_hc(A, Bc, m, N);
+                } else {
+                    plane[(size_t)m * ncol + c0 + c] = buf[fpad<V>(m * W + c)];
                 }
-            }
-        } else {
-            for (int e = tid; e < W * N; e += 256) {
-                const int c = e % W, m = e / W;
-                if (c < nb) {
-                    V P = buf0[fpad<V>(m * W + c)], Q = buf0[fpad<V>((m == 0 ? 0 : N - m) * W + c)];
-                    buf1[fpad<V>(m * W + c)] = merge_hc(P, Q, m, N);
-                }
-            }
-            __syncthreads();
-            V *res = ct_batch<V, false, true, N, W, W, 1, 256>(buf1, buf0, nb, tw, tid);
-            for (int e = tid; e < W * N; e += 256) {
-                const int c = e % W, m = e / W;
-                if (c < nb) plane[(size_t)m * ncol + c0 + c] = res[fpad<V>(m * W + c)];
             }
         }
-        __syncthreads();
     }
+    cp_async_wait<0>();
 }
-
 // ------------------------------------------------------------------------
 // Tridiagonal kernels (FP64 arithmetic in both precision modes)
 // ------------------------------------------------------------------------
@@ -693,9 +703,11 @@ static int launch_x_ct(const Ppe *s, const T *in, size_t in_off, size_t in_sj, s
     const size_t shm = sizeof(V) * (2 * (size_t)fpad_elems<V>(NB * N) + N);
     const V *tw = reinterpret_cast<const V *>(sizeof(T) == 8 ? (const void *)s->d_twx64 : (const void *)s->d_twx32);
     const size_t sk = (size_t)N * s->ny;
-    if (in_off == 0 && out_off == 0 && in_sj == (size_t)N && out_sj == (size_t)N && in_sk == sk && out_sk == sk) {
-        constexpr int NBP = pf_x_lines<T, N>(), NT = pf_x_threads<T>();
-        const size_t shmp = sizeof(V) * (2 * (size_t)fpad_elems<V>(NBP * N) + N);
+    const bool aligned = ((uintptr_t)in % 16 == 0) && ((uintptr_t)out % 16 == 0);
+    if (aligned && in_off == 0 && out_off == 0 && in_sj == (size_t)N && out_sj == (size_t)N && in_sk == sk &&
+        out_sk == sk) {
+        constexpr int NT = pf_x_threads<T>(), NBP = pf_x_lines<T, N>();
+        const size_t shmp = sizeof(V) * (size_t)pf_x_smem_elems<T, N>();
         if (shmp > 48 * 1024)
             PL_CUDA_TRY(
                 cudaFuncSetAttribute(k_xfft_pf<T, N, FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmp));
@@ -718,7 +730,7 @@ template <typename T, int N, bool FWD> static int launch_y_ct(const Ppe *s, T *d
 {
     using V = typename cplx_of<T>::type;
     constexpr int W = pf_y_cols<V, N>();
-    const size_t shm = sizeof(V) * (2 * (size_t)fpad_elems<V>(W * N) + N);
+    const size_t shm = sizeof(V) * (size_t)pf_y_smem_elems<T, N>();
     if (shm > 48 * 1024)
         PL_CUDA_TRY(cudaFuncSetAttribute(k_yfft_pf<T, N, FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
     const V *tw = reinterpret_cast<const V *>(sizeof(T) == 8 ? (const void *)s->d_twy64 : (const void *)s->d_twy32);
@@ -768,7 +780,9 @@ template <typename T> static int launch_y(const Ppe *s, bool fwd, T *data, cudaS
     switch (s->ny) {
 #define PL_Y_CASE(n)                                                                                               \
     case n:                                                                                                        \
-        return fwd ? launch_y_ct<T, n, true>(s, data, st) : launch_y_ct<T, n, false>(s, data, st);
+        if ((uintptr_t)data % 16 == 0)                                                                             \
+            return fwd ? launch_y_ct<T, n, true>(s, data, st) : launch_y_ct<T, n, false>(s, data, st);             \
+        break;
         PL_FFT_CT_SIZES(PL_Y_CASE)
 #undef PL_Y_CASE
     default:
