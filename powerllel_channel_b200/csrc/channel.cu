@@ -428,25 +428,19 @@ extern "C" int pl_phase_rk2(pl_channel *c)
 // mixed path pressure prediction: the first two projections after the
 // initial field solve for the full pressure (the first one removes the
 // initial divergence, an outlier in time); then the increment over p_n, and
-// from the fourth on over the extrapolation 2 p_n - p_{n-1}
-static int mixed_mode(const pl_channel *c, const double **pn, const double **pnm1)
-{
-    *pn = c->p;
-    *pnm1 = c->p;
-    if (!c->incremental || c->nsolve < 2) return 0;
-    if (c->nsolve >= 3) *pnm1 = c->pm;
-    return 1;
-}
+// from the fourth on over the extrapolation 2 p_n - p_{n-1}.  The prediction
+// for the next projection is written by the solve's inverse x transform into
+// pb and rotated into pm, where the next residual reads it.
+static int mixed_incremental(const pl_channel *c) { return (c->incremental && c->nsolve >= 2) ? 1 : 0; }
 
 extern "C" int pl_phase_calc_rhs(pl_channel *c)
 {
     int rc;
     if (is_mixed(c)) {
         const double dx = c->cfg.lx / c->nx, dy = c->cfg.ly / c->ny;
-        const double *pn, *pnm1;
-        const int inc = mixed_mode(c, &pn, &pnm1);
-        rc = launch_rhs_mixed(c->u, c->v, c->w, pn, pnm1, c->r32, c->plane_part, c->mode0, c->sp, c->m, c->ppe.d_a,
-                              c->ppe.d_bt, c->ppe.d_c, 1.0 / (dx * dx), 1.0 / (dy * dy), inc, c->stream);
+        rc = launch_rhs_mixed(c->u, c->v, c->w, c->pm, c->r32, c->plane_part, c->mode0, c->sp, c->m, c->ppe.d_a,
+                              c->ppe.d_bt, c->ppe.d_c, 1.0 / (dx * dx), 1.0 / (dy * dy), mixed_incremental(c),
+                              c->stream);
     } else {
         rc = launch_calc_rhs_fp64(c->u, c->v, c->w, c->p, c->sp, c->m, c->stream);
     }
@@ -456,27 +450,28 @@ extern "C" int pl_phase_calc_rhs(pl_channel *c)
 
 extern "C" int pl_phase_poisson(pl_channel *c)
 {
-    if (is_mixed(c)) return ppe_solve_fp32(&c->ppe, c->r32, c->mode0, c->stream);
+    if (is_mixed(c)) {
+        // the increment solve; its inverse x transform also forms
+        // p_n <- prediction + increment (in place) and, in pb, the next
+        // prediction, extrapolated from the third projection on
+        PressureUpdate pu;
+        pu.q = c->pm;
+        pu.p = c->p;
+        pu.qnext = c->pb;
+        pu.incremental = mixed_incremental(c);
+        pu.qmode = (c->nsolve + 1 >= 3) ? 1 : 0;
+        return ppe_solve_fp32(&c->ppe, c->r32, c->mode0, c->stream, &pu);
+    }
     return ppe_solve_fp64(&c->ppe, c->p, c->stream);
 }
 
 extern "C" int pl_phase_correct_force(pl_channel *c)
 {
-    int rc;
+    const int rc = launch_correct_force_fp64(c->p, c->u, c->v, c->w, c->sp, c->m, c->cfg.is_forced[0], c->ms.scalar,
+                                             c->stream);
     if (is_mixed(c)) {
-        const double *pn, *pnm1;
-        const int inc = mixed_mode(c, &pn, &pnm1);
-        rc = launch_correct_mixed(pn, pnm1, c->r32, c->pb, c->u, c->v, c->w, c->sp, c->m, c->cfg.is_forced[0],
-                                  c->ms.scalar, inc, c->stream);
-        // rotate: p_{n-1} <- p_n, p_n <- p_new
-        double *old_pm = c->pm;
-        c->pm = c->p;
-        c->p = c->pb;
-        c->pb = old_pm;
+        std::swap(c->pm, c->pb); // the prediction written by the solve
         c->nsolve++;
-    } else {
-        rc = launch_correct_force_fp64(c->p, c->u, c->v, c->w, c->sp, c->m, c->cfg.is_forced[0], c->ms.scalar,
-                                       c->stream);
     }
     channel_mark(c, "correct_force");
     return rc;

@@ -20,8 +20,9 @@ struct pl_channel {
     pl::MeshDev m{};
     // FP64 path: u,v,w = ua,va,wa; stage-1 fields u1,v1,w1; p
     // mixed path: u,v,w ping-pong between (ua,va,wa) and (ub,vb,wb); stage-1
-    // increments d1u,d1v,d1w (FP32); p ping-pong between p and pb (FP64); the
-    // PPE works in place on r32 (FP32)
+    // increments d1u,d1v,d1w (FP32); p = p_n (FP64, updated in place); the
+    // pressure prediction for the next projection in pm, written into pb by
+    // the correction and swapped (FP64); the PPE works in place on r32 (FP32)
     double *u = nullptr, *v = nullptr, *w = nullptr;
     double *u1 = nullptr, *v1 = nullptr, *w1 = nullptr;
     double *p = nullptr;

@@ -184,6 +184,24 @@ __global__ void __launch_bounds__(256) k_xfft_ct(const T *__restrict__ in, size_
     }
 }
 
+// pressure update of one point o (PressureUpdate in ppe.cuh); dp is the
+// FP32 increment widened to FP64
+__device__ __forceinline__ void pressure_update(const PressureUpdate &pu, size_t o, double dp)
+{
+    const double pn = (pu.incremental ? __ldg(pu.q + o) : 0.0) + dp;
+    const double pold = __ldg(pu.p + o);
+    // the prediction first: storing over the just-read p before another
+    // stream measured markedly slower on B200
+    pu.qnext[o] = pu.qmode ? 2.0 * pn - pold : pn;
+    pu.p[o] = pn;
+}
+
+__global__ void __launch_bounds__(256) k_pressure_update(const float *__restrict__ dp, PressureUpdate pu, size_t n)
+{
+    for (size_t o = (size_t)blockIdx.x * 256 + threadIdx.x; o < n; o += (size_t)gridDim.x * 256)
+        pressure_update(pu, o, (double)__ldg(dp + o));
+}
+
 // Persistent versions on the compact layout [k][j][i] (the device solves).
 // Each CTA walks line groups g = blockIdx.x, + gridDim.x, ...  The raw data
 // of the next group is copied global -> shared with cp.async into a staging
@@ -222,7 +240,7 @@ template <typename T, int N> __host__ __device__ constexpr int pf_y_smem_elems()
 template <typename T, int N, bool FWD>
 __global__ void __launch_bounds__(pf_x_threads<T>()) k_xfft_pf(const T *__restrict__ in, T *__restrict__ out,
                                                                const typename cplx_of<T>::type *__restrict__ twg,
-                                                               int ny, int total, T scale)
+                                                               int ny, int total, T scale, PressureUpdate pu)
 {
     using V = typename cplx_of<T>::type;
     constexpr int NT = pf_x_threads<T>();
@@ -278,8 +296,15 @@ __global__ void __launch_bounds__(pf_x_threads<T>()) k_xfft_pf(const T *__restri
                 dst[(size_t)(2 * b + 1) * N + m] = h.y;
             } else {
                 V z = buf[fpad<V>(b * N + m)];
-                dst[(size_t)2 * b * N + m] = z.x * scale;
-                dst[(size_t)(2 * b + 1) * N + m] = z.y * scale;
+                const T d0 = z.x * scale, d1 = z.y * scale;
+                if (sizeof(T) == 4 && pu.p) {
+                    const size_t o = (size_t)k * N * ny + (size_t)2 * p0 * N + (size_t)2 * b * N + m;
+                    pressure_update(pu, o, (double)d0);
+                    pressure_update(pu, o + N, (double)d1);
+                } else {
+                    dst[(size_t)2 * b * N + m] = d0;
+                    dst[(size_t)(2 * b + 1) * N + m] = d1;
+                }
             }
         }
     }
@@ -696,7 +721,7 @@ template <typename K> static int persistent_grid(K kernel, size_t shm, int total
 
 template <typename T, int N, bool FWD>
 static int launch_x_ct(const Ppe *s, const T *in, size_t in_off, size_t in_sj, size_t in_sk, T *out, size_t out_off,
-                       size_t out_sj, size_t out_sk, T scale, cudaStream_t st)
+                       size_t out_sj, size_t out_sk, T scale, cudaStream_t st, const PressureUpdate *pu, bool *fused)
 {
     using V = typename cplx_of<T>::type;
     constexpr int NB = ct_x_lines<N>();
@@ -713,8 +738,9 @@ static int launch_x_ct(const Ppe *s, const T *in, size_t in_off, size_t in_sj, s
                 cudaFuncSetAttribute(k_xfft_pf<T, N, FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmp));
         const int total = ((s->ny / 2 + NBP - 1) / NBP) * s->nz;
         k_xfft_pf<T, N, FWD><<<persistent_grid(k_xfft_pf<T, N, FWD>, shmp, total, NT), NT, shmp, st>>>(
-            in, out, tw, s->ny, total, scale);
+            in, out, tw, s->ny, total, scale, (pu && !FWD) ? *pu : PressureUpdate{});
         PL_CHECK_LAUNCH();
+        *fused = (pu != nullptr) && !FWD;
         return 0;
     }
     if (shm > 48 * 1024)
@@ -744,21 +770,42 @@ template <typename T, int N, bool FWD> static int launch_y_ct(const Ppe *s, T *d
 // runtime-length kernels
 #define PL_FFT_CT_SIZES(X) X(64) X(128) X(192) X(256) X(384) X(512) X(768) X(1024)
 
+template <typename T> static int launch_pressure_update(const Ppe *s, const T *dp, const PressureUpdate *pu, cudaStream_t st)
+{
+    if (sizeof(T) != 4) {
+        set_error("pressure update: FP32 increments only");
+        return -1;
+    }
+    const size_t n = (size_t)s->nx * s->ny * s->nz;
+    const int grid = (int)std::min<size_t>((n + 255) / 256, (size_t)sm_count() * 16);
+    k_pressure_update<<<grid, 256, 0, st>>>(reinterpret_cast<const float *>(dp), *pu, n);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
 template <typename T>
 static int launch_x(const Ppe *s, bool fwd, const T *in, size_t in_off, size_t in_sj, size_t in_sk, T *out,
-                    size_t out_off, size_t out_sj, size_t out_sk, T scale, cudaStream_t st)
+                    size_t out_off, size_t out_sj, size_t out_sk, T scale, cudaStream_t st,
+                    const PressureUpdate *pu = nullptr)
 {
     using V = typename cplx_of<T>::type;
+    bool fused = false;
+    int rc = 1;
     switch (s->nx) {
 #define PL_X_CASE(n)                                                                                               \
     case n:                                                                                                        \
-        return fwd ? launch_x_ct<T, n, true>(s, in, in_off, in_sj, in_sk, out, out_off, out_sj, out_sk, scale, st)  \
-                   : launch_x_ct<T, n, false>(s, in, in_off, in_sj, in_sk, out, out_off, out_sj, out_sk, scale, st);
+        rc = fwd ? launch_x_ct<T, n, true>(s, in, in_off, in_sj, in_sk, out, out_off, out_sj, out_sk, scale, st,    \
+                                           pu, &fused)                                                              \
+                 : launch_x_ct<T, n, false>(s, in, in_off, in_sj, in_sk, out, out_off, out_sj, out_sk, scale, st,   \
+                                            pu, &fused);                                                            \
+        break;
         PL_FFT_CT_SIZES(PL_X_CASE)
 #undef PL_X_CASE
     default:
         break;
     }
+    if (rc == 0) return (pu && !fused) ? launch_pressure_update(s, out, pu, st) : 0;
+    if (rc < 0) return rc;
     const int pb = x_pairs_per_cta(s->nx, s->ny);
     dim3 grid((s->ny / 2 + pb - 1) / pb, s->nz);
     const size_t shm = 2 * sizeof(V) * (size_t)fpad_elems<V>(pb * s->nx);
@@ -771,7 +818,7 @@ static int launch_x(const Ppe *s, bool fwd, const T *in, size_t in_off, size_t i
         k_xfft<T, false><<<grid, 256, shm, st>>>(in, in_off, in_sj, in_sk, out, out_off, out_sj, out_sk, plan,
                                                  s->ny, pb, scale);
     PL_CHECK_LAUNCH();
-    return 0;
+    return pu ? launch_pressure_update(s, out, pu, st) : 0;
 }
 
 template <typename T> static int launch_y(const Ppe *s, bool fwd, T *data, cudaStream_t st)
@@ -858,18 +905,24 @@ int ppe_solve_fp64(Ppe *s, double *d_var, cudaStream_t st)
     return ppe_solve_fp64_strided(s, d_var, d_var, 0, nxl, nxy, d_var, st);
 }
 
-int ppe_solve_fp32(Ppe *s, float *d_var, const double *mode0, cudaStream_t st)
+int ppe_solve_fp32(Ppe *s, float *d_var, const double *mode0, cudaStream_t st, const PressureUpdate *pu)
 {
     const size_t nxl = s->nx, nxy = (size_t)s->nx * s->ny;
     if (launch_x<float>(s, true, d_var, 0, nxl, nxy, d_var, 0, nxl, nxy, 1.0f, st)) return -1;
     mark(s, "ppe_xfft_fwd");
+    return ppe_solve_fp32_from_x(s, d_var, mode0, st, pu);
+}
+
+int ppe_solve_fp32_from_x(Ppe *s, float *d_var, const double *mode0, cudaStream_t st, const PressureUpdate *pu)
+{
+    const size_t nxl = s->nx, nxy = (size_t)s->nx * s->ny;
     if (launch_y<float>(s, true, d_var, st)) return -1;
     mark(s, "ppe_yfft_fwd");
     if (launch_trid<float>(s, d_var, st, s->nparts == 0 ? mode0 : nullptr)) return -1;
     mark(s, s->nparts ? "ppe_pdd" : "ppe_thomas");
     if (launch_y<float>(s, false, d_var, st)) return -1;
     mark(s, "ppe_yfft_bwd");
-    if (launch_x<float>(s, false, d_var, 0, nxl, nxy, d_var, 0, nxl, nxy, (float)s->norm, st)) return -1;
+    if (launch_x<float>(s, false, d_var, 0, nxl, nxy, d_var, 0, nxl, nxy, (float)s->norm, st, pu)) return -1;
     mark(s, "ppe_xfft_bwd");
     return 0;
 }

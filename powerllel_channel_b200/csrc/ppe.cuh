@@ -59,7 +59,21 @@ int ppe_solve_fp64(Ppe *s, double *d_var, cudaStream_t st);
 // mode0 (optional, FP64 [nz]): the plane sums of the right-hand side; when
 // given, the (kx,ky) = (0,0) system is solved from them in FP64 with the
 // gauge x[nz-1] = 0 (Thomas only) instead of from the FP32 transform.
-int ppe_solve_fp32(Ppe *s, float *d_var, const double *mode0, cudaStream_t st);
+// Mixed step: the pressure update applied to the FP32 solution dp of the
+// increment solve, fused into the inverse x transform where the layout
+// allows (one kernel otherwise): p_new = (incremental ? q : 0) + dp stored
+// in p (in place of p_n), and the next prediction qnext = qmode ?
+// 2 p_new - p_n : p_new (FP64, interior-only layout).
+struct PressureUpdate {
+    const double *q = nullptr;
+    double *p = nullptr, *qnext = nullptr;
+    int incremental = 0, qmode = 0;
+};
+int ppe_solve_fp32(Ppe *s, float *d_var, const double *mode0, cudaStream_t st, const PressureUpdate *pu = nullptr);
+// the same solve when d_var already holds the forward x transform
+int ppe_solve_fp32_from_x(Ppe *s, float *d_var, const double *mode0, cudaStream_t st,
+                          const PressureUpdate *pu = nullptr);
+
 
 // Solve reading from / writing to a strided device array (the reference's
 // ghosted layout): element (i,j,k), 0-based interior, at base[off + i +

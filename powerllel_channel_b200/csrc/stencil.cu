@@ -459,20 +459,14 @@ __global__ void __launch_bounds__(256) k_rk2_mixed(const double *__restrict__ u,
 // sums of r (the (kx,ky) = (0,0) right-hand side, solved in FP64).
 // p_pred = 2 p_n - p_{n-1} is the linear extrapolation of the pressure in
 // time: every FP32 error of the increment solve scales with |r|, and the
-// extrapolation makes r the second difference of p in time.
+// extrapolation makes r the second difference of p in time.  The previous
+// step's correction kernel stores p_pred (pq), so the residual reads one
+// FP64 pressure array.
 // L is exactly the operator the PPE inverts: periodic second differences
 // over dx^2, dy^2 and the tridiagonal row a, bt, c in z.
-struct ZOp {
-    const double *a, *bt, *c; // per k (0-based interior), set_trid_coeff rows
-};
-
-struct PPred {
-    const double *__restrict__ pn, *__restrict__ pnm1;
-    __device__ __forceinline__ double operator()(size_t q) const { return 2.0 * __ldg(pn + q) - __ldg(pnm1 + q); }
-};
-
 __global__ void __launch_bounds__(256) k_rhs_mixed(const double *__restrict__ u, const double *__restrict__ v,
-                                                   const double *__restrict__ w, PPred pp, float *__restrict__ r,
+                                                   const double *__restrict__ w, const double *__restrict__ pq,
+                                                   float *__restrict__ r,
                                                    double *__restrict__ warp_part, StepParams p, MeshDev m, ZOp z,
                                                    double dxi2, double dyi2, int incremental)
 {
@@ -487,6 +481,7 @@ __global__ void __launch_bounds__(256) k_rhs_mixed(const double *__restrict__ u,
         double rhs = (__ldg(u + n.c) - __ldg(u + n.xm)) * dtidxi + (__ldg(v + n.c) - __ldg(v + n.ym)) * dtidyi +
                      (__ldg(w + n.c) - __ldg(w + n.zm)) * dti * __ldg(m.dzf_inv + k);
         if (incremental) {
+            const auto pp = [&](size_t q) { return __ldg(pq + q); };
             const size_t pc = n.c - sk;
             const double p0 = pp(pc);
             double lp = (pp(n.xp - sk) - 2.0 * p0 + pp(n.xm - sk)) * dxi2 + (pp(n.yp - sk) - 2.0 * p0 + pp(n.ym - sk)) * dyi2;
@@ -524,40 +519,6 @@ __global__ void k_plane_sums(const double *part, int nper, int nz, double *mode0
         __syncthreads();
     }
     if (threadIdx.x == 0) mode0[k] = sh[0];
-}
-
-// correctVel with p = p_pred + dp (FP64 prediction + FP32 increment), the new
-// p stored in FP64 in a third buffer, + forceVel shift + wall fill
-__global__ void __launch_bounds__(256) k_correct_mixed(PPred pp, const float *__restrict__ dp,
-                                                       double *__restrict__ pnew, double *u, double *v, double *w,
-                                                       StepParams p, MeshDev m, int forced_x, const double *scalar,
-                                                       int incremental)
-{
-    PL_POINT_INDEX();
-    const Nb n = neighbours(i, j, k, p.nx, p.ny);
-    const size_t pc = n.c - sk;
-    auto P = [&](size_t q) { return (incremental ? pp(q) : 0.0) + (double)__ldg(dp + q); };
-    const double dt = p.dt, dtdxi = dt * p.dx_inv, dtdyi = dt * p.dy_inv;
-    const double p0 = P(pc);
-    const double pxp = P(n.xp - sk), pyp = P(n.yp - sk);
-    const double pzp = (k < p.nz) ? P(pc + sk) : p0;
-    pnew[pc] = p0;
-    double nu = u[n.c] - (pxp - p0) * dtdxi;
-    if (forced_x) nu = nu + __ldg(scalar + 3);
-    const double nv = v[n.c] - (pyp - p0) * dtdyi;
-    const double nw = w[n.c] - (pzp - p0) * dt * __ldg(m.dzc_inv + k);
-    u[n.c] = nu;
-    v[n.c] = nv;
-    w[n.c] = nw;
-    const double bcu = 0.0 - p.u_crf;
-    if (k == 1) {
-        u[n.c - sk] = 2.0 * bcu - nu;
-        v[n.c - sk] = -nv;
-    }
-    if (k == p.nz) {
-        u[n.c + sk] = 2.0 * bcu - nu;
-        v[n.c + sk] = -nv;
-    }
 }
 
 // ------------------------------------------------------------------------
@@ -720,28 +681,17 @@ int launch_rk2_mixed(const double *u, const double *v, const double *w, const fl
     return 0;
 }
 
-int launch_rhs_mixed(const double *u, const double *v, const double *w, const double *pn, const double *pnm1,
-                     float *r, double *warp_part, double *mode0, const StepParams &p, const MeshDev &m,
-                     const double *za, const double *zbt, const double *zc, double dxi2, double dyi2, int incremental,
-                     cudaStream_t st)
+int launch_rhs_mixed(const double *u, const double *v, const double *w, const double *pq, float *r,
+                     double *warp_part, double *mode0, const StepParams &p, const MeshDev &m, const double *za,
+                     const double *zbt, const double *zc, double dxi2, double dyi2, int incremental, cudaStream_t st)
 {
     ZOp z{za, zbt, zc};
-    k_rhs_mixed<<<point_grid(p), point_block(), 0, st>>>(u, v, w, PPred{pn, pnm1}, r, warp_part, p, m, z, dxi2, dyi2,
+    k_rhs_mixed<<<point_grid(p), point_block(), 0, st>>>(u, v, w, pq, r, warp_part, p, m, z, dxi2, dyi2,
                                                           incremental);
     PL_CHECK_LAUNCH();
     dim3 g = point_grid(p);
     const int nper = (int)(g.x * g.y) * (int)((point_block().x * point_block().y) / 32);
     k_plane_sums<<<p.nz, 256, 0, st>>>(warp_part, nper, p.nz, mode0);
-    PL_CHECK_LAUNCH();
-    return 0;
-}
-
-int launch_correct_mixed(const double *pn, const double *pnm1, const float *dp, double *pnew, double *u, double *v,
-                         double *w, const StepParams &p, const MeshDev &m, int forced_x, const double *scalar,
-                         int incremental, cudaStream_t st)
-{
-    k_correct_mixed<<<point_grid(p), point_block(), 0, st>>>(PPred{pn, pnm1}, dp, pnew, u, v, w, p, m, forced_x,
-                                                              scalar, incremental);
     PL_CHECK_LAUNCH();
     return 0;
 }

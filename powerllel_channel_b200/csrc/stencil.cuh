@@ -24,6 +24,12 @@ struct ReduceBuf {
     int max_blocks = 0;
 };
 
+// Mixed path: the z operator of the incremental pressure residual
+struct ZOp {
+    const double *a, *bt, *c; // per k (0-based interior), set_trid_coeff rows
+};
+
+
 // FP64 step kernels (one launch each)
 int launch_rk1_fp64(const double *u, const double *v, const double *w, double *u1, double *v1, double *w1,
                     const StepParams &p, const MeshDev &m, cudaStream_t st);
@@ -68,13 +74,9 @@ int launch_rk1_mixed(const double *u, const double *v, const double *w, float *d
 int launch_rk2_mixed(const double *u, const double *v, const double *w, const float *d1u, const float *d1v,
                      const float *d1w, double *uo, double *vo, double *wo, const StepParams &p, const MeshDev &m,
                      MeanState &ms, cudaStream_t st);
-int launch_rhs_mixed(const double *u, const double *v, const double *w, const double *pn, const double *pnm1,
-                     float *r, double *warp_part, double *mode0, const StepParams &p, const MeshDev &m,
-                     const double *za, const double *zbt, const double *zc, double dxi2, double dyi2, int incremental,
-                     cudaStream_t st);
-int launch_correct_mixed(const double *pn, const double *pnm1, const float *dp, double *pnew, double *u, double *v,
-                         double *w, const StepParams &p, const MeshDev &m, int forced_x, const double *scalar,
-                         int incremental, cudaStream_t st);
+int launch_rhs_mixed(const double *u, const double *v, const double *w, const double *pq, float *r,
+                     double *warp_part, double *mode0, const StepParams &p, const MeshDev &m, const double *za,
+                     const double *zbt, const double *zc, double dxi2, double dyi2, int incremental, cudaStream_t st);
 int warp_partials_per_plane(const StepParams &p);
 
 // diagnostics: out[0] = max|div| , out[1] = max CFL (already * dt), out[2] =
