@@ -41,8 +41,8 @@ WORKLOAD = "channel 512x384x256, Re_tau 1000, tanh stretch 2.0, Thomas, dt 1e-4,
 ALG_BYTES = {
     "fp64": {"rk_fused": 48, "rk1": 48, "rk2": 72, "calc_rhs": 32, "ppe_xfft_fwd": 16, "ppe_yfft_fwd": 16, "ppe_thomas": 24,
              "ppe_pdd": 40, "ppe_yfft_bwd": 16, "ppe_xfft_bwd": 16, "correct_force": 56},
-    "mixed": {"rk_fused": 48, "rk1": 36, "rk2": 60, "calc_rhs": 36, "ppe_xfft_fwd": 8, "ppe_yfft_fwd": 8, "ppe_thomas": 24,
-              "ppe_pdd": 32, "ppe_yfft_bwd": 8, "ppe_xfft_bwd": 36, "correct_force": 56},
+    "mixed": {"rk_fused": 56, "rk1": 36, "rk2": 68, "calc_rhs": 28, "ppe_xfft_fwd": 8, "ppe_yfft_fwd": 8, "ppe_thomas": 24,
+              "ppe_pdd": 32, "ppe_yfft_bwd": 8, "ppe_xfft_bwd": 40, "correct_force": 52},
 }
 # kernel launches per step (this library's kernels only)
 LAUNCHES = {"fp64": 8, "mixed": 9}

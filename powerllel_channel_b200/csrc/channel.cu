@@ -401,6 +401,16 @@ extern "C" int pl_channel_init_flow(pl_channel *c, uint64_t seed, double noise)
 
 static inline bool is_mixed(const pl_channel *c) { return c->cfg.precision == PL_MIXED; }
 
+// mixed path pressure prediction: the first two projections after the
+// initial field solve for the full pressure (the first one removes the
+// initial divergence, an outlier in time); then the increment over p_n, and
+// from the fourth on over the extrapolation 2 p_n - p_{n-1}.  The prediction
+// for the next projection is written by the solve's inverse x transform into
+// pb and rotated into pm.  For an incremental projection the RK kernel stores
+// u_hat = u* - dt G p_pred, so the residual is div(u_hat) / dt and the
+// correction uses the FP32 increment alone.
+static int mixed_incremental(const pl_channel *c) { return (c->incremental && c->nsolve >= 2) ? 1 : 0; }
+
 extern "C" int pl_phase_rk1(pl_channel *c)
 {
     int rc = is_mixed(c) ? launch_rk1_mixed(c->u, c->v, c->w, c->d1u, c->d1v, c->d1w, c->sp, c->m, c->stream)
@@ -414,7 +424,7 @@ extern "C" int pl_phase_rk2(pl_channel *c)
     int rc;
     if (is_mixed(c)) {
         rc = launch_rk2_mixed(c->u, c->v, c->w, c->d1u, c->d1v, c->d1w, c->ub, c->vb, c->wb, c->sp, c->m, c->ms,
-                              c->stream);
+                              c->pm, mixed_incremental(c), c->stream);
         std::swap(c->u, c->ub);
         std::swap(c->v, c->vb);
         std::swap(c->w, c->wb);
@@ -425,25 +435,13 @@ extern "C" int pl_phase_rk2(pl_channel *c)
     return rc;
 }
 
-// mixed path pressure prediction: the first two projections after the
-// initial field solve for the full pressure (the first one removes the
-// initial divergence, an outlier in time); then the increment over p_n, and
-// from the fourth on over the extrapolation 2 p_n - p_{n-1}.  The prediction
-// for the next projection is written by the solve's inverse x transform into
-// pb and rotated into pm, where the next residual reads it.
-static int mixed_incremental(const pl_channel *c) { return (c->incremental && c->nsolve >= 2) ? 1 : 0; }
-
 extern "C" int pl_phase_calc_rhs(pl_channel *c)
 {
     int rc;
-    if (is_mixed(c)) {
-        const double dx = c->cfg.lx / c->nx, dy = c->cfg.ly / c->ny;
-        rc = launch_rhs_mixed(c->u, c->v, c->w, c->pm, c->r32, c->plane_part, c->mode0, c->sp, c->m, c->ppe.d_a,
-                              c->ppe.d_bt, c->ppe.d_c, 1.0 / (dx * dx), 1.0 / (dy * dy), mixed_incremental(c),
-                              c->stream);
-    } else {
+    if (is_mixed(c))
+        rc = launch_rhs_mixed(c->u, c->v, c->w, c->r32, c->plane_part, c->mode0, c->sp, c->m, c->stream);
+    else
         rc = launch_calc_rhs_fp64(c->u, c->v, c->w, c->p, c->sp, c->m, c->stream);
-    }
     channel_mark(c, "calc_rhs");
     return rc;
 }
@@ -467,8 +465,11 @@ extern "C" int pl_phase_poisson(pl_channel *c)
 
 extern "C" int pl_phase_correct_force(pl_channel *c)
 {
-    const int rc = launch_correct_force_fp64(c->p, c->u, c->v, c->w, c->sp, c->m, c->cfg.is_forced[0], c->ms.scalar,
-                                             c->stream);
+    // mixed: the RK kernel applied -dt G p_pred, the increment remains
+    const int rc = is_mixed(c) ? launch_correct_force_f32(c->r32, c->u, c->v, c->w, c->sp, c->m,
+                                                          c->cfg.is_forced[0], c->ms.scalar, c->stream)
+                               : launch_correct_force_fp64(c->p, c->u, c->v, c->w, c->sp, c->m, c->cfg.is_forced[0],
+                                                           c->ms.scalar, c->stream);
     if (is_mixed(c)) {
         std::swap(c->pm, c->pb); // the prediction written by the solve
         c->nsolve++;
@@ -486,7 +487,8 @@ extern "C" int pl_phase_rk(pl_channel *c)
         if (!rc) rc = pl_phase_rk2(c);
         return rc;
     }
-    rc = is_mixed(c) ? launch_rk_fused_mixed(c->u, c->v, c->w, c->ub, c->vb, c->wb, c->sp, c->m, c->ms, c->stream)
+    rc = is_mixed(c) ? launch_rk_fused_mixed(c->u, c->v, c->w, c->ub, c->vb, c->wb, c->sp, c->m, c->ms, c->pm,
+                                             mixed_incremental(c), c->stream)
                      : launch_rk_fused_fp64(c->u, c->v, c->w, c->ub, c->vb, c->wb, c->sp, c->m, c->ms, c->stream);
     std::swap(c->u, c->ub);
     std::swap(c->v, c->vb);

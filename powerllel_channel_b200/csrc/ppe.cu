@@ -299,6 +299,8 @@ __global__ void __launch_bounds__(pf_x_threads<T>()) k_xfft_pf(const T *__restri
                 const T d0 = z.x * scale, d1 = z.y * scale;
                 if (sizeof(T) == 4 && pu.p) {
                     const size_t o = (size_t)k * N * ny + (size_t)2 * p0 * N + (size_t)2 * b * N + m;
+                    dst[(size_t)2 * b * N + m] = d0; // the increment itself, for the correction
+                    dst[(size_t)(2 * b + 1) * N + m] = d1;
                     pressure_update(pu, o, (double)d0);
                     pressure_update(pu, o + N, (double)d1);
                 } else {

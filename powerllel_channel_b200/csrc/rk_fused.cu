@@ -58,11 +58,12 @@ __device__ __forceinline__ Nb32 ring_nb(int x, int y, int s0, int sm, int sp)
     return n;
 }
 
-template <bool MIXED>
-__global__ void __launch_bounds__(FX *FY) k_rk_fused(const double *__restrict__ u, const double *__restrict__ v,
+template <bool MIXED, bool CRF>
+__global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double *__restrict__ u, const double *__restrict__ v,
                                                      const double *__restrict__ w, double *__restrict__ uo,
                                                      double *__restrict__ vo, double *__restrict__ wo, StepParams p,
-                                                     MeshDev m, MeanRed red, int kchunk)
+                                                     MeshDev m, MeanRed red, int kchunk,
+                                                     const double *__restrict__ pq, int pinc)
 {
     using R = typename RkTraits<MIXED>::R;
     constexpr int NS = RkTraits<MIXED>::NS;
@@ -98,11 +99,12 @@ __global__ void __launch_bounds__(FX *FY) k_rk_fused(const double *__restrict__ 
     auto produce = [&](int mq) {
         const int s0 = mq % NS, sm = (mq - 1) % NS, sp = (mq + 1) % NS;
         for (int q = tid; q < (FX + 2) * (FY + 2); q += nthr) {
+            const RhsConst<R> cst = rhs_const<R>(p, m, mq);
             const int x = q % (FX + 2) + 1, y = q / (FX + 2) + 1;
             const Nb32 n = ring_nb(x, y, s0, sm, sp);
             R ru, rv, rw;
-            momentum_rhs<R>(RingLoad<R>{ur}, RingLoad<R>{ur + FS}, RingLoad<R>{ur + 2 * FS}, n, mq, p, m, ru, rv,
-                            rw);
+            momentum_rhs_c<R, CRF>(RingLoad<R>{ur}, RingLoad<R>{ur + FS}, RingLoad<R>{ur + 2 * FS}, n, cst, ru, rv,
+                                   rw);
             if (MIXED) { // increments, and u1 = u + d1 for the stage-2 stencils
                 const R du = dt * ru, dv = dt * rv, dw = (mq == p.nz) ? (R)0 : dt * rw; // w1(nz) = 0 = w(nz)
                 qr[n.c] = du;
@@ -146,19 +148,36 @@ __global__ void __launch_bounds__(FX *FY) k_rk_fused(const double *__restrict__ 
     auto stage2 = [&](int kq) {
         const int s0 = kq % NS, sm = (kq - 1) % NS, sp = (kq + 1) % NS;
         const Nb32 n = ring_nb(tx + 2, ty + 2, s0, sm, sp);
-        R ru, rv, rw;
-        if (MIXED)
-            momentum_rhs<R>(RingLoad<R>{sr}, RingLoad<R>{sr + FS}, RingLoad<R>{sr + 2 * FS}, n, kq, p, m, ru, rv, rw);
-        else
-            momentum_rhs<R>(RingLoad<R>{qr}, RingLoad<R>{qr + FS}, RingLoad<R>{qr + 2 * FS}, n, kq, p, m, ru, rv,
-                            rw);
+        // global loads first, so their latency overlaps the stencil
         const size_t g = (size_t)(i0 + tx) + (size_t)p.nx * (j0 + ty) + sk * kq;
         const double uc = __ldg(u + g), vc = __ldg(v + g), wc = __ldg(w + g);
+        double q0 = 0.0, qxp = 0.0, qyp = 0.0, qzp = 0.0;
+        if (MIXED && pinc) { // u_hat = u* - dt G p_pred (FP64): its divergence is the increment's residual
+            const int ip = (i0 + tx == p.nx - 1) ? 0 : i0 + tx + 1, jp = (j0 + ty == p.ny - 1) ? 0 : j0 + ty + 1;
+            const size_t pc = g - sk;
+            q0 = __ldg(pq + pc);
+            qxp = __ldg(pq + (size_t)ip + (size_t)p.nx * (j0 + ty) + sk * (kq - 1));
+            qyp = __ldg(pq + (size_t)(i0 + tx) + (size_t)p.nx * jp + sk * (kq - 1));
+            qzp = (kq < p.nz) ? __ldg(pq + pc + sk) : q0;
+        }
+        const RhsConst<R> cst = rhs_const<R>(p, m, kq);
+        R ru, rv, rw;
+        if (MIXED)
+            momentum_rhs_c<R, CRF>(RingLoad<R>{sr}, RingLoad<R>{sr + FS}, RingLoad<R>{sr + 2 * FS}, n, cst, ru, rv,
+                                   rw);
+        else
+            momentum_rhs_c<R, CRF>(RingLoad<R>{qr}, RingLoad<R>{qr + FS}, RingLoad<R>{qr + 2 * FS}, n, cst, ru, rv,
+                                   rw);
         double nu, nv, nw;
         if (MIXED) {
             nu = ((uc + (double)qr[n.c]) + (double)(dt * ru) + uc) * 0.5;
             nv = ((vc + (double)qr[FS + n.c]) + (double)(dt * rv) + vc) * 0.5;
             nw = ((wc + (double)qr[2 * FS + n.c]) + (double)(dt * rw) + wc) * 0.5;
+            if (pinc) {
+                nu = nu - (qxp - q0) * (p.dt * p.dx_inv);
+                nv = nv - (qyp - q0) * (p.dt * p.dy_inv);
+                nw = nw - (qzp - q0) * p.dt * __ldg(m.dzc_inv + kq);
+            }
         } else {
             nu = ((double)qr[n.c] + p.dt * ((double)ru + p.fb[0]) + uc) * 0.5;
             nv = ((double)qr[FS + n.c] + p.dt * ((double)rv + p.fb[1]) + vc) * 0.5;
@@ -213,7 +232,8 @@ int rk_fused_blocks(const StepParams &p) { return (p.nx / FX) * (p.ny / FY) * fu
 
 template <bool MIXED>
 static int launch_rk_fused_t(const double *u, const double *v, const double *w, double *uo, double *vo, double *wo,
-                             const StepParams &p, const MeshDev &m, MeanState &ms, cudaStream_t st)
+                             const StepParams &p, const MeshDev &m, MeanState &ms, cudaStream_t st,
+                             const double *pq = nullptr, int pinc = 0)
 {
     if (!rk_fused_supported(p)) {
         set_error("fused RK kernel needs nx % 32 == 0 and ny % 8 == 0");
@@ -228,16 +248,14 @@ static int launch_rk_fused_t(const double *u, const double *v, const double *w, 
     }
     using R = typename RkTraits<MIXED>::R;
     const size_t shm = sizeof(R) * (MIXED ? 9 : 6) * RkTraits<MIXED>::NS * UPS;
-    static bool attr_set = false;
-    if (!attr_set) {
-        PL_CUDA_TRY(cudaFuncSetAttribute(k_rk_fused<MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
-        // prefer the largest shared-memory carve-out: several CTAs per SM
-        PL_CUDA_TRY(cudaFuncSetAttribute(k_rk_fused<MIXED>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                         (int)cudaSharedmemCarveoutMaxShared));
-        attr_set = true;
-    }
+    // u_crf == 0 (the channel's usual frame) drops the frame-velocity terms
+    auto kern = (p.u_crf != 0.0) ? k_rk_fused<MIXED, true> : k_rk_fused<MIXED, false>;
+    PL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+    // prefer the largest shared-memory carve-out: several CTAs per SM
+    PL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     (int)cudaSharedmemCarveoutMaxShared));
     MeanRed r{ms.partial, ms.counter, ms.scalar, (double)p.nx, (double)p.ny, ms.vel_force};
-    k_rk_fused<MIXED><<<grid, dim3(FX, FY), shm, st>>>(u, v, w, uo, vo, wo, p, m, r, kchunk);
+    kern<<<grid, dim3(FX, FY), shm, st>>>(u, v, w, uo, vo, wo, p, m, r, kchunk, pq, pinc);
     PL_CHECK_LAUNCH();
     return 0;
 }
@@ -249,9 +267,10 @@ int launch_rk_fused_fp64(const double *u, const double *v, const double *w, doub
 }
 
 int launch_rk_fused_mixed(const double *u, const double *v, const double *w, double *uo, double *vo, double *wo,
-                          const StepParams &p, const MeshDev &m, MeanState &ms, cudaStream_t st)
+                          const StepParams &p, const MeshDev &m, MeanState &ms, const double *pq, int pinc,
+                          cudaStream_t st)
 {
-    return launch_rk_fused_t<true>(u, v, w, uo, vo, wo, p, m, ms, st);
+    return launch_rk_fused_t<true>(u, v, w, uo, vo, wo, p, m, ms, st, pq, pinc);
 }
 
 } // namespace pl

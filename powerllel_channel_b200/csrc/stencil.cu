@@ -430,7 +430,8 @@ __global__ void __launch_bounds__(256) k_rk2_mixed(const double *__restrict__ u,
                                                    const double *__restrict__ w, const float *__restrict__ du,
                                                    const float *__restrict__ dv, const float *__restrict__ dw,
                                                    double *__restrict__ uo, double *__restrict__ vo,
-                                                   double *__restrict__ wo, StepParams p, MeshDev m, MeanRed red)
+                                                   double *__restrict__ wo, StepParams p, MeshDev m, MeanRed red,
+                                                   const double *__restrict__ pq, int pinc)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -443,32 +444,36 @@ __global__ void __launch_bounds__(256) k_rk2_mixed(const double *__restrict__ u,
         momentum_rhs<float>(LoadSum{u, du}, LoadSum{v, dv}, LoadSum{w, dw}, n, k, p, m, ru, rv, rw);
         const float dtf = (float)p.dt;
         const double uc = __ldg(u + n.c), vc = __ldg(v + n.c), wc = __ldg(w + n.c);
-        const double nu = ((uc + (double)__ldg(du + n.c)) + (double)(dtf * ru) + uc) * 0.5;
-        const double nv = ((vc + (double)__ldg(dv + n.c)) + (double)(dtf * rv) + vc) * 0.5;
+        double nu = ((uc + (double)__ldg(du + n.c)) + (double)(dtf * ru) + uc) * 0.5;
+        double nv = ((vc + (double)__ldg(dv + n.c)) + (double)(dtf * rv) + vc) * 0.5;
+        double nw = ((wc + (double)__ldg(dw + n.c)) + (double)(dtf * rw) + wc) * 0.5;
+        if (pinc) { // u_hat = u* - dt G p_pred (FP64): its divergence is the increment's residual
+            const size_t pc = n.c - sk;
+            const double q0 = __ldg(pq + pc), qxp = __ldg(pq + n.xp - sk), qyp = __ldg(pq + n.yp - sk);
+            const double qzp = (k < p.nz) ? __ldg(pq + pc + sk) : q0;
+            nu = nu - (qxp - q0) * (p.dt * p.dx_inv);
+            nv = nv - (qyp - q0) * (p.dt * p.dy_inv);
+            nw = nw - (qzp - q0) * p.dt * __ldg(m.dzc_inv + k);
+        }
         uo[n.c] = nu;
         vo[n.c] = nv;
-        if (k != p.nz) wo[n.c] = ((wc + (double)__ldg(dw + n.c)) + (double)(dtf * rw) + wc) * 0.5;
+        if (k != p.nz) wo[n.c] = nw;
         wall_fill<double>(uo, vo, wo, n.c, k, sk, p.nz, 0.0 - p.u_crf, nu, nv);
         su = nu * __ldg(m.dzflzi + k);
     }
     mean_reduce(su, red);
 }
 
-// Incremental pressure residual: r = div(u)/dt - L p_pred in FP64, stored in
-// FP32 (it is the small increment's right-hand side), with the FP64 plane
-// sums of r (the (kx,ky) = (0,0) right-hand side, solved in FP64).
-// p_pred = 2 p_n - p_{n-1} is the linear extrapolation of the pressure in
-// time: every FP32 error of the increment solve scales with |r|, and the
-// extrapolation makes r the second difference of p in time.  The previous
-// step's correction kernel stores p_pred (pq), so the residual reads one
-// FP64 pressure array.
-// L is exactly the operator the PPE inverts: periodic second differences
-// over dx^2, dy^2 and the tridiagonal row a, bt, c in z.
+// Mixed residual: r = div(u)/dt in FP64, stored in FP32 (the increment's
+// right-hand side), with the FP64 plane sums of r (the (kx,ky) = (0,0)
+// right-hand side, solved in FP64).  For an incremental projection u is
+// u_hat = u* - dt G p_pred (stored by the RK kernel), so r = div(u*)/dt -
+// L p_pred, L being exactly the operator the PPE inverts; p_pred = 2 p_n -
+// p_{n-1} makes r the second difference of p in time, and every FP32 error
+// of the increment solve scales with |r|.
 __global__ void __launch_bounds__(256) k_rhs_mixed(const double *__restrict__ u, const double *__restrict__ v,
-                                                   const double *__restrict__ w, const double *__restrict__ pq,
-                                                   float *__restrict__ r,
-                                                   double *__restrict__ warp_part, StepParams p, MeshDev m, ZOp z,
-                                                   double dxi2, double dyi2, int incremental)
+                                                   const double *__restrict__ w, float *__restrict__ r,
+                                                   double *__restrict__ warp_part, StepParams p, MeshDev m)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -478,19 +483,8 @@ __global__ void __launch_bounds__(256) k_rhs_mixed(const double *__restrict__ u,
     if (i < p.nx && j < p.ny) {
         const Nb n = neighbours(i, j, k, p.nx, p.ny);
         const double dti = 1.0 / p.dt, dtidxi = dti * p.dx_inv, dtidyi = dti * p.dy_inv;
-        double rhs = (__ldg(u + n.c) - __ldg(u + n.xm)) * dtidxi + (__ldg(v + n.c) - __ldg(v + n.ym)) * dtidyi +
-                     (__ldg(w + n.c) - __ldg(w + n.zm)) * dti * __ldg(m.dzf_inv + k);
-        if (incremental) {
-            const auto pp = [&](size_t q) { return __ldg(pq + q); };
-            const size_t pc = n.c - sk;
-            const double p0 = pp(pc);
-            double lp = (pp(n.xp - sk) - 2.0 * p0 + pp(n.xm - sk)) * dxi2 + (pp(n.yp - sk) - 2.0 * p0 + pp(n.ym - sk)) * dyi2;
-            const int kk = k - 1;
-            lp += __ldg(z.bt + kk) * p0;
-            if (kk > 0) lp += __ldg(z.a + kk) * pp(pc - sk);
-            if (kk < p.nz - 1) lp += __ldg(z.c + kk) * pp(pc + sk);
-            rhs -= lp;
-        }
+        const double rhs = (__ldg(u + n.c) - __ldg(u + n.xm)) * dtidxi + (__ldg(v + n.c) - __ldg(v + n.ym)) * dtidyi +
+                           (__ldg(w + n.c) - __ldg(w + n.zm)) * dti * __ldg(m.dzf_inv + k);
         r[n.c - sk] = (float)rhs;
         val = rhs;
     }
@@ -659,6 +653,14 @@ int launch_correct_force_fp64(const double *p_, double *u, double *v, double *w,
     return 0;
 }
 
+int launch_correct_force_f32(const float *p_, double *u, double *v, double *w, const StepParams &p, const MeshDev &m,
+                             int forced_x, const double *scalar, cudaStream_t st)
+{
+    k_correct_force<float><<<point_grid(p), point_block(), 0, st>>>(p_, u, v, w, p, m, forced_x, scalar);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
 int launch_rk1_mixed(const double *u, const double *v, const double *w, float *d1u, float *d1v, float *d1w,
                      const StepParams &p, const MeshDev &m, cudaStream_t st)
 {
@@ -669,25 +671,22 @@ int launch_rk1_mixed(const double *u, const double *v, const double *w, float *d
 
 int launch_rk2_mixed(const double *u, const double *v, const double *w, const float *d1u, const float *d1v,
                      const float *d1w, double *uo, double *vo, double *wo, const StepParams &p, const MeshDev &m,
-                     MeanState &ms, cudaStream_t st)
+                     MeanState &ms, const double *pq, int pinc, cudaStream_t st)
 {
     if (nblocks(p) > ms.max_blocks) {
         set_error("mean buffer too small");
         return -1;
     }
     MeanRed r{ms.partial, ms.counter, ms.scalar, (double)p.nx, (double)p.ny, ms.vel_force};
-    k_rk2_mixed<<<point_grid(p), point_block(), 0, st>>>(u, v, w, d1u, d1v, d1w, uo, vo, wo, p, m, r);
+    k_rk2_mixed<<<point_grid(p), point_block(), 0, st>>>(u, v, w, d1u, d1v, d1w, uo, vo, wo, p, m, r, pq, pinc);
     PL_CHECK_LAUNCH();
     return 0;
 }
 
-int launch_rhs_mixed(const double *u, const double *v, const double *w, const double *pq, float *r,
-                     double *warp_part, double *mode0, const StepParams &p, const MeshDev &m, const double *za,
-                     const double *zbt, const double *zc, double dxi2, double dyi2, int incremental, cudaStream_t st)
+int launch_rhs_mixed(const double *u, const double *v, const double *w, float *r, double *warp_part, double *mode0,
+                     const StepParams &p, const MeshDev &m, cudaStream_t st)
 {
-    ZOp z{za, zbt, zc};
-    k_rhs_mixed<<<point_grid(p), point_block(), 0, st>>>(u, v, w, pq, r, warp_part, p, m, z, dxi2, dyi2,
-                                                          incremental);
+    k_rhs_mixed<<<point_grid(p), point_block(), 0, st>>>(u, v, w, r, warp_part, p, m);
     PL_CHECK_LAUNCH();
     dim3 g = point_grid(p);
     const int nper = (int)(g.x * g.y) * (int)((point_block().x * point_block().y) / 32);

@@ -24,12 +24,6 @@ struct ReduceBuf {
     int max_blocks = 0;
 };
 
-// Mixed path: the z operator of the incremental pressure residual
-struct ZOp {
-    const double *a, *bt, *c; // per k (0-based interior), set_trid_coeff rows
-};
-
-
 // FP64 step kernels (one launch each)
 int launch_rk1_fp64(const double *u, const double *v, const double *w, double *u1, double *v1, double *w1,
                     const StepParams &p, const MeshDev &m, cudaStream_t st);
@@ -60,23 +54,29 @@ bool rk_fused_supported(const StepParams &p);
 int rk_fused_blocks(const StepParams &p);
 int launch_rk_fused_fp64(const double *u, const double *v, const double *w, double *uo, double *vo, double *wo,
                          const StepParams &p, const MeshDev &m, MeanState &ms, cudaStream_t st);
+// mixed: with pinc, u_hat = u* - dt G pq (pq: the pressure prediction,
+// interior-only layout) is stored, whose divergence / dt is the increment's
+// residual
 int launch_rk_fused_mixed(const double *u, const double *v, const double *w, double *uo, double *vo, double *wo,
-                          const StepParams &p, const MeshDev &m, MeanState &ms, cudaStream_t st);
+                          const StepParams &p, const MeshDev &m, MeanState &ms, const double *pq, int pinc,
+                          cudaStream_t st);
 
 int launch_rk2m_fp64(double *u, double *v, double *w, const double *u1, const double *v1, const double *w1,
                      const StepParams &p, const MeshDev &m, MeanState &ms, cudaStream_t st);
 int launch_correct_force_fp64(const double *p_, double *u, double *v, double *w, const StepParams &p,
                               const MeshDev &m, int forced_x, const double *scalar, cudaStream_t st);
+// the same with an FP32 pressure (the mixed path's increment)
+int launch_correct_force_f32(const float *p_, double *u, double *v, double *w, const StepParams &p,
+                             const MeshDev &m, int forced_x, const double *scalar, cudaStream_t st);
 
 // mixed precision: u, v, w, p in FP64; stage-1 increments and PPE in FP32
 int launch_rk1_mixed(const double *u, const double *v, const double *w, float *d1u, float *d1v, float *d1w,
                      const StepParams &p, const MeshDev &m, cudaStream_t st);
 int launch_rk2_mixed(const double *u, const double *v, const double *w, const float *d1u, const float *d1v,
                      const float *d1w, double *uo, double *vo, double *wo, const StepParams &p, const MeshDev &m,
-                     MeanState &ms, cudaStream_t st);
-int launch_rhs_mixed(const double *u, const double *v, const double *w, const double *pq, float *r,
-                     double *warp_part, double *mode0, const StepParams &p, const MeshDev &m, const double *za,
-                     const double *zbt, const double *zc, double dxi2, double dyi2, int incremental, cudaStream_t st);
+                     MeanState &ms, const double *pq, int pinc, cudaStream_t st);
+int launch_rhs_mixed(const double *u, const double *v, const double *w, float *r, double *warp_part, double *mode0,
+                     const StepParams &p, const MeshDev &m, cudaStream_t st);
 int warp_partials_per_plane(const StepParams &p);
 
 // diagnostics: out[0] = max|div| , out[1] = max CFL (already * dt), out[2] =

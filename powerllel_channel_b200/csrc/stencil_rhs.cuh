@@ -62,14 +62,40 @@ struct Nb32 {
     int c, xm, xp, ym, yp, zm, zp, xpym, xmyp, xpzm, xmzp, ypzm, ymzp;
 };
 
-template <typename TC, typename AU, typename AV, typename AW, typename NB = Nb>
-__device__ __forceinline__ void momentum_rhs(const AU &u, const AV &v, const AW &w, const NB &n, int k,
-                                             const StepParams &p, const MeshDev &m, TC &ru, TC &rv, TC &rw)
+// the run and mesh constants of one k-plane of the momentum stencil
+template <typename TC> struct RhsConst {
+    TC dx_inv, dy_inv, re_inv, u_crf;
+    TC dzf_k, dzf_kp, dzf_km, dzci_k, dzci_km, dzfi_k, dzfi_kp;
+};
+
+template <typename TC>
+__device__ __forceinline__ RhsConst<TC> rhs_const(const StepParams &p, const MeshDev &m, int k)
 {
-    const TC dx_inv = (TC)p.dx_inv, dy_inv = (TC)p.dy_inv, re_inv = (TC)p.re_inv, u_crf = (TC)p.u_crf;
-    const TC dzf_k = (TC)__ldg(m.dzf + k), dzf_kp = (TC)__ldg(m.dzf + k + 1), dzf_km = (TC)__ldg(m.dzf + k - 1);
-    const TC dzci_k = (TC)__ldg(m.dzc_inv + k), dzci_km = (TC)__ldg(m.dzc_inv + k - 1);
-    const TC dzfi_k = (TC)__ldg(m.dzf_inv + k), dzfi_kp = (TC)__ldg(m.dzf_inv + k + 1);
+    RhsConst<TC> c;
+    c.dx_inv = (TC)p.dx_inv;
+    c.dy_inv = (TC)p.dy_inv;
+    c.re_inv = (TC)p.re_inv;
+    c.u_crf = (TC)p.u_crf;
+    c.dzf_k = (TC)__ldg(m.dzf + k);
+    c.dzf_kp = (TC)__ldg(m.dzf + k + 1);
+    c.dzf_km = (TC)__ldg(m.dzf + k - 1);
+    c.dzci_k = (TC)__ldg(m.dzc_inv + k);
+    c.dzci_km = (TC)__ldg(m.dzc_inv + k - 1);
+    c.dzfi_k = (TC)__ldg(m.dzf_inv + k);
+    c.dzfi_kp = (TC)__ldg(m.dzf_inv + k + 1);
+    return c;
+}
+
+// the momentum right-hand sides with the plane's constants given; CRF false
+// drops the u_crf advection terms (exact when u_crf == 0: they add zero)
+template <typename TC, bool CRF, typename AU, typename AV, typename AW, typename NB>
+__device__ __forceinline__ void momentum_rhs_c(const AU &u, const AV &v, const AW &w, const NB &n,
+                                               const RhsConst<TC> &cst, TC &ru, TC &rv, TC &rw)
+{
+    const TC dx_inv = cst.dx_inv, dy_inv = cst.dy_inv, re_inv = cst.re_inv, u_crf = cst.u_crf;
+    const TC dzf_k = cst.dzf_k, dzf_kp = cst.dzf_kp, dzf_km = cst.dzf_km;
+    const TC dzci_k = cst.dzci_k, dzci_km = cst.dzci_km;
+    const TC dzfi_k = cst.dzfi_k, dzfi_kp = cst.dzfi_kp;
     const TC h = (TC)0.25, half = (TC)0.5;
 
     const TC uc = u(n.c), uxp = u(n.xp), uxm = u(n.xm), uyp = u(n.yp), uym = u(n.ym), uzp = u(n.zp), uzm = u(n.zm);
@@ -96,7 +122,7 @@ __device__ __forceinline__ void momentum_rhs(const AU &u, const AV &v, const AW 
     dqt = (uzp - uc) * dzci_k;
     dqb = (uc - uzm) * dzci_km;
     conv = h * ((ue * ue - uw * uw) * dx_inv + (un * vn - us * vs) * dy_inv + (ut * wt - ub * wb) * dzfi_k);
-    conv = conv + half * u_crf * (ue - uw) * dx_inv;
+    if (CRF) conv = conv + half * u_crf * (ue - uw) * dx_inv;
     visc = ((dqe - dqw) * dx_inv + (dqn - dqs) * dy_inv + (dqt - dqb) * dzfi_k) * re_inv;
     ru = visc - conv;
 
@@ -118,7 +144,7 @@ __device__ __forceinline__ void momentum_rhs(const AU &u, const AV &v, const AW 
     dqt = (vzp - vc) * dzci_k;
     dqb = (vc - vzm) * dzci_km;
     conv = h * ((ue * ve - uw * vw) * dx_inv + (vn * vn - vs * vs) * dy_inv + (wt * vt - wb * vb) * dzfi_k);
-    conv = conv + half * u_crf * (ve - vw) * dx_inv;
+    if (CRF) conv = conv + half * u_crf * (ve - vw) * dx_inv;
     visc = ((dqe - dqw) * dx_inv + (dqn - dqs) * dy_inv + (dqt - dqb) * dzfi_k) * re_inv;
     rv = visc - conv;
 
@@ -140,9 +166,16 @@ __device__ __forceinline__ void momentum_rhs(const AU &u, const AV &v, const AW 
     dqt = (wzp - wc) * dzfi_kp;
     dqb = (wc - wzm) * dzfi_k;
     conv = h * ((ue * we - uw * ww) * dx_inv + (vn * wn - vs * ws) * dy_inv + (wt * wt - wb * wb) * dzci_k);
-    conv = conv + half * u_crf * (we - ww) * dx_inv;
+    if (CRF) conv = conv + half * u_crf * (we - ww) * dx_inv;
     visc = ((dqe - dqw) * dx_inv + (dqn - dqs) * dy_inv + (dqt - dqb) * dzci_k) * re_inv;
     rw = visc - conv;
+}
+
+template <typename TC, typename AU, typename AV, typename AW, typename NB = Nb>
+__device__ __forceinline__ void momentum_rhs(const AU &u, const AV &v, const AW &w, const NB &n, int k,
+                                             const StepParams &p, const MeshDev &m, TC &ru, TC &rv, TC &rw)
+{
+    momentum_rhs_c<TC, true>(u, v, w, n, rhs_const<TC>(p, m, k), ru, rv, rw);
 }
 
 
