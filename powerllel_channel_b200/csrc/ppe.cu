@@ -184,6 +184,16 @@ __global__ void __launch_bounds__(256) k_xfft_ct(const T *__restrict__ in, size_
     }
 }
 
+// threadIdx.x through a volatile move: index arithmetic derived from it inside
+// a persistent loop is recomputed per iteration instead of being hoisted and
+// held in registers across the whole loop (which cost occupancy)
+__device__ __forceinline__ int opaque_tid()
+{
+    int t;
+    asm volatile("mov.u32 %0, %%tid.x;" : "=r"(t));
+    return t;
+}
+
 // pressure update of one point o (PressureUpdate in ppe.cuh); dp is the
 // FP32 increment widened to FP64
 __device__ __forceinline__ void pressure_update(const PressureUpdate &pu, size_t o, double dp)
@@ -262,6 +272,7 @@ __global__ void __launch_bounds__(pf_x_threads<T>()) k_xfft_pf(const T *__restri
     };
     if (blockIdx.x < total) fetch(blockIdx.x);
     for (int g = blockIdx.x; g < total; g += gridDim.x) {
+        const int tid = opaque_tid();
         const int k = g / gpk, p0 = (g % gpk) * NB, nb = min(NB, ny / 2 - p0);
         cp_async_wait<0>(); // this thread's copies of group g have landed
         __syncthreads();    // ... and everyone's; the previous group is done with buf

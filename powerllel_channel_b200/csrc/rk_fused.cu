@@ -38,6 +38,27 @@ template <typename R> struct RingLoad {
     __device__ __forceinline__ R operator()(int q) const { return a[q]; }
 };
 
+// Neighbour codes known at compile time (plane -1/0/+1, dx, dy): with the
+// three per-plane base pointers of RingLoad3 every stencil read becomes a
+// shared-memory load at a constant offset from one of three registers.
+__host__ __device__ constexpr int ring_enc(int pl, int dx, int dy) { return (pl + 1) * 1024 + (dy + 8) * 32 + (dx + 8); }
+struct RingNbC {
+    static constexpr int c = ring_enc(0, 0, 0), xm = ring_enc(0, -1, 0), xp = ring_enc(0, 1, 0), ym = ring_enc(0, 0, -1),
+                         yp = ring_enc(0, 0, 1), zm = ring_enc(-1, 0, 0), zp = ring_enc(1, 0, 0), xpym = ring_enc(0, 1, -1),
+                         xmyp = ring_enc(0, -1, 1), xpzm = ring_enc(-1, 1, 0), xmzp = ring_enc(1, -1, 0), ypzm = ring_enc(-1, 0, 1),
+                         ymzp = ring_enc(1, 0, -1);
+};
+
+template <typename R> struct RingLoad3 {
+    const R *pm, *pc, *pp; // the point's element in the planes below, at and above
+    __device__ __forceinline__ R operator()(int code) const
+    {
+        const int pl = code / 1024 - 1, dy = (code / 32) % 32 - 8, dx = code % 32 - 8;
+        const R *b = pl < 0 ? pm : (pl > 0 ? pp : pc);
+        return b[dx + dy * UW];
+    }
+};
+
 __device__ __forceinline__ Nb32 ring_nb(int x, int y, int s0, int sm, int sp)
 {
     Nb32 n;
@@ -102,9 +123,13 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
             const RhsConst<R> cst = rhs_const<R>(p, m, mq);
             const int x = q % (FX + 2) + 1, y = q / (FX + 2) + 1;
             const Nb32 n = ring_nb(x, y, s0, sm, sp);
+            const int xy = y * UW + x;
+            const int om = sm * UPS + xy, oc = s0 * UPS + xy, op = sp * UPS + xy;
             R ru, rv, rw;
-            momentum_rhs_c<R, CRF>(RingLoad<R>{ur}, RingLoad<R>{ur + FS}, RingLoad<R>{ur + 2 * FS}, n, cst, ru, rv,
-                                   rw);
+            momentum_rhs_c<R, CRF>(RingLoad3<R>{ur + om, ur + oc, ur + op},
+                                   RingLoad3<R>{ur + FS + om, ur + FS + oc, ur + FS + op},
+                                   RingLoad3<R>{ur + 2 * FS + om, ur + 2 * FS + oc, ur + 2 * FS + op}, RingNbC{}, cst,
+                                   ru, rv, rw);
             if (MIXED) { // increments, and u1 = u + d1 for the stage-2 stencils
                 const R du = dt * ru, dv = dt * rv, dw = (mq == p.nz) ? (R)0 : dt * rw; // w1(nz) = 0 = w(nz)
                 qr[n.c] = du;
@@ -162,12 +187,15 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
         }
         const RhsConst<R> cst = rhs_const<R>(p, m, kq);
         R ru, rv, rw;
-        if (MIXED)
-            momentum_rhs_c<R, CRF>(RingLoad<R>{sr}, RingLoad<R>{sr + FS}, RingLoad<R>{sr + 2 * FS}, n, cst, ru, rv,
-                                   rw);
-        else
-            momentum_rhs_c<R, CRF>(RingLoad<R>{qr}, RingLoad<R>{qr + FS}, RingLoad<R>{qr + 2 * FS}, n, cst, ru, rv,
-                                   rw);
+        {
+            const int xy = (ty + 2) * UW + tx + 2;
+            const int om = sm * UPS + xy, oc = s0 * UPS + xy, op = sp * UPS + xy;
+            const R *b = MIXED ? sr : qr;
+            momentum_rhs_c<R, CRF>(RingLoad3<R>{b + om, b + oc, b + op},
+                                   RingLoad3<R>{b + FS + om, b + FS + oc, b + FS + op},
+                                   RingLoad3<R>{b + 2 * FS + om, b + 2 * FS + oc, b + 2 * FS + op}, RingNbC{}, cst, ru,
+                                   rv, rw);
+        }
         double nu, nv, nw;
         if (MIXED) {
             nu = ((uc + (double)qr[n.c]) + (double)(dt * ru) + uc) * 0.5;
