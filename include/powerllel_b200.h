@@ -191,6 +191,53 @@ int pl_channel_kinetic_energy(pl_channel *c, double *ke);
 int pl_adjoint_ke_gradient(pl_channel *c, int nsteps, int every, double *ke, double *d_gu, double *d_gv,
                            double *d_gw, double grad_f[3]);
 
+
+/* ======================================================================
+ * 6. Statistics and monitors (src/mod_statistics.f90, src/mod_monitor.f90),
+ *    computed on the device; the reference writes them to text and HDF5
+ *    files, here the caller receives the values.
+ * ====================================================================== */
+/* bits of `which`, in the order of stat_which_var: */
+#define PL_STAT_U (1u << 0)
+#define PL_STAT_V (1u << 1)
+#define PL_STAT_W (1u << 2)
+#define PL_STAT_U2 (1u << 3)
+#define PL_STAT_V2 (1u << 4)
+#define PL_STAT_W2 (1u << 5)
+#define PL_STAT_UV (1u << 6)
+#define PL_STAT_UW (1u << 7)
+#define PL_STAT_VW (1u << 8)
+#define PL_STAT_P (1u << 9)
+#define PL_STAT_P2 (1u << 10)
+/* allocStat + initStat (mod_statistics.f90:21-124): device sums, nx*ny*nz
+ * doubles per selected variable, sampled from nt_init_stat every
+ * sample_interval steps */
+int pl_stat_enable(pl_channel *c, unsigned which, int nt_init_stat, int sample_interval);
+int pl_stat_init(pl_channel *c); /* initStat: zero the sums and the counters */
+/* calcStat (:126-192) at step nt: adds the cell-centred u (+u_crf), v, w,
+ * their products, p and p^2 when (nt - nt_init_stat) % sample_interval == 0 */
+int pl_stat_sample(pl_channel *c, int nt);
+/* stat_info: first step, last sampled step, number of samples */
+int pl_stat_info(pl_channel *c, int *nts, int *nte, int *nspl);
+/* one sum (which = 0..10, the bit index) to a host array [k][j][i], nx*ny*nz */
+int pl_stat_get(pl_channel *c, int which, double *host);
+int pl_stat_disable(pl_channel *c); /* freeStat */
+/* calcAndWriteSkf (mod_monitor.f90:264-296): wall 0 = bottom (k = 1), 1 = top
+ * (k = nz); tau_w = <re_inv (u + u_crf)> / (dzf/2), u_tau = sqrt(tau_w),
+ * cf = tau_w / (u_ref^2 / 2) */
+int pl_monitor_skin_friction(pl_channel *c, int wall, double *u_tau, double *cf);
+/* calcAndWriteForcing (:298-318): Mean_h of the forced components (0 for the
+ * others), u_crf added to u */
+int pl_monitor_forcing(pl_channel *c, double vel_mean[3]);
+/* extractAndWriteProbePoint (:197-219): u + u_crf, v, w, p at the 1-based
+ * point (i, j, k) */
+int pl_monitor_probe(pl_channel *c, int i, int j, int k, double out[4]);
+/* extractAndWriteRegion (:320-376): cell-centred u (+u_crf), v, w and p over
+ * ijk = {i0, i1, j0, j1, k0, k1} (1-based, inclusive, clipped to the domain
+ * as initMonitor does); host_uvwp receives the four arrays one after the
+ * other, each [k][j][i] over the clipped region */
+int pl_monitor_region(pl_channel *c, const int ijk[6], double *host_uvwp);
+
 #ifdef __cplusplus
 }
 #endif

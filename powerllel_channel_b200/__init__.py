@@ -102,6 +102,16 @@ def lib():
     L.pl_channel_set_body_force.argtypes = [C.c_void_p, _dp]
     L.pl_channel_kinetic_energy.argtypes = [C.c_void_p, _dp]
     L.pl_adjoint_ke_gradient.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp, C.c_void_p, C.c_void_p, C.c_void_p, _dp]
+    L.pl_stat_enable.argtypes = [C.c_void_p, C.c_uint, C.c_int, C.c_int]
+    L.pl_stat_init.argtypes = [C.c_void_p]
+    L.pl_stat_sample.argtypes = [C.c_void_p, C.c_int]
+    L.pl_stat_info.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.pl_stat_get.argtypes = [C.c_void_p, C.c_int, _dp]
+    L.pl_stat_disable.argtypes = [C.c_void_p]
+    L.pl_monitor_skin_friction.argtypes = [C.c_void_p, C.c_int, _dp, _dp]
+    L.pl_monitor_forcing.argtypes = [C.c_void_p, _dp]
+    L.pl_monitor_probe.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, _dp]
+    L.pl_monitor_region.argtypes = [C.c_void_p, C.POINTER(C.c_int), _dp]
     for name in ("pl_phase_rk", "pl_phase_rk1", "pl_phase_rk2", "pl_phase_calc_rhs", "pl_phase_poisson", "pl_phase_correct_force"):
         getattr(L, name).argtypes = [C.c_void_p]
     _lib = L
@@ -317,6 +327,58 @@ class Channel:
         _check(lib().pl_adjoint_ke_gradient(self._h, int(nsteps), int(every), _ptr(ke), C.c_void_p(d_gu),
                                             C.c_void_p(d_gv), C.c_void_p(d_gw), _ptr(gf)), "pl_adjoint_ke_gradient")
         return float(ke[0]), gf
+
+    # statistics (mod_statistics.f90) -------------------------------------
+    STAT_NAMES = ("u", "v", "w", "u2", "v2", "w2", "uv", "uw", "vw", "p", "p2")
+
+    def stat_enable(self, names=STAT_NAMES, nt_init_stat: int = 0, sample_interval: int = 1) -> None:
+        mask = 0
+        for n in names:
+            mask |= 1 << self.STAT_NAMES.index(n)
+        _check(lib().pl_stat_enable(self._h, mask, int(nt_init_stat), int(sample_interval)), "pl_stat_enable")
+
+    def stat_sample(self, nt: int) -> None:
+        _check(lib().pl_stat_sample(self._h, int(nt)), "pl_stat_sample")
+
+    def stat_info(self):
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        _check(lib().pl_stat_info(self._h, C.byref(a), C.byref(b), C.byref(c)), "pl_stat_info")
+        return a.value, b.value, c.value
+
+    def stat_get(self, name: str) -> np.ndarray:
+        out = np.zeros((self.cfg.nz, self.cfg.ny, self.cfg.nx))
+        _check(lib().pl_stat_get(self._h, self.STAT_NAMES.index(name), _ptr(out)), "pl_stat_get")
+        return out
+
+    def stat_disable(self) -> None:
+        _check(lib().pl_stat_disable(self._h), "pl_stat_disable")
+
+    # monitors (mod_monitor.f90) ------------------------------------------
+    def skin_friction(self, wall: int):
+        ut, cf = np.zeros(1), np.zeros(1)
+        _check(lib().pl_monitor_skin_friction(self._h, int(wall), _ptr(ut), _ptr(cf)), "pl_monitor_skin_friction")
+        return float(ut[0]), float(cf[0])
+
+    def forcing_means(self) -> np.ndarray:
+        out = np.zeros(3)
+        _check(lib().pl_monitor_forcing(self._h, _ptr(out)), "pl_monitor_forcing")
+        return out
+
+    def probe(self, i: int, j: int, k: int) -> np.ndarray:
+        out = np.zeros(4)
+        _check(lib().pl_monitor_probe(self._h, int(i), int(j), int(k), _ptr(out)), "pl_monitor_probe")
+        return out
+
+    def region(self, ijk):
+        """cell-centred (u, v, w, p) over ijk = (i0, i1, j0, j1, k0, k1), 1-based inclusive, clipped"""
+        c = self.cfg
+        i0, i1 = max(ijk[0], 1), min(ijk[1], c.nx)
+        j0, j1 = max(ijk[2], 1), min(ijk[3], c.ny)
+        k0, k1 = max(ijk[4], 1), min(ijk[5], c.nz)
+        out = np.zeros((4, max(k1 - k0 + 1, 0), max(j1 - j0 + 1, 0), max(i1 - i0 + 1, 0)))
+        arr = (C.c_int * 6)(*[int(x) for x in ijk])
+        _check(lib().pl_monitor_region(self._h, arr, _ptr(out)), "pl_monitor_region")
+        return out
 
     def field_ptr(self, which: int) -> int:
         return lib().pl_channel_field(self._h, which)

@@ -231,6 +231,7 @@ static void build_mesh(pl_channel *c)
 
 static void channel_free(pl_channel *c)
 {
+    pl_stat_disable(c);
     cudaFree(c->d_mesh);
     cudaFree(c->u);
     cudaFree(c->v);

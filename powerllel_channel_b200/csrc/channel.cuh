@@ -41,6 +41,7 @@ struct pl_channel {
     long long *d_dipart = nullptr;
     int max_blocks = 0;
     cudaStream_t stream = nullptr;
+    void *stats = nullptr; // device statistics (monitor.cu), when enabled
     // profiling marks (pl_channel_profile)
     std::vector<cudaEvent_t> *prof_events = nullptr;
     std::vector<std::string> *prof_names = nullptr;
