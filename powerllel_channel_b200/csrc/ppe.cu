@@ -399,7 +399,9 @@ __device__ __forceinline__ size_t trid_class(int px, int py, const TridDev &t)
     return (size_t)ix + (size_t)t.ncx * jy;
 }
 
-constexpr int TRID_UNROLL = 8;
+// rows per load batch of the Thomas sweeps: measured best at 4 for FP64
+// data (in place) and 8 for the FP32 input with the FP64 sweep scratch
+template <typename T> __host__ __device__ constexpr int trid_unroll() { return sizeof(T) == 8 ? 4 : 8; }
 
 // Thomas on rows [k0, k0+ke) of one column.  Reads the right-hand side from
 // `xin` (type T), keeps the forward-swept values in `xs` (double; may alias
@@ -408,6 +410,7 @@ template <typename T>
 __device__ __forceinline__ void thomas_column(const T *xin, double *xs, T *xout, size_t col, size_t cls,
                                               size_t stride, size_t cstride, int k0, int ke, const TridDev &t)
 {
+    constexpr int TRID_UNROLL = trid_unroll<T>();
     // forward elimination: x_k -= (a_k / b_{k-1}) x_{k-1}   (ssolve_trid :319-330)
     double xp = (double)xin[col + (size_t)k0 * stride];
     xs[col + (size_t)k0 * stride] = xp;
