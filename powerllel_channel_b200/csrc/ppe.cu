@@ -229,7 +229,8 @@ template <typename V, int N> __host__ __device__ constexpr int pf_y_cols()
 
 // threads per CTA of the persistent x kernel, and line pairs per group: one
 // radix-8 stage of a group is one butterfly per thread
-template <typename T> __host__ __device__ constexpr int pf_x_threads() { return sizeof(T) == 8 ? 128 : 256; }
+template <typename T> __host__ __device__ constexpr int pf_y_threads() { return 256; }
+template <typename T> __host__ __device__ constexpr int pf_x_threads() { return sizeof(T) == 8 ? 64 : 256; }
 template <typename T, int N> __host__ __device__ constexpr int pf_x_lines()
 {
     return (pf_x_threads<T>() * 8 / N) < 1 ? 1 : pf_x_threads<T>() * 8 / N;
@@ -325,10 +326,11 @@ __global__ void __launch_bounds__(pf_x_threads<T>()) k_xfft_pf(const T *__restri
 }
 
 template <typename T, int N, bool FWD>
-__global__ void __launch_bounds__(256) k_yfft_pf(T *__restrict__ data, const typename cplx_of<T>::type *__restrict__ twg,
+__global__ void __launch_bounds__(pf_y_threads<T>()) k_yfft_pf(T *__restrict__ data, const typename cplx_of<T>::type *__restrict__ twg,
                                                  int nx, int total)
 {
     using V = typename cplx_of<T>::type;
+    constexpr int NT = pf_y_threads<T>();
     constexpr int W = pf_y_cols<V, N>(), BUF = (fpad_elems<V>(W * N) + 1) / 2 * 2, RAW = W * N;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int ncol = nx / 2;
@@ -337,11 +339,11 @@ __global__ void __launch_bounds__(256) k_yfft_pf(T *__restrict__ data, const typ
     V *tw = stage + RAW;
     const int tid = threadIdx.x;
     const int gpk = (ncol + W - 1) / W;
-    ct_build_twiddles<V, N, 256>(twg, tw, tid);
+    ct_build_twiddles<V, N, NT>(twg, tw, tid);
     auto fetch = [&](int g) {
         const int k = g / gpk, c0 = (g % gpk) * W, nb = min(W, ncol - c0);
         const V *plane = reinterpret_cast<const V *>(data) + (size_t)k * N * ncol;
-        for (int e = tid; e < RAW; e += 256) {
+        for (int e = tid; e < RAW; e += NT) {
             const int c = e % W, m = e / W;
             if (c < nb) {
                 if (sizeof(V) == 16)
@@ -358,7 +360,7 @@ __global__ void __launch_bounds__(256) k_yfft_pf(T *__restrict__ data, const typ
         V *plane = reinterpret_cast<V *>(data) + (size_t)k * N * ncol;
         cp_async_wait<0>();
         __syncthreads();
-        for (int e = tid; e < RAW; e += 256) {
+        for (int e = tid; e < RAW; e += NT) {
             const int c = e % W, m = e / W;
             if (c < nb) {
                 if (FWD)
@@ -369,8 +371,8 @@ __global__ void __launch_bounds__(256) k_yfft_pf(T *__restrict__ data, const typ
         }
         __syncthreads();
         if (g + (int)gridDim.x < total) fetch(g + gridDim.x);
-        ct_batch_ip<V, FWD, true, N, W, W, 1, 256>(buf, nb, tw, tid);
-        for (int e = tid; e < RAW; e += 256) {
+        ct_batch_ip<V, FWD, true, N, W, W, 1, NT>(buf, nb, tw, tid);
+        for (int e = tid; e < RAW; e += NT) {
             const int c = e % W, m = e / W;
             if (c < nb) {
                 if (FWD) {
@@ -777,7 +779,8 @@ template <typename T, int N, bool FWD> static int launch_y_ct(const Ppe *s, T *d
         PL_CUDA_TRY(cudaFuncSetAttribute(k_yfft_pf<T, N, FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
     const V *tw = reinterpret_cast<const V *>(sizeof(T) == 8 ? (const void *)s->d_twy64 : (const void *)s->d_twy32);
     const int total = ((s->nx / 2 + W - 1) / W) * s->nz;
-    k_yfft_pf<T, N, FWD><<<persistent_grid(k_yfft_pf<T, N, FWD>, shm, total), 256, shm, st>>>(data, tw, s->nx, total);
+    k_yfft_pf<T, N, FWD><<<persistent_grid(k_yfft_pf<T, N, FWD>, shm, total, pf_y_threads<T>()), pf_y_threads<T>(), shm,
+                           st>>>(data, tw, s->nx, total);
     PL_CHECK_LAUNCH();
     return 0;
 }
