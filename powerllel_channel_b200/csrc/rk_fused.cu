@@ -218,12 +218,17 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
         su += nu * __ldg(m.dzflzi + kq);
     };
 
+    // Two barriers per plane: produce(mq) reads u planes mq-1..mq+1; then
+    // stage2(mq-1), which reads only the stage-1 rings and global memory,
+    // runs together with the load of u plane mq+2 into the slot of plane
+    // mq-1 that produce(mq) has finished with, so the load's latency hides
+    // behind the stage-2 arithmetic.
     const int mstart = max(kbeg - 1, 1), mend = min(kend + 1, p.nz);
     load_u_plane(mstart - 1);
     load_u_plane(mstart);
+    load_u_plane(mstart + 1);
+    __syncthreads();
     for (int mq = mstart; mq <= mend; mq++) {
-        load_u_plane(mq + 1);
-        __syncthreads();
         produce(mq);
         __syncthreads();
         if (mq == 1) {
@@ -239,6 +244,7 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
             __syncthreads();
             if (p.nz >= kbeg && p.nz <= kend) stage2(p.nz);
         }
+        if (mq + 2 <= mend + 1) load_u_plane(mq + 2);
         __syncthreads();
     }
     mean_reduce(su, red);
