@@ -458,6 +458,35 @@ __device__ __forceinline__ void ct_batch_ip(V *buf, int nb, const V *tws, int ti
     }
 }
 
+// The first stage (NS = 1, no twiddles) with its inputs produced by `in(b, m)`
+// (line b, element m) instead of read from the work buffer: the kernels
+// read their staged raw data through it, pairing the two real lines (and,
+// for the inverse, merging the half-complex spectra) on the fly.  Writes
+// the stage's output to buf; the caller then runs the stages from S = 1.
+template <typename V, bool FWD, bool BF, int N, int NB, int SM, int SB, int NTHR, typename IN>
+__device__ __forceinline__ void ct_first_stage(V *__restrict__ buf, int nb, const IN &in, int tid)
+{
+    constexpr int R = ct_radix(N, 0), NBF = N / R, TOTAL = NBF * NB;
+    constexpr int ITERS = (TOTAL + NTHR - 1) / NTHR;
+#pragma unroll
+    for (int it = 0; it < ITERS; it++) {
+        const int q = tid + it * NTHR;
+        if (TOTAL % NTHR == 0 || q < TOTAL) {
+            const int b = BF ? q % NB : q / NBF;
+            const int j = BF ? q / NB : q % NBF;
+            if (b < nb) {
+                V a[R];
+#pragma unroll
+                for (int r = 0; r < R; r++) a[r] = in(b, j + r * NBF);
+                dft_r<V, FWD, R>(a);
+                const int base = b * SB;
+#pragma unroll
+                for (int r = 0; r < R; r++) buf[fpad<V>(base + (j * R + r) * SM)] = a[r];
+            }
+        }
+    }
+}
+
 // Asynchronous global -> shared copies (cp.async; completion is awaited with
 // cp.async.wait_group, a hardware wait on this thread's own copies).
 __device__ __forceinline__ void cp_async_8(void *smem, const void *gmem)

@@ -277,8 +277,8 @@ __global__ void __launch_bounds__(pf_x_threads<T>()) k_xfft_pf(const T *__restri
         const int k = g / gpk, p0 = (g % gpk) * NB, nb = min(NB, ny / 2 - p0);
         cp_async_wait<0>(); // this thread's copies of group g have landed
         __syncthreads();    // ... and everyone's; the previous group is done with buf
-        for (int e = tid; e < nb * N; e += NT) {
-            const int m = e % N, b = e / N;
+        // first stage straight from the staged rows: line b pairs rows 2b, 2b+1
+        auto in = [&](int b, int m) {
             const T *r0 = stage + 2 * b * N, *r1 = r0 + N;
             V z;
             if (FWD) {
@@ -293,11 +293,12 @@ __global__ void __launch_bounds__(pf_x_threads<T>()) k_xfft_pf(const T *__restri
                 Q.y = r1[mc];
                 z = merge_hc(P, Q, m, N);
             }
-            buf[fpad<V>(b * N + m)] = z;
-        }
+            return z;
+        };
+        ct_first_stage<V, FWD, false, N, NB, 1, N, NT>(buf, nb, in, tid);
         __syncthreads();
         if (g + (int)gridDim.x < total) fetch(g + gridDim.x);
-        ct_batch_ip<V, FWD, false, N, NB, 1, N, NT>(buf, nb, tw, tid);
+        ct_batch_ip<V, FWD, false, N, NB, 1, N, NT, 1>(buf, nb, tw, tid);
         T *dst = out + (size_t)k * N * ny + (size_t)2 * p0 * N;
         for (int e = tid; e < nb * N; e += NT) {
             const int m = e % N, b = e / N;
@@ -360,18 +361,15 @@ __global__ void __launch_bounds__(pf_y_threads<T>()) k_yfft_pf(T *__restrict__ d
         V *plane = reinterpret_cast<V *>(data) + (size_t)k * N * ncol;
         cp_async_wait<0>();
         __syncthreads();
-        for (int e = tid; e < RAW; e += NT) {
-            const int c = e % W, m = e / W;
-            if (c < nb) {
-                if (FWD)
-                    buf[fpad<V>(m * W + c)] = stage[e];
-                else
-                    buf[fpad<V>(m * W + c)] = merge_hc(stage[e], stage[(m == 0 ? 0 : N - m) * W + c], m, N);
-            }
-        }
+        // first stage straight from the staged columns ([m][c])
+        auto in = [&](int c, int m) {
+            if (FWD) return stage[m * W + c];
+            return merge_hc(stage[m * W + c], stage[(m == 0 ? 0 : N - m) * W + c], m, N);
+        };
+        ct_first_stage<V, FWD, true, N, W, W, 1, NT>(buf, nb, in, tid);
         __syncthreads();
         if (g + (int)gridDim.x < total) fetch(g + gridDim.x);
-        ct_batch_ip<V, FWD, true, N, W, W, 1, NT>(buf, nb, tw, tid);
+        ct_batch_ip<V, FWD, true, N, W, W, 1, NT, 1>(buf, nb, tw, tid);
         for (int e = tid; e < RAW; e += NT) {
             const int c = e % W, m = e / W;
             if (c < nb) {
