@@ -446,15 +446,64 @@ __device__ __forceinline__ void ct_stage_ip(V *buf, int nb, const V *__restrict_
     }
 }
 
-// All stages from S on, in place in buf.  Ends with a __syncthreads().
-template <typename V, bool FWD, bool BF, int N, int NB, int SM, int SB, int NTHR, int S = 0>
+// number of stages of a length-n transform
+__host__ __device__ constexpr int ct_nstages(int n)
+{
+    int s = 0;
+    while (ct_radix(n, s) != 0) s++;
+    return s;
+}
+
+// Stages S .. SEND-1 (all remaining stages by default), in place in buf.
+// Ends with a __syncthreads().
+template <typename V, bool FWD, bool BF, int N, int NB, int SM, int SB, int NTHR, int S = 0,
+          int SEND = ct_nstages(N)>
 __device__ __forceinline__ void ct_batch_ip(V *buf, int nb, const V *tws, int tid)
 {
-    if constexpr (ct_radix(N, S) != 0) {
+    if constexpr (S < SEND) {
         ct_stage_ip<V, FWD, BF, N, ct_radix(N, S), ct_ns(N, S), NB, SM, SB, NTHR>(
             buf, nb, tws + (S > 0 ? ct_twoff(N, S) : 0), tid);
         __syncthreads();
-        ct_batch_ip<V, FWD, BF, N, NB, SM, SB, NTHR, S + 1>(buf, nb, tws, tid);
+        ct_batch_ip<V, FWD, BF, N, NB, SM, SB, NTHR, S + 1, SEND>(buf, nb, tws, tid);
+    }
+}
+
+// The last stage, its outputs handed to `out(b, m, value)` (line b, element
+// m) instead of stored back: the inverse kernels write them to global memory
+// straight from registers.  For a fixed r consecutive threads hold
+// consecutive m (BF = false) or consecutive b (BF = true).  Reads buf only,
+// so it needs no barrier of its own; the caller's next write to buf must
+// follow a __syncthreads().
+template <typename V, bool FWD, bool BF, int N, int NB, int SM, int SB, int NTHR, typename OUT>
+__device__ __forceinline__ void ct_last_stage(const V *buf, int nb, const V *tws, int tid, const OUT &out)
+{
+    constexpr int S = ct_nstages(N) - 1, R = ct_radix(N, S), NS = ct_ns(N, S);
+    constexpr int NBF = N / R, TOTAL = NBF * NB;
+    constexpr int ITERS = (TOTAL + NTHR - 1) / NTHR;
+    static_assert(S > 0 && NS * R == N, "last stage of a multi-stage transform");
+    tws += ct_twoff(N, S);
+#pragma unroll
+    for (int it = 0; it < ITERS; it++) {
+        const int q = tid + it * NTHR;
+        if (TOTAL % NTHR == 0 || q < TOTAL) {
+            const int b = BF ? q % NB : q / NBF;
+            const int j = BF ? q / NB : q % NBF; // j < NS: output index j + r NS
+            if (b < nb) {
+                const int base = b * SB;
+                V a[R];
+#pragma unroll
+                for (int r = 0; r < R; r++) a[r] = buf[fpad<V>(base + (j + r * NBF) * SM)];
+#pragma unroll
+                for (int r = 1; r < R; r++) {
+                    V w = tws[(r - 1) * NS + j];
+                    if (!FWD) w.y = -w.y;
+                    a[r] = cmul(a[r], w);
+                }
+                dft_r<V, FWD, R>(a);
+#pragma unroll
+                for (int r = 0; r < R; r++) out(b, j + r * NS, a[r]);
+            }
+        }
     }
 }
 

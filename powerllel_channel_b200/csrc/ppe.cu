@@ -298,29 +298,30 @@ __global__ void __launch_bounds__(pf_x_threads<T>()) k_xfft_pf(const T *__restri
         ct_first_stage<V, FWD, false, N, NB, 1, N, NT>(buf, nb, in, tid);
         __syncthreads();
         if (g + (int)gridDim.x < total) fetch(g + gridDim.x);
-        ct_batch_ip<V, FWD, false, N, NB, 1, N, NT, 1>(buf, nb, tw, tid);
         T *dst = out + (size_t)k * N * ny + (size_t)2 * p0 * N;
-        for (int e = tid; e < nb * N; e += NT) {
-            const int m = e % N, b = e / N;
-            if (FWD) {
+        if constexpr (FWD) {
+            ct_batch_ip<V, FWD, false, N, NB, 1, N, NT, 1>(buf, nb, tw, tid);
+            for (int e = tid; e < nb * N; e += NT) {
+                const int m = e % N, b = e / N;
                 V A = buf[fpad<V>(b * N + m)], Bc = buf[fpad<V>(b * N + (m == 0 ? 0 : N - m))];
                 V h = split_hc(A, Bc, m, N);
                 dst[(size_t)2 * b * N + m] = h.x;
                 dst[(size_t)(2 * b + 1) * N + m] = h.y;
-            } else {
-                V z = buf[fpad<V>(b * N + m)];
+            }
+        } else {
+            ct_batch_ip<V, FWD, false, N, NB, 1, N, NT, 1, ct_nstages(N) - 1>(buf, nb, tw, tid);
+            // the last stage writes the two real rows of line b from registers
+            auto put = [&](int b, int m, V z) {
                 const T d0 = z.x * scale, d1 = z.y * scale;
+                dst[(size_t)2 * b * N + m] = d0; // mixed: the increment itself, for the correction
+                dst[(size_t)(2 * b + 1) * N + m] = d1;
                 if (sizeof(T) == 4 && pu.p) {
                     const size_t o = (size_t)k * N * ny + (size_t)2 * p0 * N + (size_t)2 * b * N + m;
-                    dst[(size_t)2 * b * N + m] = d0; // the increment itself, for the correction
-                    dst[(size_t)(2 * b + 1) * N + m] = d1;
                     pressure_update(pu, o, (double)d0);
                     pressure_update(pu, o + N, (double)d1);
-                } else {
-                    dst[(size_t)2 * b * N + m] = d0;
-                    dst[(size_t)(2 * b + 1) * N + m] = d1;
                 }
-            }
+            };
+            ct_last_stage<V, FWD, false, N, NB, 1, N, NT>(buf, nb, tw, tid, put);
         }
     }
     cp_async_wait<0>();
@@ -369,17 +370,19 @@ __global__ void __launch_bounds__(pf_y_threads<T>()) k_yfft_pf(T *__restrict__ d
         ct_first_stage<V, FWD, true, N, W, W, 1, NT>(buf, nb, in, tid);
         __syncthreads();
         if (g + (int)gridDim.x < total) fetch(g + gridDim.x);
-        ct_batch_ip<V, FWD, true, N, W, W, 1, NT, 1>(buf, nb, tw, tid);
-        for (int e = tid; e < RAW; e += NT) {
-            const int c = e % W, m = e / W;
-            if (c < nb) {
-                if (FWD) {
+        if constexpr (FWD) {
+            ct_batch_ip<V, FWD, true, N, W, W, 1, NT, 1>(buf, nb, tw, tid);
+            for (int e = tid; e < RAW; e += NT) {
+                const int c = e % W, m = e / W;
+                if (c < nb) {
                     V A = buf[fpad<V>(m * W + c)], Bc = buf[fpad<V>((m == 0 ? 0 : N - m) * W + c)];
                     plane[(size_t)m * ncol + c0 + c] = split_hc(A, Bc, m, N);
-                } else {
-                    plane[(size_t)m * ncol + c0 + c] = buf[fpad<V>(m * W + c)];
                 }
             }
+        } else {
+            ct_batch_ip<V, FWD, true, N, W, W, 1, NT, 1, ct_nstages(N) - 1>(buf, nb, tw, tid);
+            auto put = [&](int c, int m, V z) { plane[(size_t)m * ncol + c0 + c] = z; };
+            ct_last_stage<V, FWD, true, N, W, W, 1, NT>(buf, nb, tw, tid, put);
         }
     }
     cp_async_wait<0>();
