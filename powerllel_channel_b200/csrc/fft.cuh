@@ -536,6 +536,52 @@ __device__ __forceinline__ void ct_first_stage(V *__restrict__ buf, int nb, cons
     }
 }
 
+// The last stage of a forward transform, its outputs handed in mirror
+// pairs to `out(b, m, Z_m, Z_{N-m})` (line b; Z_N = Z_0) so that the
+// half-complex split runs from registers.  Output m = j + r NS of butterfly
+// j has its mirror N - m = (NS - j) + (R-1-r) NS in butterfly NS - j, so one
+// thread takes the butterflies {t, NS - t} for t = 1 .. NS/2-1, and the
+// thread t = 0 the two self-mirrored ones {0, NS/2}.  Reads buf only.
+template <typename V, bool FWD, bool BF, int N, int NB, int SM, int SB, int NTHR, typename OUT>
+__device__ __forceinline__ void ct_last_stage_pairs(const V *buf, int nb, const V *tws, int tid, const OUT &out)
+{
+    constexpr int S = ct_nstages(N) - 1, R = ct_radix(N, S), NS = ct_ns(N, S), H = NS / 2;
+    constexpr int TOTAL = H * NB;
+    constexpr int ITERS = (TOTAL + NTHR - 1) / NTHR;
+    static_assert(S > 0 && NS * R == N && NS % 2 == 0, "last stage of a multi-stage even transform");
+    tws += ct_twoff(N, S);
+    auto butterfly = [&](int base, int j, V *a) {
+#pragma unroll
+        for (int r = 0; r < R; r++) a[r] = buf[fpad<V>(base + (j + r * NS) * SM)];
+#pragma unroll
+        for (int r = 1; r < R; r++) {
+            V w = tws[(r - 1) * NS + j];
+            if (!FWD) w.y = -w.y;
+            a[r] = cmul(a[r], w);
+        }
+        dft_r<V, FWD, R>(a);
+    };
+#pragma unroll
+    for (int it = 0; it < ITERS; it++) {
+        const int q = tid + it * NTHR;
+        if (TOTAL % NTHR == 0 || q < TOTAL) {
+            const int b = BF ? q % NB : q / H;
+            const int t = BF ? q / NB : q % H;
+            if (b < nb) {
+                const int base = b * SB, ja = t, jb = (t == 0) ? H : NS - t;
+                V xa[R], xb[R];
+                butterfly(base, ja, xa);
+                butterfly(base, jb, xb);
+#pragma unroll
+                for (int r = 0; r < R; r++) {
+                    out(b, ja + r * NS, xa[r], (t == 0) ? xa[(R - r) % R] : xb[R - 1 - r]);
+                    out(b, jb + r * NS, xb[r], (t == 0) ? xb[R - 1 - r] : xa[R - 1 - r]);
+                }
+            }
+        }
+    }
+}
+
 // Asynchronous global -> shared copies (cp.async; completion is awaited with
 // cp.async.wait_group, a hardware wait on this thread's own copies).
 __device__ __forceinline__ void cp_async_8(void *smem, const void *gmem)

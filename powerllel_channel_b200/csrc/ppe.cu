@@ -300,14 +300,14 @@ __global__ void __launch_bounds__(pf_x_threads<T>()) k_xfft_pf(const T *__restri
         if (g + (int)gridDim.x < total) fetch(g + gridDim.x);
         T *dst = out + (size_t)k * N * ny + (size_t)2 * p0 * N;
         if constexpr (FWD) {
-            ct_batch_ip<V, FWD, false, N, NB, 1, N, NT, 1>(buf, nb, tw, tid);
-            for (int e = tid; e < nb * N; e += NT) {
-                const int m = e % N, b = e / N;
-                V A = buf[fpad<V>(b * N + m)], Bc = buf[fpad<V>(b * N + (m == 0 ? 0 : N - m))];
-                V h = split_hc(A, Bc, m, N);
+            ct_batch_ip<V, FWD, false, N, NB, 1, N, NT, 1, ct_nstages(N) - 1>(buf, nb, tw, tid);
+            // the last stage splits line b into its two half-complex rows from registers
+            auto put = [&](int b, int m, V A, V Bc) {
+                const V h = split_hc(A, Bc, m, N);
                 dst[(size_t)2 * b * N + m] = h.x;
                 dst[(size_t)(2 * b + 1) * N + m] = h.y;
-            }
+            };
+            ct_last_stage_pairs<V, FWD, false, N, NB, 1, N, NT>(buf, nb, tw, tid, put);
         } else {
             ct_batch_ip<V, FWD, false, N, NB, 1, N, NT, 1, ct_nstages(N) - 1>(buf, nb, tw, tid);
             // the last stage writes the two real rows of line b from registers
@@ -371,14 +371,9 @@ __global__ void __launch_bounds__(pf_y_threads<T>()) k_yfft_pf(T *__restrict__ d
         __syncthreads();
         if (g + (int)gridDim.x < total) fetch(g + gridDim.x);
         if constexpr (FWD) {
-            ct_batch_ip<V, FWD, true, N, W, W, 1, NT, 1>(buf, nb, tw, tid);
-            for (int e = tid; e < RAW; e += NT) {
-                const int c = e % W, m = e / W;
-                if (c < nb) {
-                    V A = buf[fpad<V>(m * W + c)], Bc = buf[fpad<V>((m == 0 ? 0 : N - m) * W + c)];
-                    plane[(size_t)m * ncol + c0 + c] = split_hc(A, Bc, m, N);
-                }
-            }
+            ct_batch_ip<V, FWD, true, N, W, W, 1, NT, 1, ct_nstages(N) - 1>(buf, nb, tw, tid);
+            auto put = [&](int c, int m, V A, V Bc) { plane[(size_t)m * ncol + c0 + c] = split_hc(A, Bc, m, N); };
+            ct_last_stage_pairs<V, FWD, true, N, W, W, 1, NT>(buf, nb, tw, tid, put);
         } else {
             ct_batch_ip<V, FWD, true, N, W, W, 1, NT, 1, ct_nstages(N) - 1>(buf, nb, tw, tid);
             auto put = [&](int c, int m, V z) { plane[(size_t)m * ncol + c0 + c] = z; };
