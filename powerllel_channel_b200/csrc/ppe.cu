@@ -20,6 +20,7 @@
 #include <string>
 
 #include "ppe.cuh"
+#include "tmem.cuh"
 #include "trid_tables.h"
 
 namespace pl {
@@ -486,6 +487,207 @@ __global__ void __launch_bounds__(128) k_thomas(const T *xin, double *xs, T *xou
     thomas_column<T>(xin, xs, xout, col, cls, stride, cstride, 0, t.nz, t);
 }
 
+// Thomas with the forward-swept values in tensor memory.  The in-place sweep
+// above writes every swept value to HBM and reads it back (32 B/point in
+// FP64), because the 402 MB of a 512x384x256 sweep does not stay in L2.
+// Here each of the 128 threads of a CTA (one per SM: its shared memory is
+// over half the SM's) keeps the nz <= 256 swept values of its column in its
+// own TMEM lane, so HBM sees the right-hand side once, the solution once and
+// the class tables.  The loads are per-thread cp.async copies into a ring of
+// TTM_NS groups of TTM_G rows in shared memory, TTM_NS - 1 groups ahead;
+// each thread reads only its own copies, so the pipeline has no barrier and
+// no wait other than cp.async.wait_group on the thread's own copies.  The
+// copy stream of a round is the forward groups (rhs + multipliers) then the
+// backward groups (reciprocal pivots), and runs on into the next round's
+// columns.  The arithmetic is thomas_column's, operation for operation.
+constexpr int TTM_THREADS = 128, TTM_G = 8, TTM_NS = 8, TTM_MAX_NZ = 256;
+
+template <typename T> __host__ __device__ constexpr size_t ttm_smem_bytes()
+{
+    // table ring [NS][G][128] (double), rhs ring [NS][G][128] (T), (0,0)-mode
+    // rhs ring [NS][G] (double), c_k [TTM_MAX_NZ], TMEM address slot; at
+    // least 116 KB so that two CTAs never share an SM (each may take all 512
+    // TMEM columns)
+    constexpr size_t b =
+        (size_t)TTM_NS * TTM_G * TTM_THREADS * (8 + sizeof(T)) + TTM_NS * TTM_G * 8 + TTM_MAX_NZ * 8 + 16;
+    return b < 116 * 1024 ? 116 * 1024 : b;
+}
+
+// Processing order of the y rows: 0, 1, ny-1, 2, ny-2, ..., ny/2 (ny even),
+// so that rows py and ny - py, which share their class tables, run together.
+__device__ __forceinline__ int trid_pair_row(int b, int ny)
+{
+    if (b == 0) return 0;
+    if (b == ny - 1) return ny / 2;
+    const int jy = (b + 1) / 2;
+    return (b & 1) ? jy : ny - jy;
+}
+
+// One thread's column in one round of the persistent loop.
+struct TtmColumn {
+    bool valid;
+    size_t col, cls;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(TTM_THREADS, 1)
+    k_thomas_tmem(const T *xin, T *xout, TridDev t, const double *mode0, int rounds, uint32_t tcols)
+{
+    constexpr int G = TTM_G, NS = TTM_NS, NT = TTM_THREADS;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *cring = reinterpret_cast<double *>(smem_raw);          // [NS][G][NT] mult (fwd) / rb (bwd)
+    T *xring = reinterpret_cast<T *>(cring + NS * G * NT);           // [NS][G][NT] right-hand side
+    double *zring = reinterpret_cast<double *>(xring + NS * G * NT); // [NS][G] (0,0) mode right-hand side
+    double *csh = zring + NS * G;                                    // [nz] c_k
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(csh + TTM_MAX_NZ);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int nz = t.nz, ngf = nz / G, per_round = 2 * ngf;
+    const size_t stride = (size_t)t.nx * t.ny, cstride = (size_t)t.ncx * t.ncy;
+    const int ncol = t.nx * t.ny;
+
+    for (int k = tid; k < nz; k += NT) csh[k] = __ldg(t.c + k);
+    if (warp == 0) tmem_alloc(tslot, tcols);
+    tmem_fence_before_sync();
+    __syncthreads();
+    tmem_fence_after_sync();
+    const uint32_t tbase = *tslot + ((uint32_t)(warp * 32) << 16);
+
+    auto column = [&](int r) {
+        TtmColumn c{false, 0, 0};
+        const int q = (r * (int)gridDim.x + (int)blockIdx.x) * NT + tid;
+        if (q < ncol) {
+            const int b = q / t.nx, px = q - b * t.nx, py = trid_pair_row(b, t.ny);
+            c = TtmColumn{true, (size_t)px + (size_t)t.nx * py, trid_class(px, py, t)};
+        }
+        return c;
+    };
+    // the (0,0) mode of the mixed path: column 0, which is thread 0's of
+    // CTA 0 in round 0 (processing row 0 is y row 0)
+    const bool zcta = (mode0 != nullptr) && blockIdx.x == 0;
+
+    // copy stream: round ir, group ig, ring slot islot; the source pointers
+    // walk down (forward) and up (backward) the current column row by row
+    int ir = 0, ig = 0, islot = 0;
+    TtmColumn ic = column(0);
+    const T *xsrc = xin + ic.col;
+    const double *msrc = t.mult + ic.cls, *rsrc = t.rb + ic.cls + (size_t)(nz - 1) * cstride;
+    auto issue_next = [&]() {
+        if (ir < rounds) {
+            double *cdst = cring + islot * G * NT + tid;
+            if (ig < ngf) {
+                T *xdst = xring + islot * G * NT + tid;
+                const bool z = zcta && ir == 0 && tid == 0;
+                if (ic.valid) {
+#pragma unroll
+                    for (int u = 0; u < G; u++) {
+                        cp_async_8(cdst + u * NT, msrc);
+                        if (z)
+                            cp_async_8(zring + islot * G + u, mode0 + ig * G + u);
+                        else if (sizeof(T) == 8)
+                            cp_async_8(xdst + u * NT, xsrc);
+                        else
+                            cp_async_4(xdst + u * NT, xsrc);
+                        msrc += cstride;
+                        xsrc += stride;
+                    }
+                }
+            } else if (ic.valid) {
+#pragma unroll
+                for (int u = 0; u < G; u++) {
+                    cp_async_8(cdst + u * NT, rsrc);
+                    rsrc -= cstride;
+                }
+            }
+            if (++ig == per_round) {
+                ig = 0;
+                if (++ir < rounds) {
+                    ic = column(ir);
+                    xsrc = xin + ic.col;
+                    msrc = t.mult + ic.cls;
+                    rsrc = t.rb + ic.cls + (size_t)(nz - 1) * cstride;
+                }
+            }
+        }
+        cp_async_commit(); // one group per step, empty or not
+        islot = (islot + 1 == NS) ? 0 : islot + 1;
+    };
+
+    for (int q = 0; q < NS - 1; q++) issue_next();
+    int slot = 0;
+    for (int r = 0; r < rounds; r++) {
+        const TtmColumn cc = column(r);
+        const bool zr = zcta && r == 0; // warp-uniform
+        // forward elimination: x_k -= (a_k / b_{k-1}) x_{k-1}   (ssolve_trid :319-330);
+        // mult is 0 at k = 0, where it leaves x_0 as it is
+        double xp = 0.0;
+        for (int g = 0; g < ngf; g++) {
+            cp_async_wait<NS - 2>(); // this step's group has landed
+            const double *cs = cring + slot * G * NT + tid;
+            const T *xs = xring + slot * G * NT + tid;
+            double xv[G], mv[G];
+#pragma unroll
+            for (int u = 0; u < G; u++) {
+                xv[u] = (double)xs[u * NT];
+                mv[u] = cs[u * NT];
+            }
+            if (zr && tid == 0) {
+#pragma unroll
+                for (int u = 0; u < G; u++) xv[u] = zring[slot * G + u];
+            }
+            issue_next(); // refills the slot consumed one step ago
+            uint32_t v[2 * G];
+#pragma unroll
+            for (int u = 0; u < G; u++) {
+                xp = xv[u] - mv[u] * xp;
+                v[2 * u] = (uint32_t)__double2loint(xp);
+                v[2 * u + 1] = (uint32_t)__double2hiint(xp);
+            }
+            __syncwarp();
+            tmem_st16(tbase + 2 * g * G, v);
+            slot = (slot + 1 == NS) ? 0 : slot + 1;
+        }
+        tmem_wait_st();
+        // back substitution from the top row: x_k = (x_k - c_k x_{k+1}) / b_k
+        // (:346-356); at k = nz-1, with x_{nz} = 0, it is x /= b (:332-344),
+        // and the (0,0) mode takes the gauge x[nz-1] = 0 there
+        xp = 0.0;
+        T *dst = xout + cc.col + (size_t)(nz - 1) * stride;
+        for (int h = 0; h < ngf; h++) {
+            const int kt = nz - 1 - h * G; // rows kt, kt-1, ..., kt-G+1
+            uint32_t v[2 * G];
+            __syncwarp();
+            tmem_ld16_start(tbase + 2 * (kt - G + 1), v);
+            cp_async_wait<NS - 2>();
+            const double *cs = cring + slot * G * NT + tid;
+            double rv[G], cv[G];
+#pragma unroll
+            for (int u = 0; u < G; u++) {
+                rv[u] = cs[u * NT];
+                cv[u] = csh[kt - u];
+            }
+            if (zr && tid == 0 && h == 0) rv[0] = 0.0;
+            issue_next();
+            tmem_wait_ld(v);
+#pragma unroll
+            for (int u = 0; u < G; u++) {
+                const int i = G - 1 - u;
+                const double x = __hiloint2double((int)v[2 * i + 1], (int)v[2 * i]);
+                xp = (x - cv[u] * xp) * rv[u];
+                if (cc.valid) *dst = (T)xp;
+                dst -= stride;
+            }
+            slot = (slot + 1 == NS) ? 0 : slot + 1;
+        }
+    }
+    cp_async_wait<0>();
+    tmem_fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tmem_fence_after_sync();
+        tmem_free(*tslot, tcols);
+    }
+}
+
 constexpr int PDD_MAX_PARTS = 64;
 
 struct PddDev {
@@ -868,7 +1070,17 @@ template <typename T> static int launch_trid(Ppe *s, T *x, cudaStream_t st, cons
     TridDev t{s->nx, s->ny, s->nz, s->ncx, s->ncy, s->d_mult, s->d_rb, s->d_c};
     dim3 grid((s->nx + 127) / 128, s->ny);
     double *xs = (sizeof(T) == 8 && s->nparts == 0) ? reinterpret_cast<double *>(x) : s->d_scratch;
-    if (s->nparts == 0) {
+    if (s->nparts == 0 && s->nz % TTM_G == 0 && s->nz <= TTM_MAX_NZ) {
+        // swept values in TMEM: one 128-thread CTA per SM, persistent over the columns
+        const size_t shm = ttm_smem_bytes<T>();
+        PL_CUDA_TRY(cudaFuncSetAttribute(k_thomas_tmem<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        const int ncol = s->nx * s->ny;
+        const int ctas = std::max(1, std::min(sm_count(), (ncol + TTM_THREADS - 1) / TTM_THREADS));
+        const int rounds = (ncol + ctas * TTM_THREADS - 1) / (ctas * TTM_THREADS);
+        uint32_t tcols = 32;
+        while (tcols < 2u * (uint32_t)s->nz) tcols *= 2;
+        k_thomas_tmem<T><<<ctas, TTM_THREADS, shm, st>>>(x, x, t, mode0, rounds, tcols);
+    } else if (s->nparts == 0) {
         k_thomas<T><<<grid, 128, 0, st>>>(x, xs, x, t, mode0);
     } else {
         if (sizeof(T) == 4) {

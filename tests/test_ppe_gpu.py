@@ -91,8 +91,11 @@ def test_device_ppe_vs_golden(gpu, path):
     assert torch.equal(x, y)
 
 
+# Thomas runs in tensor memory for nz % 8 == 0 and nz <= 256 (768x32x256: two
+# rounds of columns per CTA), in HBM otherwise
 @pytest.mark.parametrize("nx,ny,nz,nparts", [(64, 64, 64, 0), (128, 96, 48, 0), (256, 192, 32, 4),
-                                            (64, 48, 40, 8), (96, 72, 30, 4), (64, 48, 32, 2)])
+                                            (64, 48, 40, 8), (96, 72, 30, 4), (64, 48, 32, 2),
+                                            (64, 48, 30, 0), (32, 24, 264, 0), (768, 32, 256, 0)])
 def test_ppe_vs_oracle_live(gpu, oracle_mod, nx, ny, nz, nparts):
     """Sizes beyond the fixtures (radix-3 lengths, uneven PDD partitions)."""
     import torch
