@@ -117,10 +117,9 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
     };
 
     // stage 1 on the halo-1 region of plane mq (1 <= mq <= nz)
-    auto produce = [&](int mq) {
+    auto produce = [&](int mq, const RhsConst<R> &cst) {
         const int s0 = mq % NS, sm = (mq - 1) % NS, sp = (mq + 1) % NS;
         for (int q = tid; q < (FX + 2) * (FY + 2); q += nthr) {
-            const RhsConst<R> cst = rhs_const<R>(p, m, mq);
             const int x = q % (FX + 2) + 1, y = q / (FX + 2) + 1;
             const Nb32 n = ring_nb(x, y, s0, sm, sp);
             const int xy = y * UW + x;
@@ -170,7 +169,7 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
 
     double su = 0.0;
     // stage 2 at interior plane kq from the stage-1 planes kq-1, kq, kq+1
-    auto stage2 = [&](int kq) {
+    auto stage2 = [&](int kq, const RhsConst<R> &cst) {
         const int s0 = kq % NS, sm = (kq - 1) % NS, sp = (kq + 1) % NS;
         const Nb32 n = ring_nb(tx + 2, ty + 2, s0, sm, sp);
         // global loads first, so their latency overlaps the stencil
@@ -185,7 +184,6 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
             qyp = __ldg(pq + (size_t)(i0 + tx) + (size_t)p.nx * jp + sk * (kq - 1));
             qzp = (kq < p.nz) ? __ldg(pq + pc + sk) : q0;
         }
-        const RhsConst<R> cst = rhs_const<R>(p, m, kq);
         R ru, rv, rw;
         {
             const int xy = (ty + 2) * UW + tx + 2;
@@ -223,28 +221,43 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
     // runs together with the load of u plane mq+2 into the slot of plane
     // mq-1 that produce(mq) has finished with, so the load's latency hides
     // behind the stage-2 arithmetic.
+    //
+    // The mesh constants of plane mq (cur) and mq-1 (prev) roll in
+    // registers: moving up one plane loads three values, dzf(mq+2),
+    // dzc_inv(mq+1) and dzf_inv(mq+2), instead of all eleven per evaluation.
     const int mstart = max(kbeg - 1, 1), mend = min(kend + 1, p.nz);
+    RhsConst<R> cur = rhs_const<R>(p, m, mstart), prev = cur; // prev is unused until mq = mstart + 1
     load_u_plane(mstart - 1);
     load_u_plane(mstart);
     load_u_plane(mstart + 1);
     __syncthreads();
     for (int mq = mstart; mq <= mend; mq++) {
-        produce(mq);
+        produce(mq, cur);
         __syncthreads();
         if (mq == 1) {
             wall(0, 1);
             __syncthreads();
         }
-        if (mq - 1 >= kbeg && mq - 1 <= kend) stage2(mq - 1);
+        if (mq - 1 >= kbeg && mq - 1 <= kend) stage2(mq - 1, prev);
         if (mq == p.nz) {
             // the top wall plane reuses the ring slot of u1(nz-2), which
             // stage2(nz-1) above has just consumed
             __syncthreads();
             wall(p.nz + 1, p.nz);
             __syncthreads();
-            if (p.nz >= kbeg && p.nz <= kend) stage2(p.nz);
+            if (p.nz >= kbeg && p.nz <= kend) stage2(p.nz, cur);
         }
         if (mq + 2 <= mend + 1) load_u_plane(mq + 2);
+        if (mq < mend) { // constants of plane mq + 1 <= nz: indices up to mq + 2 <= nz + 1
+            prev = cur;
+            cur.dzf_km = cur.dzf_k;
+            cur.dzf_k = cur.dzf_kp;
+            cur.dzf_kp = (R)__ldg(m.dzf + mq + 2);
+            cur.dzci_km = cur.dzci_k;
+            cur.dzci_k = (R)__ldg(m.dzc_inv + mq + 1);
+            cur.dzfi_k = cur.dzfi_kp;
+            cur.dzfi_kp = (R)__ldg(m.dzf_inv + mq + 2);
+        }
         __syncthreads();
     }
     mean_reduce(su, red);
