@@ -100,29 +100,53 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
     const R dt = (R)p.dt;
     const R bcu = (R)(0.0 - p.u_crf);
 
-    auto load_u_plane = [&](int kq) { // kq in [0, nz+1]; periodic x, y halo
+    // This thread's points of a ring plane (UPS = 432 over 256 threads: two
+    // slots, the second for tid < 176) and their in-plane global offsets
+    // with the periodic x, y wrap, fixed for the whole march.
+    constexpr int LSLOTS = (UPS + FX * FY - 1) / (FX * FY);
+    int loff[LSLOTS];
+#pragma unroll
+    for (int sl = 0; sl < LSLOTS; sl++) {
+        const int q = tid + sl * nthr, lx = q % UW, ly = q / UW;
+        int gi = i0 - 2 + lx, gj = j0 - 2 + ly;
+        gi += (gi < 0) ? p.nx : 0;
+        gi -= (gi >= p.nx) ? p.nx : 0;
+        gj += (gj < 0) ? p.ny : 0;
+        gj -= (gj >= p.ny) ? p.ny : 0;
+        loff[sl] = gi + p.nx * gj;
+    }
+    auto load_u_plane = [&](int kq) { // kq in [0, nz+1]
         const int s = kq % NS;
-        for (int q = tid; q < UPS; q += nthr) {
-            const int lx = q % UW, ly = q / UW;
-            int gi = i0 - 2 + lx, gj = j0 - 2 + ly;
-            gi += (gi < 0) ? p.nx : 0;
-            gi -= (gi >= p.nx) ? p.nx : 0;
-            gj += (gj < 0) ? p.ny : 0;
-            gj -= (gj >= p.ny) ? p.ny : 0;
-            const size_t g = (size_t)gi + (size_t)p.nx * gj + sk * kq;
-            ur[0 * FS + s * UPS + q] = (R)__ldg(u + g);
-            ur[1 * FS + s * UPS + q] = (R)__ldg(v + g);
-            ur[2 * FS + s * UPS + q] = (R)__ldg(w + g);
+        const size_t gk = sk * kq;
+#pragma unroll
+        for (int sl = 0; sl < LSLOTS; sl++) {
+            const int q = tid + sl * nthr;
+            if (UPS % (FX * FY) == 0 || q < UPS) {
+                const size_t g = gk + loff[sl];
+                ur[0 * FS + s * UPS + q] = (R)__ldg(u + g);
+                ur[1 * FS + s * UPS + q] = (R)__ldg(v + g);
+                ur[2 * FS + s * UPS + q] = (R)__ldg(w + g);
+            }
         }
     };
 
     // stage 1 on the halo-1 region of plane mq (1 <= mq <= nz)
+    // this thread's points of the halo-1 region (34 x 10 over 256 threads),
+    // as in-plane ring offsets
+    constexpr int HPTS = (FX + 2) * (FY + 2), HSLOTS = (HPTS + FX * FY - 1) / (FX * FY);
+    int hxy[HSLOTS];
+#pragma unroll
+    for (int sl = 0; sl < HSLOTS; sl++) {
+        const int q = tid + sl * nthr;
+        hxy[sl] = (q / (FX + 2) + 1) * UW + q % (FX + 2) + 1;
+    }
+
     auto produce = [&](int mq, const RhsConst<R> &cst) {
         const int s0 = mq % NS, sm = (mq - 1) % NS, sp = (mq + 1) % NS;
-        for (int q = tid; q < (FX + 2) * (FY + 2); q += nthr) {
-            const int x = q % (FX + 2) + 1, y = q / (FX + 2) + 1;
-            const Nb32 n = ring_nb(x, y, s0, sm, sp);
-            const int xy = y * UW + x;
+#pragma unroll
+        for (int sl = 0; sl < HSLOTS; sl++) {
+            if (HPTS % (FX * FY) != 0 && tid + sl * nthr >= HPTS) break;
+            const int xy = hxy[sl];
             const int om = sm * UPS + xy, oc = s0 * UPS + xy, op = sp * UPS + xy;
             R ru, rv, rw;
             momentum_rhs_c<R, CRF>(RingLoad3<R>{ur + om, ur + oc, ur + op},
@@ -131,16 +155,16 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
                                    ru, rv, rw);
             if (MIXED) { // increments, and u1 = u + d1 for the stage-2 stencils
                 const R du = dt * ru, dv = dt * rv, dw = (mq == p.nz) ? (R)0 : dt * rw; // w1(nz) = 0 = w(nz)
-                qr[n.c] = du;
-                qr[FS + n.c] = dv;
-                qr[2 * FS + n.c] = dw;
-                sr[n.c] = ur[n.c] + du;
-                sr[FS + n.c] = ur[FS + n.c] + dv;
-                sr[2 * FS + n.c] = ur[2 * FS + n.c] + dw;
+                qr[oc] = du;
+                qr[FS + oc] = dv;
+                qr[2 * FS + oc] = dw;
+                sr[oc] = ur[oc] + du;
+                sr[FS + oc] = ur[FS + oc] + dv;
+                sr[2 * FS + oc] = ur[2 * FS + oc] + dw;
             } else {      // u1 = u + dt*(visc - conv)
-                qr[n.c] = ur[n.c] + dt * (ru + (R)p.fb[0]);
-                qr[FS + n.c] = ur[FS + n.c] + dt * (rv + (R)p.fb[1]);
-                qr[2 * FS + n.c] = (mq == p.nz) ? (R)0 : ur[2 * FS + n.c] + dt * (rw + (R)p.fb[2]);
+                qr[oc] = ur[oc] + dt * (ru + (R)p.fb[0]);
+                qr[FS + oc] = ur[FS + oc] + dt * (rv + (R)p.fb[1]);
+                qr[2 * FS + oc] = (mq == p.nz) ? (R)0 : ur[2 * FS + oc] + dt * (rw + (R)p.fb[2]);
             }
         }
     };
@@ -148,9 +172,10 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
     // imposeNoSlipBC on the stage-1 field: plane kg from plane ki (0 <- 1, nz+1 <- nz)
     auto wall = [&](int kg, int ki) {
         const int sg = kg % NS, si = ki % NS;
-        for (int q = tid; q < (FX + 2) * (FY + 2); q += nthr) {
-            const int x = q % (FX + 2) + 1, y = q / (FX + 2) + 1;
-            const int xy = y * UW + x;
+#pragma unroll
+        for (int sl = 0; sl < HSLOTS; sl++) {
+            if (HPTS % (FX * FY) != 0 && tid + sl * nthr >= HPTS) break;
+            const int xy = hxy[sl];
             if (MIXED) { // u1(g) = 2bc - u1(i) and u(g) = 2bc - u(i)  =>  d1(g) = -d1(i)
                 const R du = -qr[si * UPS + xy], dv = -qr[FS + si * UPS + xy];
                 qr[sg * UPS + xy] = du;
