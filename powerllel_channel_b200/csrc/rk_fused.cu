@@ -89,6 +89,7 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
     using R = typename RkTraits<MIXED>::R;
     constexpr int NS = RkTraits<MIXED>::NS;
     constexpr int FS = NS * UPS; // ring size per field
+    static_assert(NS == 3, "the ring slot rotation of the march assumes three-plane rings");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R *ur = reinterpret_cast<R *>(smem_raw); // u, v, w rings
     R *qr = ur + 3 * FS;                     // u1 (FP64) or d1 (mixed) rings
@@ -115,8 +116,7 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
         gj -= (gj >= p.ny) ? p.ny : 0;
         loff[sl] = gi + p.nx * gj;
     }
-    auto load_u_plane = [&](int kq) { // kq in [0, nz+1]
-        const int s = kq % NS;
+    auto load_u_plane = [&](int kq, int s) { // kq in [0, nz+1], into ring slot s = kq % NS
         const size_t gk = sk * kq;
 #pragma unroll
         for (int sl = 0; sl < LSLOTS; sl++) {
@@ -141,8 +141,8 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
         hxy[sl] = (q / (FX + 2) + 1) * UW + q % (FX + 2) + 1;
     }
 
-    auto produce = [&](int mq, const RhsConst<R> &cst) {
-        const int s0 = mq % NS, sm = (mq - 1) % NS, sp = (mq + 1) % NS;
+    // ring slots sm, s0, sp of the planes mq-1, mq, mq+1
+    auto produce = [&](int mq, int sm, int s0, int sp, const RhsConst<R> &cst) {
 #pragma unroll
         for (int sl = 0; sl < HSLOTS; sl++) {
             if (HPTS % (FX * FY) != 0 && tid + sl * nthr >= HPTS) break;
@@ -194,8 +194,7 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
 
     double su = 0.0;
     // stage 2 at interior plane kq from the stage-1 planes kq-1, kq, kq+1
-    auto stage2 = [&](int kq, const RhsConst<R> &cst) {
-        const int s0 = kq % NS, sm = (kq - 1) % NS, sp = (kq + 1) % NS;
+    auto stage2 = [&](int kq, int sm, int s0, int sp, const RhsConst<R> &cst) {
         const Nb32 n = ring_nb(tx + 2, ty + 2, s0, sm, sp);
         // global loads first, so their latency overlaps the stencil
         const size_t g = (size_t)(i0 + tx) + (size_t)p.nx * (j0 + ty) + sk * kq;
@@ -252,27 +251,35 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
     // dzc_inv(mq+1) and dzf_inv(mq+2), instead of all eleven per evaluation.
     const int mstart = max(kbeg - 1, 1), mend = min(kend + 1, p.nz);
     RhsConst<R> cur = rhs_const<R>(p, m, mstart), prev = cur; // prev is unused until mq = mstart + 1
-    load_u_plane(mstart - 1);
-    load_u_plane(mstart);
-    load_u_plane(mstart + 1);
+    // ring slots of the planes mq-1, mq, mq+1, rotated once per plane
+    int sa = (mstart - 1) % NS, sb = mstart % NS, sc = (mstart + 1) % NS;
+    load_u_plane(mstart - 1, sa);
+    load_u_plane(mstart, sb);
+    load_u_plane(mstart + 1, sc);
     __syncthreads();
     for (int mq = mstart; mq <= mend; mq++) {
-        produce(mq, cur);
+        if (!MIXED) { // measured: the FP64 kernel is faster with the slots recomputed
+            sa = (mq - 1) % NS;
+            sb = mq % NS;
+            sc = (mq + 1) % NS;
+        }
+        produce(mq, sa, sb, sc, cur);
         __syncthreads();
         if (mq == 1) {
             wall(0, 1);
             __syncthreads();
         }
-        if (mq - 1 >= kbeg && mq - 1 <= kend) stage2(mq - 1, prev);
+        // plane mq-2 sits in slot sc
+        if (mq - 1 >= kbeg && mq - 1 <= kend) stage2(mq - 1, sc, sa, sb, prev);
         if (mq == p.nz) {
             // the top wall plane reuses the ring slot of u1(nz-2), which
             // stage2(nz-1) above has just consumed
             __syncthreads();
             wall(p.nz + 1, p.nz);
             __syncthreads();
-            if (p.nz >= kbeg && p.nz <= kend) stage2(p.nz, cur);
+            if (p.nz >= kbeg && p.nz <= kend) stage2(p.nz, sa, sb, sc, cur);
         }
-        if (mq + 2 <= mend + 1) load_u_plane(mq + 2);
+        if (mq + 2 <= mend + 1) load_u_plane(mq + 2, sa); // (mq + 2) % 3 == (mq - 1) % 3
         if (mq < mend) { // constants of plane mq + 1 <= nz: indices up to mq + 2 <= nz + 1
             prev = cur;
             cur.dzf_km = cur.dzf_k;
@@ -283,6 +290,10 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
             cur.dzfi_k = cur.dzfi_kp;
             cur.dzfi_kp = (R)__ldg(m.dzf_inv + mq + 2);
         }
+        const int st = sa;
+        sa = sb;
+        sb = sc;
+        sc = st;
         __syncthreads();
     }
     mean_reduce(su, red);
