@@ -94,58 +94,81 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
     R *ur = reinterpret_cast<R *>(smem_raw); // u, v, w rings
     R *qr = ur + 3 * FS;                     // u1 (FP64) or d1 (mixed) rings
     R *sr = qr + 3 * FS;                     // mixed: u1 = u + d1 in FP32 (the stage-2 stencil input)
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + ty * FX, nthr = FX * FY;
+    const int tx = threadIdx.x, ty = threadIdx.y;
     const int i0 = blockIdx.x * FX, j0 = blockIdx.y * FY;
     const int kbeg = blockIdx.z * kchunk + 1, kend = min(kbeg + kchunk - 1, p.nz);
     const size_t sk = (size_t)p.nx * p.ny;
     const R dt = (R)p.dt;
     const R bcu = (R)(0.0 - p.u_crf);
 
-    // This thread's points of a ring plane (UPS = 432 over 256 threads: two
-    // slots, the second for tid < 176) and their in-plane global offsets
-    // with the periodic x, y wrap, fixed for the whole march.
-    constexpr int LSLOTS = (UPS + FX * FY - 1) / (FX * FY);
-    int loff[LSLOTS];
+    // This thread's points of a ring plane and of the stage-1 (halo-1)
+    // region, fixed for the whole march.  Each warp takes 32 consecutive x of
+    // one row, so its shared-memory accesses are free of bank conflicts and
+    // its global loads are whole 32-element row segments; the columns left
+    // over are taken four (load) or one (stage 1) per row.
+    //   ring plane, 36 x 12: slot 0 = x 2..33 of rows 0..7 (warp = row);
+    //     slot 1 = x 2..33 of rows 8..11 (warps 0-3), and x 0, 1, 34, 35 of
+    //     rows 0..11 (warp 4 and half of warp 5: 48 points)
+    //   stage-1 region, x 1..34, y 1..10: slot 0 = x 2..33 of rows 1..8;
+    //     slot 1 = x 2..33 of rows 9, 10 (warps 0, 1), and x 1, 34 of rows
+    //     1..10 (20 lanes of warp 2)
+    static_assert(FX == 32 && FY == 8 && UW == 36 && UH == 12, "slot maps of the 32 x 8 tile");
+    const int lane = tx, wid = ty;
+    int loff[2], lxy[2];
+    bool lval1;
+    {
+        int lx[2], ly[2];
+        lx[0] = 2 + lane;
+        ly[0] = wid;
+        if (wid < 4) {
+            lx[1] = 2 + lane;
+            ly[1] = 8 + wid;
+        } else {
+            const int e = (wid - 4) * 32 + lane, c = e % 4; // e < 48 on warps 4, 5
+            lx[1] = c < 2 ? c : 32 + c;
+            ly[1] = min(e / 4, UH - 1);
+        }
+        lval1 = wid < 5 || (wid == 5 && lane < 16);
 #pragma unroll
-    for (int sl = 0; sl < LSLOTS; sl++) {
-        const int q = tid + sl * nthr, lx = q % UW, ly = q / UW;
-        int gi = i0 - 2 + lx, gj = j0 - 2 + ly;
-        gi += (gi < 0) ? p.nx : 0;
-        gi -= (gi >= p.nx) ? p.nx : 0;
-        gj += (gj < 0) ? p.ny : 0;
-        gj -= (gj >= p.ny) ? p.ny : 0;
-        loff[sl] = gi + p.nx * gj;
+        for (int sl = 0; sl < 2; sl++) {
+            int gi = i0 - 2 + lx[sl], gj = j0 - 2 + ly[sl];
+            gi += (gi < 0) ? p.nx : 0;
+            gi -= (gi >= p.nx) ? p.nx : 0;
+            gj += (gj < 0) ? p.ny : 0;
+            gj -= (gj >= p.ny) ? p.ny : 0;
+            loff[sl] = gi + p.nx * gj;
+            lxy[sl] = ly[sl] * UW + lx[sl];
+        }
     }
     auto load_u_plane = [&](int kq, int s) { // kq in [0, nz+1], into ring slot s = kq % NS
         const size_t gk = sk * kq;
 #pragma unroll
-        for (int sl = 0; sl < LSLOTS; sl++) {
-            const int q = tid + sl * nthr;
-            if (UPS % (FX * FY) == 0 || q < UPS) {
+        for (int sl = 0; sl < 2; sl++) {
+            if (sl == 0 || lval1) {
                 const size_t g = gk + loff[sl];
-                ur[0 * FS + s * UPS + q] = (R)__ldg(u + g);
-                ur[1 * FS + s * UPS + q] = (R)__ldg(v + g);
-                ur[2 * FS + s * UPS + q] = (R)__ldg(w + g);
+                const int q = s * UPS + lxy[sl];
+                ur[0 * FS + q] = (R)__ldg(u + g);
+                ur[1 * FS + q] = (R)__ldg(v + g);
+                ur[2 * FS + q] = (R)__ldg(w + g);
             }
         }
     };
 
-    // stage 1 on the halo-1 region of plane mq (1 <= mq <= nz)
-    // this thread's points of the halo-1 region (34 x 10 over 256 threads),
-    // as in-plane ring offsets
-    constexpr int HPTS = (FX + 2) * (FY + 2), HSLOTS = (HPTS + FX * FY - 1) / (FX * FY);
-    int hxy[HSLOTS];
-#pragma unroll
-    for (int sl = 0; sl < HSLOTS; sl++) {
-        const int q = tid + sl * nthr;
-        hxy[sl] = (q / (FX + 2) + 1) * UW + q % (FX + 2) + 1;
-    }
+    int hxy[2];
+    bool hval1;
+    hxy[0] = (1 + wid) * UW + 2 + lane;
+    if (wid < 2)
+        hxy[1] = (9 + wid) * UW + 2 + lane;
+    else
+        hxy[1] = (1 + lane % 10) * UW + (lane < 10 ? 1 : 34);
+    hval1 = wid < 2 || (wid == 2 && lane < 20);
+    constexpr int HSLOTS = 2;
 
     // ring slots sm, s0, sp of the planes mq-1, mq, mq+1
     auto produce = [&](int mq, int sm, int s0, int sp, const RhsConst<R> &cst) {
 #pragma unroll
         for (int sl = 0; sl < HSLOTS; sl++) {
-            if (HPTS % (FX * FY) != 0 && tid + sl * nthr >= HPTS) break;
+            if (sl == 1 && !hval1) break;
             const int xy = hxy[sl];
             const int om = sm * UPS + xy, oc = s0 * UPS + xy, op = sp * UPS + xy;
             R ru, rv, rw;
@@ -174,7 +197,7 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
         const int sg = kg % NS, si = ki % NS;
 #pragma unroll
         for (int sl = 0; sl < HSLOTS; sl++) {
-            if (HPTS % (FX * FY) != 0 && tid + sl * nthr >= HPTS) break;
+            if (sl == 1 && !hval1) break;
             const int xy = hxy[sl];
             if (MIXED) { // u1(g) = 2bc - u1(i) and u(g) = 2bc - u(i)  =>  d1(g) = -d1(i)
                 const R du = -qr[si * UPS + xy], dv = -qr[FS + si * UPS + xy];
