@@ -281,11 +281,6 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
     load_u_plane(mstart + 1, sc);
     __syncthreads();
     for (int mq = mstart; mq <= mend; mq++) {
-        if (!MIXED) { // measured: the FP64 kernel is faster with the slots recomputed
-            sa = (mq - 1) % NS;
-            sb = mq % NS;
-            sc = (mq + 1) % NS;
-        }
         produce(mq, sa, sb, sc, cur);
         __syncthreads();
         if (mq == 1) {
