@@ -317,19 +317,44 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
     mean_reduce(su, red);
 }
 
-static int fused_chunks(const StepParams &p)
+// z-chunks per tile column: the count that minimises the modelled time,
+// waves x (planes per chunk + the 2 planes of stage 1 that each chunk
+// recomputes at its ends), where a wave is `resident` CTAs (all CTAs do the
+// same work, so they retire in waves).  Chunks keep at least 16 planes.
+static int fused_chunks(const StepParams &p, long resident)
 {
     const int tiles = (p.nx / FX) * (p.ny / FY);
-    int nch = (1184 + tiles - 1) / tiles;
     const int maxch = p.nz / 16 > 1 ? p.nz / 16 : 1;
-    if (nch > maxch) nch = maxch;
-    if (nch < 1) nch = 1;
-    return nch;
+    int best = 1;
+    long best_cost = -1;
+    for (int nch = 1; nch <= maxch; nch++) {
+        const int kchunk = (p.nz + nch - 1) / nch;
+        const long nblk = (long)tiles * ((p.nz + kchunk - 1) / kchunk);
+        const long cost = ((nblk + resident - 1) / resident) * (kchunk + 2);
+        if (best_cost < 0 || cost < best_cost) {
+            best_cost = cost;
+            best = nch;
+        }
+    }
+    return best;
 }
 
 bool rk_fused_supported(const StepParams &p) { return p.nx % FX == 0 && p.ny % FY == 0 && p.nz >= 2; }
 
-int rk_fused_blocks(const StepParams &p) { return (p.nx / FX) * (p.ny / FY) * fused_chunks(p); }
+// an upper bound of the launch's CTA count (fused_chunks never exceeds nz/16)
+int rk_fused_blocks(const StepParams &p) { return (p.nx / FX) * (p.ny / FY) * (p.nz / 16 > 1 ? p.nz / 16 : 1); }
+
+static int sm_count_rk()
+{
+    static int n = 0;
+    if (n == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 1;
+    }
+    return n;
+}
 
 template <bool MIXED>
 static int launch_rk_fused_t(const double *u, const double *v, const double *w, double *uo, double *vo, double *wo,
@@ -340,13 +365,6 @@ static int launch_rk_fused_t(const double *u, const double *v, const double *w, 
         set_error("fused RK kernel needs nx % 32 == 0 and ny % 8 == 0");
         return -1;
     }
-    const int nch = fused_chunks(p);
-    const int kchunk = (p.nz + nch - 1) / nch;
-    dim3 grid(p.nx / FX, p.ny / FY, (p.nz + kchunk - 1) / kchunk);
-    if ((int)(grid.x * grid.y * grid.z) > ms.max_blocks) {
-        set_error("mean buffer too small for the fused RK kernel");
-        return -1;
-    }
     using R = typename RkTraits<MIXED>::R;
     const size_t shm = sizeof(R) * (MIXED ? 9 : 6) * RkTraits<MIXED>::NS * UPS;
     // u_crf == 0 (the channel's usual frame) drops the frame-velocity terms
@@ -355,6 +373,16 @@ static int launch_rk_fused_t(const double *u, const double *v, const double *w, 
     // prefer the largest shared-memory carve-out: several CTAs per SM
     PL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
                                      (int)cudaSharedmemCarveoutMaxShared));
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, FX * FY, shm) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    const int nch = fused_chunks(p, (long)per_sm * sm_count_rk());
+    const int kchunk = (p.nz + nch - 1) / nch;
+    dim3 grid(p.nx / FX, p.ny / FY, (p.nz + kchunk - 1) / kchunk);
+    if ((int)(grid.x * grid.y * grid.z) > ms.max_blocks) {
+        set_error("mean buffer too small for the fused RK kernel");
+        return -1;
+    }
     MeanRed r{ms.partial, ms.counter, ms.scalar, (double)p.nx, (double)p.ny, ms.vel_force};
     kern<<<grid, dim3(FX, FY), shm, st>>>(u, v, w, uo, vo, wo, p, m, r, kchunk, pq, pinc);
     PL_CHECK_LAUNCH();
