@@ -471,31 +471,50 @@ __global__ void __launch_bounds__(256) k_rk2_mixed(const double *__restrict__ u,
 // L p_pred, L being exactly the operator the PPE inverts; p_pred = 2 p_n -
 // p_{n-1} makes r the second difference of p in time, and every FP32 error
 // of the increment solve scales with |r|.
-__global__ void __launch_bounds__(256) k_rhs_mixed(const double *__restrict__ u, const double *__restrict__ v,
-                                                   const double *__restrict__ w, float *__restrict__ r,
-                                                   double *__restrict__ warp_part, StepParams p, MeshDev m)
+// Two adjacent points (i, i+1), i even, per thread: 16-byte loads of the
+// u, v, w pairs and of the v and w pairs at j-1 and k-1, one float2 store,
+// and one warp reduction per two points.  nx is even (the transforms pair
+// lines), so every pair is 16-byte aligned and lies in one row.
+constexpr int RHS_BX = 32, RHS_BY = 8; // threads; a block covers 64 x 8 points of a plane
+__global__ void __launch_bounds__(RHS_BX *RHS_BY) k_rhs_mixed(const double *__restrict__ u, const double *__restrict__ v,
+                                                              const double *__restrict__ w, float *__restrict__ r,
+                                                              double *__restrict__ warp_part, StepParams p, MeshDev m)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i = 2 * (blockIdx.x * RHS_BX + threadIdx.x);
+    const int j = blockIdx.y * RHS_BY + threadIdx.y;
     const int k = blockIdx.z + 1;
     const size_t sk = (size_t)p.nx * p.ny;
     double val = 0.0;
     if (i < p.nx && j < p.ny) {
-        const Nb n = neighbours(i, j, k, p.nx, p.ny);
+        const int im = (i == 0) ? p.nx - 1 : i - 1, jm = (j == 0) ? p.ny - 1 : j - 1;
+        const size_t row = (size_t)p.nx * j + sk * k, c = row + i;
+        const size_t ym = (size_t)p.nx * jm + sk * k + i;
         const double dti = 1.0 / p.dt, dtidxi = dti * p.dx_inv, dtidyi = dti * p.dy_inv;
-        const double rhs = (__ldg(u + n.c) - __ldg(u + n.xm)) * dtidxi + (__ldg(v + n.c) - __ldg(v + n.ym)) * dtidyi +
-                           (__ldg(w + n.c) - __ldg(w + n.zm)) * dti * __ldg(m.dzf_inv + k);
-        r[n.c - sk] = (float)rhs;
-        val = rhs;
+        const double2 uc = __ldg(reinterpret_cast<const double2 *>(u + c));
+        const double uxm = __ldg(u + row + im);
+        const double2 vc = __ldg(reinterpret_cast<const double2 *>(v + c));
+        const double2 vym = __ldg(reinterpret_cast<const double2 *>(v + ym));
+        const double2 wc = __ldg(reinterpret_cast<const double2 *>(w + c));
+        const double2 wzm = __ldg(reinterpret_cast<const double2 *>(w + c - sk));
+        // the expressions of k_calc_rhs_fp64, per point
+        const double r0 = (uc.x - uxm) * dtidxi + (vc.x - vym.x) * dtidyi + (wc.x - wzm.x) * dti * __ldg(m.dzf_inv + k);
+        const double r1 = (uc.y - uc.x) * dtidxi + (vc.y - vym.y) * dtidyi + (wc.y - wzm.y) * dti * __ldg(m.dzf_inv + k);
+        *reinterpret_cast<float2 *>(r + c - sk) = make_float2((float)r0, (float)r1);
+        val = r0 + r1;
     }
     // warp partials (no block barrier); summed per plane in a fixed order
     for (int o = 16; o > 0; o >>= 1) val += __shfl_down_sync(0xffffffffu, val, o);
-    const int t = threadIdx.x + threadIdx.y * blockDim.x;
+    const int t = threadIdx.x + threadIdx.y * RHS_BX;
     if ((t & 31) == 0) {
-        const int wpb = (blockDim.x * blockDim.y) >> 5;
+        constexpr int wpb = (RHS_BX * RHS_BY) >> 5;
         const size_t b = blockIdx.x + (size_t)gridDim.x * blockIdx.y;
         warp_part[((size_t)blockIdx.z * gridDim.x * gridDim.y + b) * wpb + (t >> 5)] = val;
     }
+}
+
+static inline dim3 rhs_mixed_grid(const StepParams &p)
+{
+    return dim3((p.nx / 2 + RHS_BX - 1) / RHS_BX, (p.ny + RHS_BY - 1) / RHS_BY, p.nz);
 }
 
 // per-plane sums of the warp partials (fixed order): mode0[k] = sum_ij r
@@ -683,22 +702,24 @@ int launch_rk2_mixed(const double *u, const double *v, const double *w, const fl
     return 0;
 }
 
+int warp_partials_per_plane(const StepParams &p)
+{
+    const dim3 g = rhs_mixed_grid(p);
+    return (int)(g.x * g.y) * ((RHS_BX * RHS_BY) / 32);
+}
+
 int launch_rhs_mixed(const double *u, const double *v, const double *w, float *r, double *warp_part, double *mode0,
                      const StepParams &p, const MeshDev &m, cudaStream_t st)
 {
-    k_rhs_mixed<<<point_grid(p), point_block(), 0, st>>>(u, v, w, r, warp_part, p, m);
+    if (p.nx % 2 != 0) {
+        set_error("the mixed right-hand side needs an even nx");
+        return -1;
+    }
+    k_rhs_mixed<<<rhs_mixed_grid(p), dim3(RHS_BX, RHS_BY), 0, st>>>(u, v, w, r, warp_part, p, m);
     PL_CHECK_LAUNCH();
-    dim3 g = point_grid(p);
-    const int nper = (int)(g.x * g.y) * (int)((point_block().x * point_block().y) / 32);
-    k_plane_sums<<<p.nz, 256, 0, st>>>(warp_part, nper, p.nz, mode0);
+    k_plane_sums<<<p.nz, 256, 0, st>>>(warp_part, warp_partials_per_plane(p), p.nz, mode0);
     PL_CHECK_LAUNCH();
     return 0;
-}
-
-int warp_partials_per_plane(const StepParams &p)
-{
-    dim3 g = point_grid(p);
-    return (int)(g.x * g.y) * (int)((point_block().x * point_block().y) / 32);
 }
 
 } // namespace pl
