@@ -328,7 +328,7 @@ extern "C" int pl_channel_create(pl_channel **out, const pl_channel_config *cfg)
     if (ok && mixed)
         ok = dalloc(&c->pb, c->np) && dalloc(&c->pm, c->np) && falloc(&c->d1u, c->nf) && falloc(&c->d1v, c->nf) &&
              falloc(&c->d1w, c->nf) && falloc(&c->r32, c->np) && dalloc(&c->mode0, c->nz) &&
-             dalloc(&c->plane_part, (size_t)warp_partials_per_plane(c->sp) * c->nz);
+             dalloc(&c->plane_part, (size_t)std::max(warp_partials_per_plane(c->sp), c->sp.ny / 2) * c->nz);
     if (!ok) {
         set_error("pl_channel_create: out of device memory for the fields");
         return fail();
@@ -447,21 +447,62 @@ extern "C" int pl_phase_calc_rhs(pl_channel *c)
     return rc;
 }
 
+// The mixed increment solve's pressure update: its inverse x transform also
+// forms p_n <- prediction + increment (in place) and, in pb, the next
+// prediction, extrapolated from the third projection on.
+static PressureUpdate mixed_pressure_update(const pl_channel *c)
+{
+    PressureUpdate pu;
+    pu.q = c->pm;
+    pu.p = c->p;
+    pu.qnext = c->pb;
+    pu.incremental = mixed_incremental(c);
+    pu.qmode = (c->nsolve + 1 >= 3) ? 1 : 0;
+    return pu;
+}
+
 extern "C" int pl_phase_poisson(pl_channel *c)
 {
     if (is_mixed(c)) {
-        // the increment solve; its inverse x transform also forms
-        // p_n <- prediction + increment (in place) and, in pb, the next
-        // prediction, extrapolated from the third projection on
-        PressureUpdate pu;
-        pu.q = c->pm;
-        pu.p = c->p;
-        pu.qnext = c->pb;
-        pu.incremental = mixed_incremental(c);
-        pu.qmode = (c->nsolve + 1 >= 3) ? 1 : 0;
+        const PressureUpdate pu = mixed_pressure_update(c);
         return ppe_solve_fp32(&c->ppe, c->r32, c->mode0, c->stream, &pu);
     }
     return ppe_solve_fp64(&c->ppe, c->p, c->stream);
+}
+
+// calcRHS + the Poisson solve, with calcRHS fused into the solve's forward x
+// transform where the transform length allows (the right-hand side then
+// never crosses HBM); otherwise the two phases.  The FP64 right-hand side
+// and its transform are the same numbers either way; the mixed path's FP64
+// plane sums are summed per line pair instead of per warp.
+static int phase_rhs_poisson(pl_channel *c)
+{
+    DivIn d;
+    d.u = c->u;
+    d.v = c->v;
+    d.w = c->w;
+    d.dzf_inv = c->m.dzf_inv;
+    d.dti = 1.0 / c->sp.dt;
+    d.dtidxi = d.dti * c->sp.dx_inv;
+    d.dtidyi = d.dti * c->sp.dy_inv;
+    if (is_mixed(c)) {
+        const int rc = ppe_xfwd_div<float>(&c->ppe, d, c->r32, c->plane_part, c->stream);
+        if (rc < 0) return -1;
+        if (rc == 0) {
+            if (launch_plane_sums(c->plane_part, c->sp.ny / 2, c->nz, c->mode0, c->stream)) return -1;
+            channel_mark(c, "rhs_xfft");
+            const PressureUpdate pu = mixed_pressure_update(c);
+            return ppe_solve_fp32_from_x(&c->ppe, c->r32, c->mode0, c->stream, &pu);
+        }
+    } else {
+        const int rc = ppe_xfwd_div<double>(&c->ppe, d, c->p, nullptr, c->stream);
+        if (rc < 0) return -1;
+        if (rc == 0) {
+            channel_mark(c, "rhs_xfft");
+            return ppe_solve_fp64_from_x(&c->ppe, c->p, c->stream);
+        }
+    }
+    return (pl_phase_calc_rhs(c) || pl_phase_poisson(c)) ? -1 : 0;
 }
 
 extern "C" int pl_phase_correct_force(pl_channel *c)
@@ -545,7 +586,7 @@ extern "C" int pl_channel_profile(pl_channel *c, int nsteps, double *ms, char *n
 extern "C" int pl_channel_step(pl_channel *c, int nsteps)
 {
     for (int s = 0; s < nsteps; s++) {
-        if (pl_phase_rk(c) || pl_phase_calc_rhs(c) || pl_phase_poisson(c) || pl_phase_correct_force(c)) return -1;
+        if (pl_phase_rk(c) || phase_rhs_poisson(c) || pl_phase_correct_force(c)) return -1;
     }
     return 0;
 }

@@ -383,6 +383,93 @@ __global__ void __launch_bounds__(pf_y_threads<T>()) k_yfft_pf(T *__restrict__ d
     }
     cp_async_wait<0>();
 }
+// calcRHS (mod_calcRHS.f90:19-33) fused into the forward x transform.  One
+// group is one line pair (rows 2p, 2p+1 of interior plane k); its staging
+// holds, as FP64 rows of the ghosted fields (plane kg = k + 1): u rows 2p,
+// 2p+1; v rows 2p-1 (periodic), 2p, 2p+1; w rows 2p, 2p+1 of planes kg and
+// kg - 1.  The first Stockham stage forms rhs = div(u)/dt of the two rows
+// with k_calc_rhs_fp64's expression (u_{i-1} is in the same periodic row)
+// and pairs them into one complex line, so neither the right-hand side nor
+// its re-read crosses HBM.  When `part` is given, each group also writes the
+// FP64 sum of its rhs values (in a fixed order) for the plane sums of the
+// mixed path's (0,0) mode.
+constexpr int XDIV_THREADS = 64;
+
+template <typename T, int N> __host__ __device__ constexpr int xdiv_smem_bytes()
+{
+    using V = typename cplx_of<T>::type;
+    // work buffer, 9 staged FP64 rows, per-stage twiddles, 2 warp sums
+    return (int)(sizeof(V) * ((fpad_elems<V>(N) + 1) / 2 * 2) + 8 * 9 * N + sizeof(V) * N + 16);
+}
+
+template <typename T, int N>
+__global__ void __launch_bounds__(XDIV_THREADS) k_xfft_div_pf(DivIn d, T *__restrict__ out,
+                                                              const typename cplx_of<T>::type *__restrict__ twg,
+                                                              int ny, int total, double *__restrict__ part)
+{
+    using V = typename cplx_of<T>::type;
+    constexpr int NT = XDIV_THREADS, BUF = (fpad_elems<V>(N) + 1) / 2 * 2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *buf = reinterpret_cast<V *>(smem_raw);
+    double *stage = reinterpret_cast<double *>(buf + BUF); // rows: u0 u1 | v- v0 v1 | w0 w1 | w0m w1m
+    V *tw = reinterpret_cast<V *>(stage + 9 * N);
+    double *wsum = reinterpret_cast<double *>(tw + N);
+    const int tid = threadIdx.x;
+    const int gpk = ny / 2;
+    const size_t sk = (size_t)N * ny;
+    ct_build_twiddles<V, N, NT>(twg, tw, tid);
+    auto copy_rows = [&](double *dst, const double *src, int n) {
+        for (int e = tid * 2; e < n; e += NT * 2) cp_async_16(dst + e, src + e);
+    };
+    auto fetch = [&](int g) {
+        const int k = g / gpk, p = g % gpk, kg = k + 1;
+        const size_t r0 = sk * kg + (size_t)2 * p * N;
+        copy_rows(stage, d.u + r0, 2 * N);
+        copy_rows(stage + 2 * N, d.v + sk * kg + (size_t)(p == 0 ? ny - 1 : 2 * p - 1) * N, N);
+        copy_rows(stage + 3 * N, d.v + r0, 2 * N);
+        copy_rows(stage + 5 * N, d.w + r0, 2 * N);
+        copy_rows(stage + 7 * N, d.w + r0 - sk, 2 * N);
+        cp_async_commit();
+    };
+    if (blockIdx.x < total) fetch(blockIdx.x);
+    for (int g = blockIdx.x; g < total; g += gridDim.x) {
+        const int k = g / gpk, p = g % gpk;
+        const double dtidzi_k = __ldg(d.dzf_inv + k + 1);
+        cp_async_wait<0>();
+        __syncthreads();
+        double acc = 0.0;
+        auto in = [&](int, int m) {
+            const int mm = (m == 0) ? N - 1 : m - 1;
+            const double *u0 = stage, *u1 = stage + N, *vm = stage + 2 * N, *v0 = stage + 3 * N, *v1 = stage + 4 * N;
+            const double *w0 = stage + 5 * N, *w1 = stage + 6 * N, *w0m = stage + 7 * N, *w1m = stage + 8 * N;
+            const double r0 = (u0[m] - u0[mm]) * d.dtidxi + (v0[m] - vm[m]) * d.dtidyi + (w0[m] - w0m[m]) * d.dti * dtidzi_k;
+            const double r1 = (u1[m] - u1[mm]) * d.dtidxi + (v1[m] - v0[m]) * d.dtidyi + (w1[m] - w1m[m]) * d.dti * dtidzi_k;
+            acc += r0 + r1;
+            V z;
+            z.x = (T)r0;
+            z.y = (T)r1;
+            return z;
+        };
+        ct_first_stage<V, true, false, N, 1, 1, N, NT>(buf, 1, in, tid);
+        if (part != nullptr) { // the group's sum, in a fixed order
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+            if ((tid & 31) == 0) wsum[tid >> 5] = acc;
+        }
+        __syncthreads();
+        if (part != nullptr && tid == 0) part[g] = wsum[0] + wsum[1];
+        if (g + (int)gridDim.x < total) fetch(g + gridDim.x);
+        T *dst = out + (size_t)k * N * ny + (size_t)2 * p * N;
+        ct_batch_ip<V, true, false, N, 1, 1, N, NT, 1, ct_nstages(N) - 1>(buf, 1, tw, tid);
+        auto put = [&](int, int m, V A, V Bc) {
+            const V h = split_hc(A, Bc, m, N);
+            dst[m] = h.x;
+            dst[N + m] = h.y;
+        };
+        ct_last_stage_pairs<V, true, false, N, 1, 1, N, NT>(buf, 1, tw, tid, put);
+    }
+    cp_async_wait<0>();
+}
+
 // ------------------------------------------------------------------------
 // Tridiagonal kernels (FP64 arithmetic in both precision modes)
 // ------------------------------------------------------------------------
@@ -1122,6 +1209,49 @@ int ppe_solve_fp64_strided(Ppe *s, const double *in, double *out, size_t off, si
     if (launch_y<double>(s, false, d_work, st)) return -1;
     mark(s, "ppe_yfft_bwd");
     if (launch_x<double>(s, false, d_work, 0, nxl, nxy, out, off, sj, sk, s->norm, st)) return -1;
+    mark(s, "ppe_xfft_bwd");
+    return 0;
+}
+
+template <typename T, int N> static int launch_xdiv(Ppe *s, const DivIn &d, T *out, double *part, cudaStream_t st)
+{
+    using V = typename cplx_of<T>::type;
+    constexpr int shm = xdiv_smem_bytes<T, N>();
+    const V *tw = reinterpret_cast<const V *>(sizeof(T) == 8 ? (const void *)s->d_twx64 : (const void *)s->d_twx32);
+    if (shm > 48 * 1024)
+        PL_CUDA_TRY(cudaFuncSetAttribute(k_xfft_div_pf<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm));
+    const int total = (s->ny / 2) * s->nz;
+    k_xfft_div_pf<T, N><<<persistent_grid(k_xfft_div_pf<T, N>, shm, total, XDIV_THREADS), XDIV_THREADS, shm, st>>>(
+        d, out, tw, s->ny, total, part);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
+template <typename T> int ppe_xfwd_div(Ppe *s, const DivIn &d, T *out, double *part, cudaStream_t st)
+{
+    switch (s->nx) {
+#define PL_XDIV_CASE(n)                                                                                               \
+    case n:                                                                                                          \
+        return launch_xdiv<T, n>(s, d, out, part, st);
+        PL_FFT_CT_SIZES(PL_XDIV_CASE)
+#undef PL_XDIV_CASE
+    default:
+        return 1;
+    }
+}
+template int ppe_xfwd_div<double>(Ppe *, const DivIn &, double *, double *, cudaStream_t);
+template int ppe_xfwd_div<float>(Ppe *, const DivIn &, float *, double *, cudaStream_t);
+
+int ppe_solve_fp64_from_x(Ppe *s, double *d_var, cudaStream_t st)
+{
+    const size_t nxl = s->nx, nxy = (size_t)s->nx * s->ny;
+    if (launch_y<double>(s, true, d_var, st)) return -1;
+    mark(s, "ppe_yfft_fwd");
+    if (launch_trid<double>(s, d_var, st)) return -1;
+    mark(s, s->nparts ? "ppe_pdd" : "ppe_thomas");
+    if (launch_y<double>(s, false, d_var, st)) return -1;
+    mark(s, "ppe_yfft_bwd");
+    if (launch_x<double>(s, false, d_var, 0, nxl, nxy, d_var, 0, nxl, nxy, s->norm, st)) return -1;
     mark(s, "ppe_xfft_bwd");
     return 0;
 }

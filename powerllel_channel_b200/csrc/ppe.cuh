@@ -64,6 +64,25 @@ int ppe_solve_fp64(Ppe *s, double *d_var, cudaStream_t st);
 // allows (one kernel otherwise): p_new = (incremental ? q : 0) + dp stored
 // in p (in place of p_n), and the next prediction qnext = qmode ?
 // 2 p_new - p_n : p_new (FP64, interior-only layout).
+// The ghosted velocity fields and factors of calcRHS
+// (rhs = (u_i - u_{i-1}) dt^-1 dx^-1 + (v_j - v_{j-1}) dt^-1 dy^-1
+//        + (w_k - w_{k-1}) dt^-1 dzf_k^-1, mod_calcRHS.f90:19-33) for the
+// forward x transform with calcRHS fused in; dtidxi = (1/dt) (1/dx),
+// dtidyi = (1/dt) (1/dy), dti = 1/dt as the stencil kernels form them.
+struct DivIn {
+    const double *u, *v, *w; // [k = 0..nz+1][j][i]
+    const double *dzf_inv;   // index 0..nz+1
+    double dtidxi, dtidyi, dti;
+};
+// Forward x transform of rhs = div(u)/dt computed on the fly, into the
+// interior-only array out (T = double: the FP64 solve's, float: the mixed
+// one's); part (optional, nz * ny/2 doubles): per line pair, the FP64 sum of
+// its rhs values.  Returns 1 (nothing launched) where the fused kernel does
+// not apply: nx not a compile-time transform length.
+template <typename T> int ppe_xfwd_div(Ppe *s, const DivIn &d, T *out, double *part, cudaStream_t st);
+// FP64 solve when d_var already holds the forward x transform
+int ppe_solve_fp64_from_x(Ppe *s, double *d_var, cudaStream_t st);
+
 struct PressureUpdate {
     const double *q = nullptr;
     double *p = nullptr, *qnext = nullptr;

@@ -708,6 +708,13 @@ int warp_partials_per_plane(const StepParams &p)
     return (int)(g.x * g.y) * ((RHS_BX * RHS_BY) / 32);
 }
 
+int launch_plane_sums(const double *part, int nper, int nz, double *mode0, cudaStream_t st)
+{
+    k_plane_sums<<<nz, 256, 0, st>>>(part, nper, nz, mode0);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
 int launch_rhs_mixed(const double *u, const double *v, const double *w, float *r, double *warp_part, double *mode0,
                      const StepParams &p, const MeshDev &m, cudaStream_t st)
 {

@@ -78,6 +78,8 @@ int launch_rk2_mixed(const double *u, const double *v, const double *w, const fl
 int launch_rhs_mixed(const double *u, const double *v, const double *w, float *r, double *warp_part, double *mode0,
                      const StepParams &p, const MeshDev &m, cudaStream_t st);
 int warp_partials_per_plane(const StepParams &p);
+// mode0[k] = sum over the nper partials of plane k, in a fixed order
+int launch_plane_sums(const double *part, int nper, int nz, double *mode0, cudaStream_t st);
 
 // diagnostics: out[0] = max|div| , out[1] = max CFL (already * dt), out[2] =
 // NaN count over u,v,w (ghosts included); loc[0..2] ijk of the div max,
