@@ -41,17 +41,15 @@ WORKLOAD = "channel 512x384x256, Re_tau 1000, tanh stretch 2.0, Thomas, dt 1e-4,
 # and the solution once each, plus its two FP64 class tables (mult, 1/b),
 # each row of which serves four columns: 2 x 8 B / 4 = 4 B per point.
 # rhs_xfft: calcRHS fused into the forward x transform (u, v, w read once,
-# the transform written once).  rk_fused: the step defers its correction
-# into the next step's RK kernel, which then also reads p (FP64) or the FP32
-# pressure increment (mixed) once.
+# the transform written once)
 ALG_BYTES = {
-    "fp64": {"rk_fused": 56, "rk1": 48, "rk2": 72, "calc_rhs": 32, "rhs_xfft": 32, "ppe_xfft_fwd": 16, "ppe_yfft_fwd": 16,
+    "fp64": {"rk_fused": 48, "rk1": 48, "rk2": 72, "calc_rhs": 32, "rhs_xfft": 32, "ppe_xfft_fwd": 16, "ppe_yfft_fwd": 16,
              "ppe_thomas": 20, "ppe_pdd": 40, "ppe_yfft_bwd": 16, "ppe_xfft_bwd": 16, "correct_force": 56},
-    "mixed": {"rk_fused": 60, "rk1": 36, "rk2": 68, "calc_rhs": 28, "rhs_xfft": 28, "ppe_xfft_fwd": 8, "ppe_yfft_fwd": 8,
+    "mixed": {"rk_fused": 56, "rk1": 36, "rk2": 68, "calc_rhs": 28, "rhs_xfft": 28, "ppe_xfft_fwd": 8, "ppe_yfft_fwd": 8,
               "ppe_thomas": 12, "ppe_pdd": 32, "ppe_yfft_bwd": 8, "ppe_xfft_bwd": 40, "correct_force": 52},
 }
 # kernel launches per step (this library's kernels only)
-LAUNCHES = {"fp64": 6, "mixed": 7}
+LAUNCHES = {"fp64": 7, "mixed": 8}
 
 
 def peaks():
@@ -324,9 +322,6 @@ def run_b200(args):
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "precision": "mixed", "grid": [NX, NY, NZ],
                        "l2": "inputs larger than L2 (403 MB per FP64 field), no flush",
-                       "correction": "each step's correctVel + forceVel is applied by the next step's RK kernel "
-                                     "as it loads u; the K timed steps apply K corrections, the first one the "
-                                     "last warm-up step's; e2e downloads apply it before the copy",
                        "parallelism": "1 GPU" if world == 1 else f"{world} independent replicas"},
             "fp64_steps_per_s": sps64, "fp64_ms_per_step": ms64 / args.steps,
             "mixed_over_fp64": spsm / sps64,

@@ -126,15 +126,7 @@ int pl_channel_destroy(pl_channel *c);
  * splitmix64(seed + (n+1)*0x9E3779B97F4A7C15) >> 11 scaled by 2^-53), then
  * transform2CRF and the boundary fills (main.f90:98-102). */
 int pl_channel_init_flow(pl_channel *c, uint64_t seed, double noise_intensity);
-/* nsteps RK2 projection steps, asynchronous on the channel's stream.  Where
- * the fused RK kernel applies (nx % 32 == 0, ny % 8 == 0), each step's
- * correctVel + forceVel + updateBoundVel is deferred into the next step's RK
- * kernel, which applies it to u, v, w as it loads them; every entry below
- * that reads the fields (diagnostics, getters, pl_channel_field, statistics,
- * monitors, the adjoint) first applies a pending correction, so callers
- * always see the corrected fields.  Calculation of the right-hand side is
- * fused into the Poisson solve's forward x transform where nx is one of the
- * compile-time transform lengths. */
+/* nsteps RK2 projection steps, asynchronous on the channel's stream */
 int pl_channel_step(pl_channel *c, int nsteps);
 int pl_channel_synchronize(pl_channel *c);
 int pl_channel_diagnostics(pl_channel *c, pl_diag *out);
@@ -153,9 +145,7 @@ int pl_channel_upload_compact(pl_channel *c, const double *uvw);
 int pl_channel_download_compact(pl_channel *c, double *uvw);
 /* device pointers of the current fields (for per-phase entries and tests):
  * which = 0..2 u,v,w (FP64, nx*ny*(nz+2)), 3 = p (interior), 4..6 = stage-1
- * fields u1,v1,w1 (FP64 path) or stage-1 increments (mixed path, FP32).
- * Applies a pending correction first; the pointers of u, v, w change with
- * every step (double buffering), so fetch them again after stepping. */
+ * fields u1,v1,w1 (FP64 path) or stage-1 increments (mixed path, FP32) */
 void *pl_channel_field(pl_channel *c, int which);
 void *pl_channel_stream(pl_channel *c);
 
@@ -169,8 +159,7 @@ int pl_phase_rk1(pl_channel *c);        /* timeIntVelRK1 + updateBoundVel(u1) */
 int pl_phase_rk2(pl_channel *c);        /* timeIntVelRK2 + updateBoundVel(u) */
 int pl_phase_calc_rhs(pl_channel *c);   /* calcRHS into p */
 int pl_phase_poisson(pl_channel *c);    /* execute_poisson_solver(p) */
-int pl_phase_correct_force(pl_channel *c); /* updateBoundP, correctVel, forceVel, updateBoundVel
-                                              (applied at once; pl_channel_step defers it) */
+int pl_phase_correct_force(pl_channel *c); /* updateBoundP, correctVel, forceVel, updateBoundVel */
 
 /* Per-kernel device time: runs nsteps steps with a CUDA event between every
  * kernel launch (same kernels and order as pl_channel_step) and writes the

@@ -13,7 +13,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libpowerllel_b200.so")
 SOURCES = ["ppe.cu", "stencil.cu", "rk_fused.cu", "channel.cu", "adjoint.cu", "monitor.cu"]
-HEADERS = ["common.cuh", "fft.cuh", "ppe.cuh", "stencil.cuh", "stencil_rhs.cuh", "trid_tables.h", "channel.cuh"]
+HEADERS = ["common.cuh", "fft.cuh", "ppe.cuh", "stencil.cuh", "stencil_rhs.cuh", "tmem.cuh", "trid_tables.h", "channel.cuh"]
 
 NVCC_FLAGS = [
     "-std=c++17", "-O3", "-lineinfo",

@@ -357,7 +357,6 @@ extern "C" int pl_channel_set_body_force(pl_channel *c, const double f[3])
 
 extern "C" int pl_channel_kinetic_energy(pl_channel *c, double *ke)
 {
-    if (channel_settle(c)) return -1;
     double *part = nullptr, *out = nullptr;
     PL_CUDA_TRY(cudaMalloc(&part, sizeof(double) * (3 * SUM_PARTS * (size_t)c->nz + 4)));
     out = part + 3 * SUM_PARTS * (size_t)c->nz;
@@ -407,9 +406,7 @@ extern "C" int pl_adjoint_ke_gradient(pl_channel *c, int nsteps, int every, doub
     W.fbar = W.scal + 4;
     auto state = [&](double *base, int slot) { return base + 3 * nf * (size_t)slot; };
 
-    // forward sweep with checkpoints (each step's correction applied at once:
-    // the checkpoints hold the corrected fields)
-    if (channel_settle(c)) return -1;
+    // forward sweep with checkpoints
     if (launch_fill_bc_vel(c->u, c->v, c->w, p, st)) return -1;
     if (copy3(state(W.ck, 0), state(W.ck, 0) + nf, state(W.ck, 0) + 2 * nf, c->u, c->v, c->w, nf, st)) return -1;
     for (int n = 0; n < nsteps; n++) {
@@ -417,7 +414,7 @@ extern "C" int pl_adjoint_ke_gradient(pl_channel *c, int nsteps, int every, doub
             double *s = state(W.ck, n / every);
             if (copy3(s, s + nf, s + 2 * nf, c->u, c->v, c->w, nf, st)) return -1;
         }
-        if (pl_channel_step(c, 1) || channel_settle(c)) return -1;
+        if (pl_channel_step(c, 1)) return -1;
     }
     double *keout = W.scal + 8;
     if (level_sums(1, c->u, c->v, c->w, c, W.part, 1.0, 0, keout)) return -1;
@@ -434,12 +431,11 @@ extern "C" int pl_adjoint_ke_gradient(pl_channel *c, int nsteps, int every, doub
     for (int s = nck - 1; s >= 0; s--) {
         const int n0 = s * every, n1 = std::min(nsteps, n0 + every);
         const double *ck = state(W.ck, s);
-        channel_discard_pending(c);
         if (copy3(c->u, c->v, c->w, ck, ck + nf, ck + 2 * nf, nf, st)) return -1;
         for (int n = n0; n < n1; n++) {
             double *x = state(W.seg, n - n0);
             if (copy3(x, x + nf, x + 2 * nf, c->u, c->v, c->w, nf, st)) return -1;
-            if (n < n1 - 1 && (pl_channel_step(c, 1) || channel_settle(c))) return -1;
+            if (n < n1 - 1 && pl_channel_step(c, 1)) return -1;
         }
         for (int n = n1 - 1; n >= n0; n--) {
             const double *x = state(W.seg, n - n0);
@@ -450,7 +446,6 @@ extern "C" int pl_adjoint_ke_gradient(pl_channel *c, int nsteps, int every, doub
     // results; the fields are left at the initial state
     if (copy3(d_gu, d_gv, d_gw, W.xa, W.xa + nf, W.xa + 2 * nf, nf, st)) return -1;
     const double *x0 = state(W.ck, 0);
-    channel_discard_pending(c);
     if (copy3(c->u, c->v, c->w, x0, x0 + nf, x0 + 2 * nf, nf, st)) return -1;
     PL_CUDA_TRY(cudaMemcpyAsync(grad_f, W.fbar, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
     PL_CUDA_TRY(cudaStreamSynchronize(st));

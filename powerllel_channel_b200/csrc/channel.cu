@@ -344,7 +344,7 @@ extern "C" int pl_channel_create(pl_channel **out, const pl_channel_config *cfg)
     if (c->fused_rk && rk_fused_blocks(c->sp) > c->max_blocks) c->max_blocks = rk_fused_blocks(c->sp);
     c->rb.max_blocks = c->max_blocks;
     if (cudaMalloc(&c->rb.partial, sizeof(double) * 3 * c->max_blocks) != cudaSuccess ||
-        cudaMalloc(&c->rb.scalar, sizeof(double) * 16) != cudaSuccess ||
+        cudaMalloc(&c->rb.scalar, sizeof(double) * 8) != cudaSuccess ||
         cudaMalloc(&c->d_diag, sizeof(double) * 4) != cudaSuccess ||
         cudaMalloc(&c->d_loc, sizeof(int) * 8) != cudaSuccess ||
         cudaMalloc(&c->d_dpart, sizeof(double) * 3 * c->max_blocks) != cudaSuccess ||
@@ -355,7 +355,7 @@ extern "C" int pl_channel_create(pl_channel **out, const pl_channel_config *cfg)
         return fail();
     }
     cudaMemset(c->ms.counter, 0, sizeof(unsigned int));
-    cudaMemset(c->rb.scalar, 0, sizeof(double) * 16);
+    cudaMemset(c->rb.scalar, 0, sizeof(double) * 8);
     c->ms.scalar = c->rb.scalar;
     c->ms.max_blocks = c->max_blocks;
     c->ms.vel_force = cfg->vel_force[0];
@@ -392,7 +392,6 @@ extern "C" int pl_channel_init_flow(pl_channel *c, uint64_t seed, double noise)
     if (c->pb) PL_CUDA_TRY(cudaMemsetAsync(c->pb, 0, sizeof(double) * c->np, c->stream));
     if (c->pm) PL_CUDA_TRY(cudaMemsetAsync(c->pm, 0, sizeof(double) * c->np, c->stream));
     c->nsolve = 0;
-    channel_discard_pending(c);
     int rc = launch_init_fill(c->u, c->v, c->w, dprof, seed, noise, c->sp, c->stream);
     if (!rc) rc = launch_mean_sum(c->u, c->sp, c->m, c->rb, 0, c->stream);
     if (!rc) rc = launch_init_finish(c->u, c->v, c->w, c->sp, c->cfg.u_ref, c->rb, c->stream);
@@ -413,38 +412,8 @@ static inline bool is_mixed(const pl_channel *c) { return c->cfg.precision == PL
 // correction uses the FP32 increment alone.
 static int mixed_incremental(const pl_channel *c) { return (c->incremental && c->nsolve >= 2) ? 1 : 0; }
 
-// The RK kernels' Mean_h reduction writes one of two scalar sets in turn,
-// so a kernel that applies the previous step's deferred forcing shift reads
-// the set that it does not write.
-static void next_mean_set(pl_channel *c)
-{
-    c->ms.scalar = (c->ms.scalar == c->rb.scalar) ? c->rb.scalar + 8 : c->rb.scalar;
-}
-
-// after the correction (applied or deferred): the mixed path's prediction
-// written by the solve becomes the next step's
-static void end_projection(pl_channel *c)
-{
-    if (is_mixed(c)) {
-        std::swap(c->pm, c->pb);
-        c->nsolve++;
-    }
-}
-
-int channel_settle(pl_channel *c)
-{
-    if (!c->pending) return 0;
-    c->pending = false;
-    // mixed: the RK kernel applied -dt G p_pred, the increment remains
-    return is_mixed(c) ? launch_correct_force_f32(c->r32, c->u, c->v, c->w, c->sp, c->m, c->cfg.is_forced[0],
-                                                  c->ms.scalar, c->stream)
-                       : launch_correct_force_fp64(c->p, c->u, c->v, c->w, c->sp, c->m, c->cfg.is_forced[0],
-                                                   c->ms.scalar, c->stream);
-}
-
 extern "C" int pl_phase_rk1(pl_channel *c)
 {
-    if (channel_settle(c)) return -1;
     int rc = is_mixed(c) ? launch_rk1_mixed(c->u, c->v, c->w, c->d1u, c->d1v, c->d1w, c->sp, c->m, c->stream)
                          : launch_rk1_fp64(c->u, c->v, c->w, c->u1, c->v1, c->w1, c->sp, c->m, c->stream);
     channel_mark(c, "rk1");
@@ -453,8 +422,6 @@ extern "C" int pl_phase_rk1(pl_channel *c)
 
 extern "C" int pl_phase_rk2(pl_channel *c)
 {
-    if (channel_settle(c)) return -1;
-    next_mean_set(c);
     int rc;
     if (is_mixed(c)) {
         rc = launch_rk2_mixed(c->u, c->v, c->w, c->d1u, c->d1v, c->d1w, c->ub, c->vb, c->wb, c->sp, c->m, c->ms,
@@ -471,7 +438,6 @@ extern "C" int pl_phase_rk2(pl_channel *c)
 
 extern "C" int pl_phase_calc_rhs(pl_channel *c)
 {
-    if (channel_settle(c)) return -1;
     int rc;
     if (is_mixed(c))
         rc = launch_rhs_mixed(c->u, c->v, c->w, c->r32, c->plane_part, c->mode0, c->sp, c->m, c->stream);
@@ -541,9 +507,15 @@ static int phase_rhs_poisson(pl_channel *c)
 
 extern "C" int pl_phase_correct_force(pl_channel *c)
 {
-    c->pending = true; // this step's correction, applied now
-    const int rc = channel_settle(c);
-    end_projection(c);
+    // mixed: the RK kernel applied -dt G p_pred, the increment remains
+    const int rc = is_mixed(c) ? launch_correct_force_f32(c->r32, c->u, c->v, c->w, c->sp, c->m,
+                                                          c->cfg.is_forced[0], c->ms.scalar, c->stream)
+                               : launch_correct_force_fp64(c->p, c->u, c->v, c->w, c->sp, c->m, c->cfg.is_forced[0],
+                                                           c->ms.scalar, c->stream);
+    if (is_mixed(c)) {
+        std::swap(c->pm, c->pb); // the prediction written by the solve
+        c->nsolve++;
+    }
     channel_mark(c, "correct_force");
     return rc;
 }
@@ -557,23 +529,9 @@ extern "C" int pl_phase_rk(pl_channel *c)
         if (!rc) rc = pl_phase_rk2(c);
         return rc;
     }
-    // a deferred correction of the previous step is applied as the kernel loads u
-    PendCorr pc{};
-    const PendCorr *pend = nullptr;
-    if (c->pending) {
-        pc.p = is_mixed(c) ? (const void *)c->r32 : (const void *)c->p;
-        pc.shift = c->cfg.is_forced[0] ? c->ms.scalar + 3 : nullptr;
-        pc.dt = c->sp.dt;
-        pc.dtdxi = c->sp.dt * c->sp.dx_inv;
-        pc.dtdyi = c->sp.dt * c->sp.dy_inv;
-        pend = &pc;
-        c->pending = false;
-    }
-    next_mean_set(c);
     rc = is_mixed(c) ? launch_rk_fused_mixed(c->u, c->v, c->w, c->ub, c->vb, c->wb, c->sp, c->m, c->ms, c->pm,
-                                             mixed_incremental(c), c->stream, pend)
-                     : launch_rk_fused_fp64(c->u, c->v, c->w, c->ub, c->vb, c->wb, c->sp, c->m, c->ms, c->stream,
-                                            pend);
+                                             mixed_incremental(c), c->stream)
+                     : launch_rk_fused_fp64(c->u, c->v, c->w, c->ub, c->vb, c->wb, c->sp, c->m, c->ms, c->stream);
     std::swap(c->u, c->ub);
     std::swap(c->v, c->vb);
     std::swap(c->w, c->wb);
@@ -628,13 +586,7 @@ extern "C" int pl_channel_profile(pl_channel *c, int nsteps, double *ms, char *n
 extern "C" int pl_channel_step(pl_channel *c, int nsteps)
 {
     for (int s = 0; s < nsteps; s++) {
-        if (pl_phase_rk(c) || phase_rhs_poisson(c)) return -1;
-        if (c->fused_rk) { // the correction goes into the next RK kernel's loads
-            c->pending = true;
-            end_projection(c);
-        } else if (pl_phase_correct_force(c)) {
-            return -1;
-        }
+        if (pl_phase_rk(c) || phase_rhs_poisson(c) || pl_phase_correct_force(c)) return -1;
     }
     return 0;
 }
@@ -647,7 +599,6 @@ extern "C" int pl_channel_synchronize(pl_channel *c)
 
 extern "C" int pl_channel_diagnostics(pl_channel *c, pl_diag *out)
 {
-    if (channel_settle(c)) return -1;
     if (launch_diagnostics_fp64(c->u, c->v, c->w, c->sp, c->m, c->d_diag, c->d_loc, c->d_dpart, c->d_dipart,
                                 c->max_blocks, c->stream))
         return -1;
@@ -688,7 +639,6 @@ static void expand_ghosted(const pl_channel *c, const double *src, double *dst, 
 
 extern "C" int pl_channel_get_fields(pl_channel *c, double *u, double *v, double *w, double *p)
 {
-    if (channel_settle(c)) return -1;
     PL_CUDA_TRY(cudaStreamSynchronize(c->stream));
     std::vector<double> tmp(c->nf);
     double *dev[3] = {c->u, c->v, c->w};
@@ -708,7 +658,6 @@ extern "C" int pl_channel_get_fields(pl_channel *c, double *u, double *v, double
 
 extern "C" int pl_channel_get_field(pl_channel *c, int which, double *host)
 {
-    if (channel_settle(c)) return -1;
     PL_CUDA_TRY(cudaStreamSynchronize(c->stream));
     if (which < 0 || which > 6 || !host) {
         set_error("pl_channel_get_field: which must be 0..6");
@@ -739,7 +688,6 @@ extern "C" int pl_channel_get_field(pl_channel *c, int which, double *host)
 
 extern "C" int pl_channel_set_fields(pl_channel *c, const double *u, const double *v, const double *w)
 {
-    channel_discard_pending(c);
     PL_CUDA_TRY(cudaStreamSynchronize(c->stream));
     c->nsolve = 0; // a new state: the pressure history no longer applies
     const int nx = c->nx, ny = c->ny, nz = c->nz;
@@ -760,7 +708,6 @@ extern "C" int pl_channel_set_fields(pl_channel *c, const double *u, const doubl
 
 extern "C" int pl_channel_upload_compact(pl_channel *c, const double *uvw)
 {
-    channel_discard_pending(c);
     double *dev[3] = {c->u, c->v, c->w};
     for (int q = 0; q < 3; q++)
         PL_CUDA_TRY(cudaMemcpyAsync(dev[q], uvw + q * c->nf, sizeof(double) * c->nf, cudaMemcpyHostToDevice,
@@ -770,7 +717,6 @@ extern "C" int pl_channel_upload_compact(pl_channel *c, const double *uvw)
 
 extern "C" int pl_channel_download_compact(pl_channel *c, double *uvw)
 {
-    if (channel_settle(c)) return -1;
     double *dev[3] = {c->u, c->v, c->w};
     for (int q = 0; q < 3; q++)
         PL_CUDA_TRY(cudaMemcpyAsync(uvw + q * c->nf, dev[q], sizeof(double) * c->nf, cudaMemcpyDeviceToHost,
@@ -780,7 +726,6 @@ extern "C" int pl_channel_download_compact(pl_channel *c, double *uvw)
 
 extern "C" void *pl_channel_field(pl_channel *c, int which)
 {
-    if (channel_settle(c)) return nullptr;
     switch (which) {
     case 0: return c->u;
     case 1: return c->v;

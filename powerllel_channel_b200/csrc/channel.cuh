@@ -32,11 +32,6 @@ struct pl_channel {
     int incremental = 1;   // mixed path: solve for a pressure increment (Thomas)
     long long nsolve = 0;  // projections since the initial field (mixed prediction schedule)
     bool fused_rk = false; // both RK stages in one kernel (rk_fused.cu)
-    // The step defers its correctVel + forceVel into the next step's RK
-    // kernel (fused grids): u, v, w then hold the RK output u* and `pending`
-    // is set.  Every reader of the fields settles it first (channel_settle);
-    // every writer discards it.
-    bool pending = false;
     pl::Ppe ppe;
     pl::ReduceBuf rb;
     pl::MeanState ms;
@@ -51,8 +46,3 @@ struct pl_channel {
     std::vector<cudaEvent_t> *prof_events = nullptr;
     std::vector<std::string> *prof_names = nullptr;
 };
-
-// Apply a deferred correction to u, v, w (no-op when none is pending).
-int channel_settle(pl_channel *c);
-// Forget a deferred correction: the fields are about to be overwritten.
-inline void channel_discard_pending(pl_channel *c) { c->pending = false; }

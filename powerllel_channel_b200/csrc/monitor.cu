@@ -184,7 +184,6 @@ extern "C" int pl_stat_init(pl_channel *c)
 
 extern "C" int pl_stat_sample(pl_channel *c, int nt)
 {
-    if (channel_settle(c)) return -1;
     pl_stats *s = stats_of(c);
     if (!s) {
         set_error("pl_stat_sample: statistics not enabled");
@@ -241,7 +240,6 @@ extern "C" int pl_stat_disable(pl_channel *c)
 // ---------------------------------------------------------------------------
 extern "C" int pl_monitor_skin_friction(pl_channel *c, int wall, double *u_tau, double *cf)
 {
-    if (channel_settle(c)) return -1;
     if (wall != 0 && wall != 1) {
         set_error("pl_monitor_skin_friction: wall must be 0 (bottom) or 1 (top)");
         return -1;
@@ -272,7 +270,6 @@ extern "C" int pl_monitor_skin_friction(pl_channel *c, int wall, double *u_tau, 
 
 extern "C" int pl_monitor_forcing(pl_channel *c, double vel_mean[3])
 {
-    if (channel_settle(c)) return -1;
     // calcAndWriteForcing (:298-318): Mean_h of the forced components, u_crf added to u
     double *part = nullptr;
     PL_CUDA_TRY(cudaMalloc(&part, sizeof(double) * ((size_t)c->nz + 1)));
@@ -298,7 +295,6 @@ extern "C" int pl_monitor_forcing(pl_channel *c, double vel_mean[3])
 
 extern "C" int pl_monitor_probe(pl_channel *c, int i, int j, int k, double out[4])
 {
-    if (channel_settle(c)) return -1;
     // extractAndWriteProbePoint (:197-219): u + u_crf, v, w, p at (i, j, k), 1-based
     if (i < 1 || i > c->nx || j < 1 || j > c->ny || k < 1 || k > c->nz) {
         set_error("pl_monitor_probe: the point is outside the domain");
@@ -316,7 +312,6 @@ extern "C" int pl_monitor_probe(pl_channel *c, int i, int j, int k, double out[4
 
 extern "C" int pl_monitor_region(pl_channel *c, const int ijk[6], double *host_uvwp)
 {
-    if (channel_settle(c)) return -1;
     // extractAndWriteRegion (:320-376) with the region clipped to the domain
     // as initMonitor does (:120-126); host_uvwp receives u, v, w, p one after
     // the other, each [k][j][i] over the clipped region

@@ -14,8 +14,6 @@
 // d1 = dt*RHS(u) and u1 = u + d1, all in float (FP32 stencil arithmetic); the
 // update u_new = ((u + d1) + dt*RHS(u1) + u)/2 uses the FP64 u of the centre
 // and is stored in FP64.
-#include <type_traits>
-
 #include "stencil.cuh"
 #include "stencil_rhs.cuh"
 
@@ -81,14 +79,12 @@ __device__ __forceinline__ Nb32 ring_nb(int x, int y, int s0, int sm, int sp)
     return n;
 }
 
-// PEND: u, v, w are the previous step's RK output u* with its correctVel +
-// forceVel + wall fill still to apply (PendCorr); every load applies it.
-template <bool MIXED, bool CRF, bool PEND>
+template <bool MIXED, bool CRF>
 __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double *__restrict__ u, const double *__restrict__ v,
                                                      const double *__restrict__ w, double *__restrict__ uo,
                                                      double *__restrict__ vo, double *__restrict__ wo, StepParams p,
                                                      MeshDev m, MeanRed red, int kchunk,
-                                                     const double *__restrict__ pq, int pinc, PendCorr pend)
+                                                     const double *__restrict__ pq, int pinc)
 {
     using R = typename RkTraits<MIXED>::R;
     constexpr int NS = RkTraits<MIXED>::NS;
@@ -119,7 +115,6 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
     static_assert(FX == 32 && FY == 8 && UW == 36 && UH == 12, "slot maps of the 32 x 8 tile");
     const int lane = tx, wid = ty;
     int loff[2], lxy[2];
-    unsigned ledge = 0; // bit 2 sl: gi == nx-1, bit 2 sl + 1: gj == ny-1 (the +1 neighbours wrap)
     bool lval1;
     {
         int lx[2], ly[2];
@@ -143,26 +138,8 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
             gj -= (gj >= p.ny) ? p.ny : 0;
             loff[sl] = gi + p.nx * gj;
             lxy[sl] = ly[sl] * UW + lx[sl];
-            ledge |= (gi == p.nx - 1 ? 1u : 0u) << (2 * sl);
-            ledge |= (gj == p.ny - 1 ? 1u : 0u) << (2 * sl + 1);
         }
     }
-    using TP = typename std::conditional<MIXED, float, double>::type;
-    const TP *__restrict__ pp = static_cast<const TP *>(pend.p);
-    const double bcu_d = 0.0 - p.u_crf;
-    // k_correct_force at the interior point (c: in-plane offset, cx / cy: its
-    // +1 neighbours in x / y) of plane k, applied to the loaded u, v, w
-    auto correct = [&](size_t c, size_t cx, size_t cy, int k, double &cu, double &cv, double &cw) {
-        const size_t pc = c + sk * (k - 1);
-        const double p0 = (double)__ldg(pp + pc);
-        const double pxp = (double)__ldg(pp + cx + sk * (k - 1)), pyp = (double)__ldg(pp + cy + sk * (k - 1));
-        const double pzp = (k < p.nz) ? (double)__ldg(pp + pc + sk) : p0;
-        double nu = cu - (pxp - p0) * pend.dtdxi;
-        if (pend.shift != nullptr) nu = nu + __ldg(pend.shift);
-        cu = nu;
-        cv = cv - (pyp - p0) * pend.dtdyi;
-        cw = cw - (pzp - p0) * pend.dt * __ldg(m.dzc_inv + k);
-    };
     auto load_u_plane = [&](int kq, int s) { // kq in [0, nz+1], into ring slot s = kq % NS
         const size_t gk = sk * kq;
 #pragma unroll
@@ -170,28 +147,9 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
             if (sl == 0 || lval1) {
                 const size_t g = gk + loff[sl];
                 const int q = s * UPS + lxy[sl];
-                if constexpr (PEND) {
-                    // a wall ghost plane is the fill of the corrected plane 1 / nz;
-                    // w keeps its ghost value
-                    const int kc = kq < 1 ? 1 : (kq > p.nz ? p.nz : kq);
-                    const size_t c = loff[sl];
-                    const size_t cx = c + ((ledge >> (2 * sl)) & 1u ? 1 - (long long)p.nx : 1);
-                    const size_t cy = c + ((ledge >> (2 * sl + 1)) & 1u ? (long long)p.nx * (1 - p.ny) : p.nx);
-                    double cu = __ldg(u + sk * kc + c), cv = __ldg(v + sk * kc + c), cw = __ldg(w + g);
-                    correct(c, cx, cy, kc, cu, cv, cw);
-                    if (kq != kc) {
-                        cu = 2.0 * bcu_d - cu;
-                        cv = -cv;
-                        cw = __ldg(w + g);
-                    }
-                    ur[0 * FS + q] = (R)cu;
-                    ur[1 * FS + q] = (R)cv;
-                    ur[2 * FS + q] = (R)cw;
-                } else {
-                    ur[0 * FS + q] = (R)__ldg(u + g);
-                    ur[1 * FS + q] = (R)__ldg(v + g);
-                    ur[2 * FS + q] = (R)__ldg(w + g);
-                }
+                ur[0 * FS + q] = (R)__ldg(u + g);
+                ur[1 * FS + q] = (R)__ldg(v + g);
+                ur[2 * FS + q] = (R)__ldg(w + g);
             }
         }
     };
@@ -263,12 +221,7 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
         const Nb32 n = ring_nb(tx + 2, ty + 2, s0, sm, sp);
         // global loads first, so their latency overlaps the stencil
         const size_t g = (size_t)(i0 + tx) + (size_t)p.nx * (j0 + ty) + sk * kq;
-        double uc = __ldg(u + g), vc = __ldg(v + g), wc = __ldg(w + g);
-        if constexpr (PEND) {
-            const int ip = (i0 + tx == p.nx - 1) ? 0 : i0 + tx + 1, jp = (j0 + ty == p.ny - 1) ? 0 : j0 + ty + 1;
-            const size_t c = (size_t)(i0 + tx) + (size_t)p.nx * (j0 + ty);
-            correct(c, (size_t)ip + (size_t)p.nx * (j0 + ty), (size_t)(i0 + tx) + (size_t)p.nx * jp, kq, uc, vc, wc);
-        }
+        const double uc = __ldg(u + g), vc = __ldg(v + g), wc = __ldg(w + g);
         double q0 = 0.0, qxp = 0.0, qyp = 0.0, qzp = 0.0;
         if (MIXED && pinc) { // u_hat = u* - dt G p_pred (FP64): its divergence is the increment's residual
             const int ip = (i0 + tx == p.nx - 1) ? 0 : i0 + tx + 1, jp = (j0 + ty == p.ny - 1) ? 0 : j0 + ty + 1;
@@ -398,7 +351,7 @@ static int sm_count_rk()
 template <bool MIXED>
 static int launch_rk_fused_t(const double *u, const double *v, const double *w, double *uo, double *vo, double *wo,
                              const StepParams &p, const MeshDev &m, MeanState &ms, cudaStream_t st,
-                             const double *pq, int pinc, const PendCorr *pend)
+                             const double *pq = nullptr, int pinc = 0)
 {
     if (!rk_fused_supported(p)) {
         set_error("fused RK kernel needs nx % 32 == 0 and ny % 8 == 0");
@@ -407,10 +360,7 @@ static int launch_rk_fused_t(const double *u, const double *v, const double *w, 
     using R = typename RkTraits<MIXED>::R;
     const size_t shm = sizeof(R) * (MIXED ? 9 : 6) * RkTraits<MIXED>::NS * UPS;
     // u_crf == 0 (the channel's usual frame) drops the frame-velocity terms
-    const bool pending = pend != nullptr && pend->p != nullptr;
-    auto kern = (p.u_crf != 0.0) ? (pending ? k_rk_fused<MIXED, true, true> : k_rk_fused<MIXED, true, false>)
-                                 : (pending ? k_rk_fused<MIXED, false, true> : k_rk_fused<MIXED, false, false>);
-    const PendCorr pc = pending ? *pend : PendCorr{nullptr, nullptr, 0.0, 0.0, 0.0};
+    auto kern = (p.u_crf != 0.0) ? k_rk_fused<MIXED, true> : k_rk_fused<MIXED, false>;
     PL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
     // prefer the largest shared-memory carve-out: several CTAs per SM
     PL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
@@ -426,22 +376,22 @@ static int launch_rk_fused_t(const double *u, const double *v, const double *w, 
         return -1;
     }
     MeanRed r{ms.partial, ms.counter, ms.scalar, (double)p.nx, (double)p.ny, ms.vel_force};
-    kern<<<grid, dim3(FX, FY), shm, st>>>(u, v, w, uo, vo, wo, p, m, r, kchunk, pq, pinc, pc);
+    kern<<<grid, dim3(FX, FY), shm, st>>>(u, v, w, uo, vo, wo, p, m, r, kchunk, pq, pinc);
     PL_CHECK_LAUNCH();
     return 0;
 }
 
 int launch_rk_fused_fp64(const double *u, const double *v, const double *w, double *uo, double *vo, double *wo,
-                         const StepParams &p, const MeshDev &m, MeanState &ms, cudaStream_t st, const PendCorr *pend)
+                         const StepParams &p, const MeshDev &m, MeanState &ms, cudaStream_t st)
 {
-    return launch_rk_fused_t<false>(u, v, w, uo, vo, wo, p, m, ms, st, nullptr, 0, pend);
+    return launch_rk_fused_t<false>(u, v, w, uo, vo, wo, p, m, ms, st);
 }
 
 int launch_rk_fused_mixed(const double *u, const double *v, const double *w, double *uo, double *vo, double *wo,
                           const StepParams &p, const MeshDev &m, MeanState &ms, const double *pq, int pinc,
-                          cudaStream_t st, const PendCorr *pend)
+                          cudaStream_t st)
 {
-    return launch_rk_fused_t<true>(u, v, w, uo, vo, wo, p, m, ms, st, pq, pinc, pend);
+    return launch_rk_fused_t<true>(u, v, w, uo, vo, wo, p, m, ms, st, pq, pinc);
 }
 
 } // namespace pl

@@ -49,27 +49,17 @@ struct MeanState {
     double vel_force = 0.0;
 };
 
-// The previous step's correctVel + forceVel + wall fill (k_correct_force),
-// deferred into the next fused RK kernel, which applies it to u, v, w as it
-// loads them, with k_correct_force's expressions.
-struct PendCorr {
-    const void *p;       // interior-only p (FP64 path) or the FP32 increment (mixed)
-    const double *shift; // forced x: the shift (vel_force - Mean_h) of the previous step; else null
-    double dtdxi, dtdyi, dt;
-};
-
 // fused RK1 + RK2 (rk_fused.cu): u -> (uo, vo, wo) out of place
 bool rk_fused_supported(const StepParams &p);
 int rk_fused_blocks(const StepParams &p);
 int launch_rk_fused_fp64(const double *u, const double *v, const double *w, double *uo, double *vo, double *wo,
-                         const StepParams &p, const MeshDev &m, MeanState &ms, cudaStream_t st,
-                         const PendCorr *pend = nullptr);
+                         const StepParams &p, const MeshDev &m, MeanState &ms, cudaStream_t st);
 // mixed: with pinc, u_hat = u* - dt G pq (pq: the pressure prediction,
 // interior-only layout) is stored, whose divergence / dt is the increment's
 // residual
 int launch_rk_fused_mixed(const double *u, const double *v, const double *w, double *uo, double *vo, double *wo,
                           const StepParams &p, const MeshDev &m, MeanState &ms, const double *pq, int pinc,
-                          cudaStream_t st, const PendCorr *pend = nullptr);
+                          cudaStream_t st);
 
 int launch_rk2m_fp64(double *u, double *v, double *w, const double *u1, const double *v1, const double *w1,
                      const StepParams &p, const MeshDev &m, MeanState &ms, cudaStream_t st);
