@@ -14,6 +14,7 @@
 // d1 = dt*RHS(u) and u1 = u + d1, all in float (FP32 stencil arithmetic); the
 // update u_new = ((u + d1) + dt*RHS(u1) + u)/2 uses the FP64 u of the centre
 // and is stored in FP64.
+#include "fft.cuh" // cp.async helpers
 #include "stencil.cuh"
 #include "stencil_rhs.cuh"
 
@@ -154,6 +155,23 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
         }
     };
 
+    // FP64 rings hold the fields as loaded: the plane can be copied
+    // asynchronously (cp.async), in flight while stage 2 runs
+    auto load_u_plane_async = [&](int kq, int s) {
+        const size_t gk = sk * kq;
+#pragma unroll
+        for (int sl = 0; sl < 2; sl++) {
+            if (sl == 0 || lval1) {
+                const size_t g = gk + loff[sl];
+                const int q = s * UPS + lxy[sl];
+                cp_async_8(ur + 0 * FS + q, u + g);
+                cp_async_8(ur + 1 * FS + q, v + g);
+                cp_async_8(ur + 2 * FS + q, w + g);
+            }
+        }
+        cp_async_commit();
+    };
+
     int hxy[2];
     bool hval1;
     hxy[0] = (1 + wid) * UW + 2 + lane;
@@ -283,6 +301,10 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
     for (int mq = mstart; mq <= mend; mq++) {
         produce(mq, sa, sb, sc, cur);
         __syncthreads();
+        const bool next = mq + 2 <= mend + 1;
+        // FP64: the copy of u plane mq+2 into the slot of plane mq-1 (which
+        // nothing reads after produce(mq)) overlaps stage 2
+        if (!MIXED && next) load_u_plane_async(mq + 2, sa);
         if (mq == 1) {
             wall(0, 1);
             __syncthreads();
@@ -297,7 +319,8 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
             __syncthreads();
             if (p.nz >= kbeg && p.nz <= kend) stage2(p.nz, sa, sb, sc, cur);
         }
-        if (mq + 2 <= mend + 1) load_u_plane(mq + 2, sa); // (mq + 2) % 3 == (mq - 1) % 3
+        if (MIXED && next) load_u_plane(mq + 2, sa); // (mq + 2) % 3 == (mq - 1) % 3
+        if (!MIXED && next) cp_async_wait<0>();
         if (mq < mend) { // constants of plane mq + 1 <= nz: indices up to mq + 2 <= nz + 1
             prev = cur;
             cur.dzf_km = cur.dzf_k;
