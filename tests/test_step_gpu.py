@@ -190,7 +190,8 @@ def test_full_size_step_invariants(gpu):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_step_matches_phases(gpu, precision):
+@pytest.mark.parametrize("nx,ny,nz", [(64, 48, 32), (192, 48, 24), (768, 16, 16)])
+def test_step_matches_phases(gpu, precision, nx, ny, nz):
     """pl_channel_step fuses calcRHS into the Poisson solve's forward x
     transform; the phase entries run calcRHS and the solve as separate
     kernels.  FP64: the same numbers bit for bit.  Mixed: the FP64 plane
@@ -198,7 +199,7 @@ def test_step_matches_phases(gpu, precision):
     round-off."""
     plb = gpu
     prec = plb.PL_FP64 if precision == "fp64" else plb.PL_MIXED
-    cfg = plb.ChannelConfig(nx=64, ny=48, nz=32, stretch_ratio=1.5, re_tau=180.0, precision=prec)
+    cfg = plb.ChannelConfig(nx=nx, ny=ny, nz=nz, stretch_ratio=1.5, re_tau=180.0, precision=prec)
     a, b = plb.Channel(cfg), plb.Channel(cfg)
     a.init_flow(5, 0.1)
     b.init_flow(5, 0.1)
