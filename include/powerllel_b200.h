@@ -126,7 +126,10 @@ int pl_channel_destroy(pl_channel *c);
  * splitmix64(seed + (n+1)*0x9E3779B97F4A7C15) >> 11 scaled by 2^-53), then
  * transform2CRF and the boundary fills (main.f90:98-102). */
 int pl_channel_init_flow(pl_channel *c, uint64_t seed, double noise_intensity);
-/* nsteps RK2 projection steps, asynchronous on the channel's stream */
+/* nsteps RK2 projection steps, asynchronous on the channel's stream.  Where
+ * nx is one of the compile-time transform lengths, calcRHS runs inside the
+ * Poisson solve's forward x transform (the per-phase entries below run it as
+ * its own kernel; in FP64 both give the same numbers bit for bit). */
 int pl_channel_step(pl_channel *c, int nsteps);
 int pl_channel_synchronize(pl_channel *c);
 int pl_channel_diagnostics(pl_channel *c, pl_diag *out);
