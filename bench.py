@@ -167,15 +167,34 @@ def cpu_reference_steps(nsteps_max, warmup, budget_s=150.0):
     return n / dt, threads, sample
 
 
-def dist_setup(n_gpus):
+def dist_setup(n_gpus, backend="nccl"):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group(backend="nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
     return world, rank, local
+
+
+def barrier(world):
+    """all ranks reach this point (no-op on one rank)"""
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world, device="cuda"):
+    """the largest x over the ranks: a multi-GPU time is its slowest rank's
+    (device: where the reduction's tensor lives, "cuda" for NCCL, "cpu" for gloo)"""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def run_reference(args):
@@ -202,19 +221,6 @@ def run_b200(args):
     torch.cuda.set_device(local)
     import powerllel_channel_b200 as plb
 
-    def barrier():
-        if world > 1:
-            import torch.distributed as dist
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if world > 1:
-            import torch.distributed as dist
-            t = torch.tensor([x], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            return float(t.item())
-        return x
-
     def timed(ch, K, W, body):
         for _ in range(W):
             body()
@@ -222,7 +228,7 @@ def run_b200(args):
         torch.cuda.synchronize()
         st = torch.cuda.ExternalStream(ch.stream_handle)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        barrier()
+        barrier(world)
         torch.cuda.synchronize()
         e0.record(st)
         for _ in range(K):
@@ -230,8 +236,8 @@ def run_b200(args):
         e1.record(st)
         ch.synchronize()
         torch.cuda.synchronize()
-        barrier()
-        return max_over_ranks(e0.elapsed_time(e1))
+        barrier(world)
+        return max_over_ranks(e0.elapsed_time(e1), world)
 
     peak, peak_kind = peaks()
     npts = NX * NY * NZ
