@@ -4,7 +4,7 @@ The mixed path keeps u, v, w and p in FP64, evaluates the momentum stencils in
 FP32 (stage-1 increments stored in FP32), and solves for the pressure
 increment with FP32 FFTs around an FP64 tridiagonal elimination; the
 right-hand side of the increment (div u/dt - L p_prev) and the (0,0) mode are
-FP64.  Acceptance (north star): velocity relative L2 error <= 1e-5 against the
+FP64.  Acceptance of the mixed path: velocity relative L2 error <= 1e-5 against the
 FP64 oracle and max |div u| <= 1e-10."""
 import numpy as np
 import pytest

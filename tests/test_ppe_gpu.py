@@ -6,7 +6,7 @@ The (kx,ky) = (0,0) system of the Neumann problem is singular up to round-off
 (its last pivot is round-off, mod_poisson_solver.c:337-342), so p is defined up
 to an additive constant that differs with the summation order of any two
 implementations: p is compared modulo its mean, with max|diff| / max|p|.
-FP64 tolerance: 1e-12 relative (the FP64 bar of the north star)."""
+FP64 tolerance: 1e-12 relative (the FP64 path's parity bar)."""
 import glob
 import os
 
