@@ -368,35 +368,6 @@ __global__ void __launch_bounds__(256) k_rk2m_fp64(double *u, double *v, double 
     mean_reduce(su, red);
 }
 
-// correctVel + forceVel (shift from the fused mean) + wall fill
-template <typename TP>
-__global__ void __launch_bounds__(256) k_correct_force(const TP *__restrict__ pp, double *u, double *v, double *w,
-                                                       StepParams p, MeshDev m, int forced_x, const double *scalar)
-{
-    PL_POINT_INDEX();
-    const Nb n = neighbours(i, j, k, p.nx, p.ny);
-    const double dt = p.dt, dtdxi = dt * p.dx_inv, dtdyi = dt * p.dy_inv;
-    const size_t pc = n.c - sk;
-    const double p0 = (double)__ldg(pp + pc);
-    const double pxp = (double)__ldg(pp + n.xp - sk), pyp = (double)__ldg(pp + n.yp - sk);
-    const double pzp = (k < p.nz) ? (double)__ldg(pp + pc + sk) : p0;
-    double nu = u[n.c] - (pxp - p0) * dtdxi;
-    if (forced_x) nu = nu + __ldg(scalar + 3);
-    const double nv = v[n.c] - (pyp - p0) * dtdyi;
-    const double nw = w[n.c] - (pzp - p0) * dt * __ldg(m.dzc_inv + k);
-    u[n.c] = nu;
-    v[n.c] = nv;
-    w[n.c] = nw;
-    const double bcu = 0.0 - p.u_crf;
-    if (k == 1) {
-        u[n.c - sk] = 2.0 * bcu - nu;
-        v[n.c - sk] = -nv;
-    }
-    if (k == p.nz) {
-        u[n.c + sk] = 2.0 * bcu - nu;
-        v[n.c + sk] = -nv;
-    }
-}
 
 // ------------------------------------------------------------------------
 // mixed precision (u, v, w, p in FP64; stage increments and PPE in FP32)
@@ -515,6 +486,68 @@ __global__ void __launch_bounds__(RHS_BX *RHS_BY) k_rhs_mixed(const double *__re
 static inline dim3 rhs_mixed_grid(const StepParams &p)
 {
     return dim3((p.nx / 2 + RHS_BX - 1) / RHS_BX, (p.ny + RHS_BY - 1) / RHS_BY, p.nz);
+}
+
+// correctVel + forceVel (shift from the fused mean) + wall fill, for two
+// adjacent points (i, i+1), i even, per thread: the u, v, w pairs and the
+// pressure pairs move as 16-byte (FP32 pressure: 8-byte) accesses (nx is
+// even, so every pair is aligned and lies in one row).  Per point the
+// expressions are correctVel's (mod_calcVel.f90:436-450) in its order.
+template <typename TP> struct PairOf;
+template <> struct PairOf<double> {
+    using type = double2;
+};
+template <> struct PairOf<float> {
+    using type = float2;
+};
+
+template <typename TP>
+__global__ void __launch_bounds__(RHS_BX *RHS_BY) k_correct_force(const TP *__restrict__ pp, double *u, double *v,
+                                                                   double *w, StepParams p, MeshDev m, int forced_x,
+                                                                   const double *scalar)
+{
+    using P2 = typename PairOf<TP>::type;
+    const int i = 2 * (blockIdx.x * RHS_BX + threadIdx.x);
+    const int j = blockIdx.y * RHS_BY + threadIdx.y;
+    const int k = blockIdx.z + 1;
+    if (i >= p.nx || j >= p.ny) return;
+    const size_t sk = (size_t)p.nx * p.ny;
+    const int ip2 = (i + 2 == p.nx) ? 0 : i + 2, jp = (j == p.ny - 1) ? 0 : j + 1;
+    const size_t c = (size_t)p.nx * j + sk * k + i, pc = c - sk;
+    const double dt = p.dt, dtdxi = dt * p.dx_inv, dtdyi = dt * p.dy_inv;
+    const P2 p0 = __ldg(reinterpret_cast<const P2 *>(pp + pc));
+    const double p0a = (double)p0.x, p0b = (double)p0.y;
+    const double pxpb = (double)__ldg(pp + (size_t)p.nx * j + sk * (k - 1) + ip2); // (i+2, j)
+    const P2 py = __ldg(reinterpret_cast<const P2 *>(pp + (size_t)p.nx * jp + sk * (k - 1) + i));
+    double pza = p0a, pzb = p0b;
+    if (k < p.nz) {
+        const P2 pz = __ldg(reinterpret_cast<const P2 *>(pp + pc + sk));
+        pza = (double)pz.x;
+        pzb = (double)pz.y;
+    }
+    const double2 uu = *reinterpret_cast<const double2 *>(u + c);
+    const double2 vv = *reinterpret_cast<const double2 *>(v + c);
+    const double2 ww = *reinterpret_cast<const double2 *>(w + c);
+    double nua = uu.x - (p0b - p0a) * dtdxi, nub = uu.y - (pxpb - p0b) * dtdxi;
+    if (forced_x) {
+        nua = nua + __ldg(scalar + 3);
+        nub = nub + __ldg(scalar + 3);
+    }
+    const double nva = vv.x - ((double)py.x - p0a) * dtdyi, nvb = vv.y - ((double)py.y - p0b) * dtdyi;
+    const double dzi = __ldg(m.dzc_inv + k);
+    const double nwa = ww.x - (pza - p0a) * dt * dzi, nwb = ww.y - (pzb - p0b) * dt * dzi;
+    *reinterpret_cast<double2 *>(u + c) = make_double2(nua, nub);
+    *reinterpret_cast<double2 *>(v + c) = make_double2(nva, nvb);
+    *reinterpret_cast<double2 *>(w + c) = make_double2(nwa, nwb);
+    const double bcu = 0.0 - p.u_crf;
+    if (k == 1) {
+        *reinterpret_cast<double2 *>(u + c - sk) = make_double2(2.0 * bcu - nua, 2.0 * bcu - nub);
+        *reinterpret_cast<double2 *>(v + c - sk) = make_double2(-nva, -nvb);
+    }
+    if (k == p.nz) {
+        *reinterpret_cast<double2 *>(u + c + sk) = make_double2(2.0 * bcu - nua, 2.0 * bcu - nub);
+        *reinterpret_cast<double2 *>(v + c + sk) = make_double2(-nva, -nvb);
+    }
 }
 
 // per-plane sums of the warp partials (fixed order): mode0[k] = sum_ij r
@@ -667,7 +700,7 @@ int launch_rk2m_fp64(double *u, double *v, double *w, const double *u1, const do
 int launch_correct_force_fp64(const double *p_, double *u, double *v, double *w, const StepParams &p,
                               const MeshDev &m, int forced_x, const double *scalar, cudaStream_t st)
 {
-    k_correct_force<double><<<point_grid(p), point_block(), 0, st>>>(p_, u, v, w, p, m, forced_x, scalar);
+    k_correct_force<double><<<rhs_mixed_grid(p), dim3(RHS_BX, RHS_BY), 0, st>>>(p_, u, v, w, p, m, forced_x, scalar);
     PL_CHECK_LAUNCH();
     return 0;
 }
@@ -675,7 +708,7 @@ int launch_correct_force_fp64(const double *p_, double *u, double *v, double *w,
 int launch_correct_force_f32(const float *p_, double *u, double *v, double *w, const StepParams &p, const MeshDev &m,
                              int forced_x, const double *scalar, cudaStream_t st)
 {
-    k_correct_force<float><<<point_grid(p), point_block(), 0, st>>>(p_, u, v, w, p, m, forced_x, scalar);
+    k_correct_force<float><<<rhs_mixed_grid(p), dim3(RHS_BX, RHS_BY), 0, st>>>(p_, u, v, w, p, m, forced_x, scalar);
     PL_CHECK_LAUNCH();
     return 0;
 }
