@@ -578,25 +578,35 @@ __global__ void __launch_bounds__(128) k_thomas(const T *xin, double *xs, T *xou
 // above writes every swept value to HBM and reads it back (32 B/point in
 // FP64), because the 402 MB of a 512x384x256 sweep does not stay in L2.
 // Here each of the 128 threads of a CTA (one per SM: its shared memory is
-// over half the SM's) keeps the nz <= 256 swept values of its column in its
-// own TMEM lane, so HBM sees the right-hand side once, the solution once and
-// the class tables.  The loads are per-thread cp.async copies into a ring of
+// over half the SM's) keeps the swept values of its column in its own TMEM
+// lane (up to 256 rows; see below for taller columns), so HBM sees the
+// right-hand side once, the solution once and the class tables.  The loads are per-thread cp.async copies into a ring of
 // TTM_NS groups of TTM_G rows in shared memory, TTM_NS - 1 groups ahead;
 // each thread reads only its own copies, so the pipeline has no barrier and
 // no wait other than cp.async.wait_group on the thread's own copies.  The
 // copy stream of a round is the forward groups (rhs + multipliers) then the
 // backward groups (reciprocal pivots), and runs on into the next round's
 // columns.  The arithmetic is thomas_column's, operation for operation.
-constexpr int TTM_THREADS = 128, TTM_G = 8, TTM_NS = 8, TTM_MAX_NZ = 256;
+//
+// A lane holds 256 doubles.  Taller columns (nz <= TTM_MAX_NZ) keep their
+// bottom TTM_TM_ROWS - TTM_TOP_ROWS and top TTM_TOP_ROWS rows in tensor
+// memory and the rows between in an HBM scratch (FP64: in place), which the
+// backward sweep prefetches through the copy ring.  The top rows stay on
+// chip because the ring runs NS - 1 groups ahead: a backward group's
+// prefetch is issued after the forward store of its rows only from the
+// NS/2-th group below the top on.
+constexpr int TTM_THREADS = 128, TTM_G = 8, TTM_NS = 8, TTM_MAX_NZ = 1024, TTM_TM_ROWS = 256, TTM_TOP_ROWS = 32;
+static_assert(TTM_TOP_ROWS >= (TTM_NS / 2) * TTM_G, "the HBM rows' prefetch must follow their store");
 
-template <typename T> __host__ __device__ constexpr size_t ttm_smem_bytes()
+template <typename T> __host__ __device__ constexpr size_t ttm_smem_bytes(int nz)
 {
     // table ring [NS][G][128] (double), rhs ring [NS][G][128] (T), (0,0)-mode
-    // rhs ring [NS][G] (double), c_k [TTM_MAX_NZ], TMEM address slot; at
-    // least 116 KB so that two CTAs never share an SM (each may take all 512
-    // TMEM columns)
-    constexpr size_t b =
-        (size_t)TTM_NS * TTM_G * TTM_THREADS * (8 + sizeof(T)) + TTM_NS * TTM_G * 8 + TTM_MAX_NZ * 8 + 16;
+    // rhs ring [NS][G] (double), c_k [TTM_MAX_NZ], TMEM address slot, and for
+    // FP32 right-hand sides of tall columns a ring of the HBM rows (double;
+    // FP64 reuses the rhs ring); at least 116 KB so that two CTAs never share
+    // an SM (each may take all 512 TMEM columns)
+    const size_t b = (size_t)TTM_NS * TTM_G * TTM_THREADS * (8 + sizeof(T)) + TTM_NS * TTM_G * 8 + TTM_MAX_NZ * 8 +
+                     16 + ((sizeof(T) == 4 && nz > TTM_TM_ROWS) ? (size_t)TTM_NS * TTM_G * TTM_THREADS * 8 : 0);
     return b < 116 * 1024 ? 116 * 1024 : b;
 }
 
@@ -618,7 +628,7 @@ struct TtmColumn {
 
 template <typename T>
 __global__ void __launch_bounds__(TTM_THREADS, 1)
-    k_thomas_tmem(const T *xin, T *xout, TridDev t, const double *mode0, int rounds, uint32_t tcols)
+    k_thomas_tmem(const T *xin, T *xout, double *xsc, TridDev t, const double *mode0, int rounds, uint32_t tcols)
 {
     constexpr int G = TTM_G, NS = TTM_NS, NT = TTM_THREADS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -627,8 +637,15 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
     double *zring = reinterpret_cast<double *>(xring + NS * G * NT); // [NS][G] (0,0) mode right-hand side
     double *csh = zring + NS * G;                                    // [nz] c_k
     uint32_t *tslot = reinterpret_cast<uint32_t *>(csh + TTM_MAX_NZ);
+    double *sring = sizeof(T) == 8 ? reinterpret_cast<double *>(xring) : csh + TTM_MAX_NZ + 2; // HBM rows, bwd
     const int tid = threadIdx.x, warp = tid >> 5;
     const int nz = t.nz, ngf = nz / G, per_round = 2 * ngf;
+    // rows [kb, kt) live in the HBM scratch (none when nz <= TTM_TM_ROWS);
+    // row k < kb sits at TMEM cell 2k, row k >= kt at 2 (kb + k - kt)
+    const bool tall = nz > TTM_TM_ROWS;
+    const int kb = tall ? TTM_TM_ROWS - TTM_TOP_ROWS : nz, kt = tall ? nz - TTM_TOP_ROWS : nz;
+    auto in_hbm = [&](int k0) { return k0 >= kb && k0 < kt; }; // k0: first row of an 8-row group
+    auto tcell = [&](int k0) { return 2 * (k0 < kb ? k0 : kb + k0 - kt); };
     const size_t stride = (size_t)t.nx * t.ny, cstride = (size_t)t.ncx * t.ncy;
     const int ncol = t.nx * t.ny;
 
@@ -658,6 +675,7 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
     TtmColumn ic = column(0);
     const T *xsrc = xin + ic.col;
     const double *msrc = t.mult + ic.cls, *rsrc = t.rb + ic.cls + (size_t)(nz - 1) * cstride;
+    const double *ssrc = xsc + ic.col + (size_t)(nz - 1) * stride;
     auto issue_next = [&]() {
         if (ir < rounds) {
             double *cdst = cring + islot * G * NT + tid;
@@ -679,10 +697,14 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
                     }
                 }
             } else if (ic.valid) {
+                const bool hb = in_hbm(nz - (ig - ngf + 1) * G);
+                double *sdst = sring + islot * G * NT + tid;
 #pragma unroll
                 for (int u = 0; u < G; u++) {
                     cp_async_8(cdst + u * NT, rsrc);
+                    if (hb) cp_async_8(sdst + u * NT, ssrc);
                     rsrc -= cstride;
+                    ssrc -= stride;
                 }
             }
             if (++ig == per_round) {
@@ -692,6 +714,7 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
                     xsrc = xin + ic.col;
                     msrc = t.mult + ic.cls;
                     rsrc = t.rb + ic.cls + (size_t)(nz - 1) * cstride;
+                    ssrc = xsc + ic.col + (size_t)(nz - 1) * stride;
                 }
             }
         }
@@ -723,14 +746,18 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
             }
             issue_next(); // refills the slot consumed one step ago
             uint32_t v[2 * G];
+            const bool hb = in_hbm(g * G); // warp-uniform
 #pragma unroll
             for (int u = 0; u < G; u++) {
                 xp = xv[u] - mv[u] * xp;
                 v[2 * u] = (uint32_t)__double2loint(xp);
                 v[2 * u + 1] = (uint32_t)__double2hiint(xp);
+                if (hb && cc.valid) xsc[cc.col + (size_t)(g * G + u) * stride] = xp;
             }
-            __syncwarp();
-            tmem_st16(tbase + 2 * g * G, v);
+            if (!hb) {
+                __syncwarp();
+                tmem_st16(tbase + tcell(g * G), v);
+            }
             slot = (slot + 1 == NS) ? 0 : slot + 1;
         }
         tmem_wait_st();
@@ -740,25 +767,29 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
         xp = 0.0;
         T *dst = xout + cc.col + (size_t)(nz - 1) * stride;
         for (int h = 0; h < ngf; h++) {
-            const int kt = nz - 1 - h * G; // rows kt, kt-1, ..., kt-G+1
+            const int ktop = nz - 1 - h * G; // rows ktop, ktop-1, ..., ktop-G+1
             uint32_t v[2 * G];
-            __syncwarp();
-            tmem_ld16_start(tbase + 2 * (kt - G + 1), v);
+            const bool hb = in_hbm(ktop - G + 1); // warp-uniform
+            if (!hb) {
+                __syncwarp();
+                tmem_ld16_start(tbase + tcell(ktop - G + 1), v);
+            }
             cp_async_wait<NS - 2>();
             const double *cs = cring + slot * G * NT + tid;
             double rv[G], cv[G];
 #pragma unroll
             for (int u = 0; u < G; u++) {
                 rv[u] = cs[u * NT];
-                cv[u] = csh[kt - u];
+                cv[u] = csh[ktop - u];
             }
             if (zr && tid == 0 && h == 0) rv[0] = 0.0;
             issue_next();
-            tmem_wait_ld(v);
+            if (!hb) tmem_wait_ld(v);
+            const double *ss = sring + slot * G * NT + tid;
 #pragma unroll
             for (int u = 0; u < G; u++) {
                 const int i = G - 1 - u;
-                const double x = __hiloint2double((int)v[2 * i + 1], (int)v[2 * i]);
+                const double x = hb ? ss[u * NT] : __hiloint2double((int)v[2 * i + 1], (int)v[2 * i]);
                 xp = (x - cv[u] * xp) * rv[u];
                 if (cc.valid) *dst = (T)xp;
                 dst -= stride;
@@ -1157,16 +1188,20 @@ template <typename T> static int launch_trid(Ppe *s, T *x, cudaStream_t st, cons
     TridDev t{s->nx, s->ny, s->nz, s->ncx, s->ncy, s->d_mult, s->d_rb, s->d_c};
     dim3 grid((s->nx + 127) / 128, s->ny);
     double *xs = (sizeof(T) == 8 && s->nparts == 0) ? reinterpret_cast<double *>(x) : s->d_scratch;
-    if (s->nparts == 0 && s->nz % TTM_G == 0 && s->nz <= TTM_MAX_NZ) {
-        // swept values in TMEM: one 128-thread CTA per SM, persistent over the columns
-        const size_t shm = ttm_smem_bytes<T>();
+    if (s->nparts == 0 && s->nz % TTM_G == 0 && s->nz <= TTM_MAX_NZ &&
+        (s->nz <= TTM_TM_ROWS || sizeof(T) == 8 || s->d_scratch != nullptr)) {
+        // swept values in TMEM (taller columns partly in the HBM scratch: in
+        // place for FP64, the FP64 sweep scratch for FP32): one 128-thread CTA
+        // per SM, persistent over the columns
+        const size_t shm = ttm_smem_bytes<T>(s->nz);
         PL_CUDA_TRY(cudaFuncSetAttribute(k_thomas_tmem<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
         const int ncol = s->nx * s->ny;
         const int ctas = std::max(1, std::min(sm_count(), (ncol + TTM_THREADS - 1) / TTM_THREADS));
         const int rounds = (ncol + ctas * TTM_THREADS - 1) / (ctas * TTM_THREADS);
         uint32_t tcols = 32;
-        while (tcols < 2u * (uint32_t)s->nz) tcols *= 2;
-        k_thomas_tmem<T><<<ctas, TTM_THREADS, shm, st>>>(x, x, t, mode0, rounds, tcols);
+        while (tcols < 2u * (uint32_t)std::min(s->nz, TTM_TM_ROWS)) tcols *= 2;
+        double *xsc = sizeof(T) == 8 ? reinterpret_cast<double *>(x) : s->d_scratch;
+        k_thomas_tmem<T><<<ctas, TTM_THREADS, shm, st>>>(x, x, xsc, t, mode0, rounds, tcols);
     } else if (s->nparts == 0) {
         k_thomas<T><<<grid, 128, 0, st>>>(x, xs, x, t, mode0);
     } else {

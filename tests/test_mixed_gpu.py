@@ -24,7 +24,7 @@ def rel_max(a, b):
     return float(np.abs(a - b).max() / np.abs(b).max())
 
 
-@pytest.mark.parametrize("nx,ny,nz,nsteps", [(64, 64, 64, 20), (96, 72, 48, 10)])
+@pytest.mark.parametrize("nx,ny,nz,nsteps", [(64, 64, 64, 20), (96, 72, 48, 10), (32, 24, 320, 8)])
 def test_mixed_vs_fp64_oracle(gpu, oracle_mod, nx, ny, nz, nsteps):
     plb, O = gpu, oracle_mod
     cfg = plb.ChannelConfig(nx=nx, ny=ny, nz=nz, stretch_ratio=1.5, re_tau=180.0, precision=plb.PL_MIXED)

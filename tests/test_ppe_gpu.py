@@ -91,13 +91,15 @@ def test_device_ppe_vs_golden(gpu, path):
     assert torch.equal(x, y)
 
 
-# Thomas runs in tensor memory for nz % 8 == 0 and nz <= 256 (768x32x256: two
-# rounds of columns per CTA; 16x8x8: one 8-row group, exactly one CTA of 128
-# columns; 8x6x16: one CTA with 80 idle threads), in HBM otherwise
+# Thomas keeps its swept values in tensor memory for nz % 8 == 0: all of them
+# for nz <= 256 (768x32x256: two rounds of columns per CTA; 16x8x8: one 8-row
+# group, exactly one CTA of 128 columns; 8x6x16: one CTA with 80 idle
+# threads), 256 of them for taller columns with the rest in HBM (32x24x264,
+# 32x24x512); in HBM alone for other nz
 @pytest.mark.parametrize("nx,ny,nz,nparts", [(64, 64, 64, 0), (128, 96, 48, 0), (256, 192, 32, 4),
                                             (64, 48, 40, 8), (96, 72, 30, 4), (64, 48, 32, 2),
                                             (64, 48, 30, 0), (32, 24, 264, 0), (768, 32, 256, 0),
-                                            (16, 8, 8, 0), (8, 6, 16, 0)])
+                                            (16, 8, 8, 0), (8, 6, 16, 0), (32, 24, 512, 0)])
 def test_ppe_vs_oracle_live(gpu, oracle_mod, nx, ny, nz, nparts):
     """Sizes beyond the fixtures (radix-3 lengths, uneven PDD partitions)."""
     import torch
