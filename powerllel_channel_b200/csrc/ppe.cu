@@ -626,7 +626,9 @@ struct TtmColumn {
     size_t col, cls;
 };
 
-template <typename T>
+// TALL: nz > TTM_TM_ROWS (the HBM-scratch rows exist); a compile-time switch,
+// so that shorter columns run the tensor-memory path alone
+template <typename T, bool TALL>
 __global__ void __launch_bounds__(TTM_THREADS, 1)
     k_thomas_tmem(const T *xin, T *xout, double *xsc, TridDev t, const double *mode0, int rounds, uint32_t tcols)
 {
@@ -642,10 +644,9 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
     const int nz = t.nz, ngf = nz / G, per_round = 2 * ngf;
     // rows [kb, kt) live in the HBM scratch (none when nz <= TTM_TM_ROWS);
     // row k < kb sits at TMEM cell 2k, row k >= kt at 2 (kb + k - kt)
-    const bool tall = nz > TTM_TM_ROWS;
-    const int kb = tall ? TTM_TM_ROWS - TTM_TOP_ROWS : nz, kt = tall ? nz - TTM_TOP_ROWS : nz;
-    auto in_hbm = [&](int k0) { return k0 >= kb && k0 < kt; }; // k0: first row of an 8-row group
-    auto tcell = [&](int k0) { return 2 * (k0 < kb ? k0 : kb + k0 - kt); };
+    const int kb = TALL ? TTM_TM_ROWS - TTM_TOP_ROWS : nz, kt = TALL ? nz - TTM_TOP_ROWS : nz;
+    auto in_hbm = [&](int k0) { return TALL && k0 >= kb && k0 < kt; }; // k0: first row of an 8-row group
+    auto tcell = [&](int k0) { return TALL ? 2 * (k0 < kb ? k0 : kb + k0 - kt) : 2 * k0; };
     const size_t stride = (size_t)t.nx * t.ny, cstride = (size_t)t.ncx * t.ncy;
     const int ncol = t.nx * t.ny;
 
@@ -702,9 +703,11 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
 #pragma unroll
                 for (int u = 0; u < G; u++) {
                     cp_async_8(cdst + u * NT, rsrc);
-                    if (hb) cp_async_8(sdst + u * NT, ssrc);
                     rsrc -= cstride;
-                    ssrc -= stride;
+                    if constexpr (TALL) {
+                        if (hb) cp_async_8(sdst + u * NT, ssrc);
+                        ssrc -= stride;
+                    }
                 }
             }
             if (++ig == per_round) {
@@ -1194,14 +1197,21 @@ template <typename T> static int launch_trid(Ppe *s, T *x, cudaStream_t st, cons
         // place for FP64, the FP64 sweep scratch for FP32): one 128-thread CTA
         // per SM, persistent over the columns
         const size_t shm = ttm_smem_bytes<T>(s->nz);
-        PL_CUDA_TRY(cudaFuncSetAttribute(k_thomas_tmem<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
         const int ncol = s->nx * s->ny;
         const int ctas = std::max(1, std::min(sm_count(), (ncol + TTM_THREADS - 1) / TTM_THREADS));
         const int rounds = (ncol + ctas * TTM_THREADS - 1) / (ctas * TTM_THREADS);
         uint32_t tcols = 32;
         while (tcols < 2u * (uint32_t)std::min(s->nz, TTM_TM_ROWS)) tcols *= 2;
         double *xsc = sizeof(T) == 8 ? reinterpret_cast<double *>(x) : s->d_scratch;
-        k_thomas_tmem<T><<<ctas, TTM_THREADS, shm, st>>>(x, x, xsc, t, mode0, rounds, tcols);
+        if (s->nz > TTM_TM_ROWS) {
+            PL_CUDA_TRY(
+                cudaFuncSetAttribute(k_thomas_tmem<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+            k_thomas_tmem<T, true><<<ctas, TTM_THREADS, shm, st>>>(x, x, xsc, t, mode0, rounds, tcols);
+        } else {
+            PL_CUDA_TRY(
+                cudaFuncSetAttribute(k_thomas_tmem<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+            k_thomas_tmem<T, false><<<ctas, TTM_THREADS, shm, st>>>(x, x, xsc, t, mode0, rounds, tcols);
+        }
     } else if (s->nparts == 0) {
         k_thomas<T><<<grid, 128, 0, st>>>(x, xs, x, t, mode0);
     } else {
