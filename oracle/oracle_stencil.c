@@ -119,8 +119,8 @@ double orc_uniform(uint64_t seed, uint64_t n)
 
 /* ---- boundary fills (mod_updateBound.f90) ----------------------------- */
 
-/* y: periodic self-exchange of updateHalo (:411-424) over all i, all k;
- * x: imposePeriodicBC idir=1 (:288-306) over all j, k */
+/* y: periodic self-exchange of updateHalo (:364-396, south/north at :378-383)
+ * over all i, all k; x: imposePeriodicBC idir=1 (:241-272) over all j, k */
 static void periodic_xy(const orc_grid *g, double *var)
 {
     const int nx = g->nx, ny = g->ny, nz = g->nz;
@@ -136,7 +136,7 @@ static void periodic_xy(const orc_grid *g, double *var)
         }
 }
 
-/* imposeNoSlipBC (:312-368) */
+/* imposeNoSlipBC (:274-330) */
 static void noslip(const orc_grid *g, int ibound, int centered, double *var, double bcvalue)
 {
     const int nx = g->nx, ny = g->ny, n = g->nz;
@@ -158,7 +158,7 @@ static void noslip(const orc_grid *g, int ibound, int centered, double *var, dou
         }
 }
 
-/* updateBoundVel (:68-93) = updateHalo + imposeBCVel (:95-146) */
+/* updateBoundVel (:30-55) = updateHalo + imposeBCVel (:57-108) */
 void orc_update_bound_vel(const orc_grid *g, double *u, double *v, double *w)
 {
     periodic_xy(g, u);
@@ -173,7 +173,7 @@ void orc_update_bound_vel(const orc_grid *g, double *u, double *v, double *w)
     noslip(g, 1, 0, w, 0.0);
 }
 
-/* updateBoundP (:224-277) with imposeZeroGradBC (:370-400) */
+/* updateBoundP (:186-239) with imposeZeroGradBC (:332-362) */
 void orc_update_bound_p(const orc_grid *g, double *p)
 {
     const int nx = g->nx, ny = g->ny, nz = g->nz;

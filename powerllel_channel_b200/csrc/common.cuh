@@ -8,7 +8,8 @@
 // The reference's ghosted Fortran array u(0:nx+1,0:ny+1,0:nz+1)
 // (mod_variables.f90:21-41) maps to this layout by dropping the x/y ghosts,
 // which on one rank always equal the periodic images of the interior
-// (mod_updateBound.f90:288-306 and the self-exchange of :411-424).
+// (imposePeriodicBC, mod_updateBound.f90:241-272, and the self-exchange of
+// updateHalo, :364-396).
 #pragma once
 
 #include <cuda_runtime.h>

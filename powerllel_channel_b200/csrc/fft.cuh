@@ -2,7 +2,7 @@
 // pairing used by the PPE kernels.
 //
 // The reference transforms each periodic direction with FFTW's R2HC / HC2R
-// (src/src_c/mod_fft_fftw.inc:100-160): forward unnormalised, output in FFTW's
+// (src/src_c/mod_fft_fftw.inc:35-95): forward unnormalised, output in FFTW's
 // half-complex order r_0..r_{n/2}, i_{(n+1)/2-1}..i_1; backward unnormalised.
 // Here two real lines are packed into one complex line (z = a + i b), one
 // complex FFT of length n is run, and the two half-complex spectra are split

@@ -5,7 +5,7 @@
 // neighbour values come through L1/L2 (each field is streamed from HBM once).
 // x and y neighbours wrap periodically; the wall ghost planes k = 0, nz+1 are
 // stored and refreshed by the kernel that writes the adjacent interior plane,
-// which reproduces imposeNoSlipBC (mod_updateBound.f90:312-368) applied after
+// which reproduces imposeNoSlipBC (mod_updateBound.f90:274-330) applied after
 // the periodic fills.
 #include "stencil.cuh"
 #include "stencil_rhs.cuh"

@@ -5,7 +5,7 @@
 // Restates, per eigenvalue class, src/src_c/mod_poisson_solver.c:
 //   set_trid_coeff (:40-103) with c_or_f = 'c' and bctype "NN",
 //   eigenvalues lambda = lambda_x/dx^2 + lambda_y/dy^2 (:227-242,
-//   mod_fft_fftw.inc:180-183), pivots b (:255-276), PDD spikes v, w and the
+//   mod_fft_fftw.inc:115-118), pivots b (:255-276), PDD spikes v, w and the
 //   exchanged plane tmp_v (init_pdd_array :105-176).
 // A class is (ix, jy) with ix <= nx/2, jy <= ny/2: half-complex slots p and
 // n-p carry the same eigenvalue (cos is even), so every per-column quantity

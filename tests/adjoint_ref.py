@@ -2,7 +2,7 @@
 
 The forward map is one step of the channel solver: the RK1/RK2 momentum
 stencils (src/mod_calcVel.f90:52-426), the wall and periodic fills
-(src/mod_updateBound.f90:95-146, 312-368), calcRHS (src/mod_calcRHS.f90:11-36),
+(src/mod_updateBound.f90:57-108, 274-330), calcRHS (src/mod_calcRHS.f90:11-36),
 the PPE (src/src_c/mod_poisson_solver.c), correctVel and forceVel
 (src/mod_calcVel.f90:428-509). It is written with torch FP64 tensor
 operations, so torch.autograd gives its exact discrete adjoint (reverse-mode

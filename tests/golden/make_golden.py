@@ -2,7 +2,7 @@
 
 Run in a container that holds the reference tree (the GPU box does not):
 
-    make -C oracle          # builds oracle/_ref/ from the reference's own C sources
+    PL_REFERENCE=<reference checkout> make -C oracle   # builds oracle/_ref/ from its own C sources
     python tests/golden/make_golden.py
 
 PPE fixtures (ppe_*.npz): the reference's execute_poisson_solver

@@ -123,7 +123,7 @@ def test_ppe_vs_oracle_live(gpu, oracle_mod, nx, ny, nz, nparts):
 def test_ppe_single_modes(gpu, oracle_mod, mx, my):
     """Manufactured solution: p = cos(2 pi mx x/Lx + 0.3) cos(2 pi my y/Ly),
     uniform in z, solves L p = lambda p exactly (lambda the discrete
-    eigenvalue, mod_fft_fftw.inc:180-183).  Tolerance relative to the input
+    eigenvalue, mod_fft_fftw.inc:115-118).  Tolerance relative to the input
     amplitude: high modes have |lambda| >> 1, so p is much smaller than f."""
     import torch
     plb, O = gpu, oracle_mod
