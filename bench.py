@@ -288,31 +288,45 @@ def run_b200(args):
     chm.close()
     del host
 
-    # accuracy of the mixed path after 100 steps from the same initial field,
-    # against the FP64 path (parity-pinned to the oracle at small sizes)
-    acc = None
-    if not args.no_accuracy:
-        out = {}
+    # accuracy after 100 steps from the same initial field: both paths against
+    # the oracle (the reference's own C PPE inside the restated stencils, run
+    # in a subprocess on all host threads).  That oracle run is also the CPU
+    # baseline: its steps after the first are the timed sample.
+    acc, cpu = None, None
+    if rank == 0 and world == 1 and not args.no_accuracy:
+        import tempfile
+        from oracle import run_channel as R  # the checker and the CPU-baseline leg
+        gpu_fields, gpu_div = {}, {}
         for name, prec in (("fp64", plb.PL_FP64), ("mixed", plb.PL_MIXED)):
             cfg = plb.ChannelConfig(nx=NX, ny=NY, nz=NZ, stretch_ratio=STRETCH, re_tau=RE_TAU, dt=DT, precision=prec)
             ch = plb.Channel(cfg)
             ch.init_flow(SEED, NOISE)
             ch.step(100)
-            out[name] = [ch.get_field(q)[1:-1, 1:-1, 1:-1] for q in range(4)] + [ch.diagnostics()]
+            gpu_fields[name] = [ch.get_field(q)[1:-1, 1:-1, 1:-1] for q in range(4)]
+            gpu_div[name] = ch.diagnostics()["div_max"]
             ch.close()
-        acc = {"steps": 100, "reference": "this library's FP64 path", "p": "modulo its mean (the Neumann null mode)"}
-        for q, n in enumerate("uvwp"):
-            a, b = out["mixed"][q], out["fp64"][q]
-            if n == "p":
-                a, b = a - a.mean(), b - b.mean()
-            acc[f"{n}_rel_l2"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
-            acc[f"{n}_rel_max"] = float(np.abs(a - b).max() / np.abs(b).max())
-        acc["div_max_mixed"] = out["mixed"][4]["div_max"]
-        acc["div_max_fp64"] = out["fp64"][4]["div_max"]
-        del out
+        with tempfile.TemporaryDirectory() as td:
+            meta = R.run(td, (NX, NY, NZ), [100], stretch=STRETCH, re_tau=RE_TAU, dt=DT, seed=SEED, noise=NOISE)
+            ref = R.load(td, 100)
+            acc = {"steps": 100, "reference": "oracle: " + meta["what"],
+                   "p": "modulo its mean (the Neumann null mode)"}
+            for name in ("fp64", "mixed"):
+                for q, n in enumerate("uvwp"):
+                    a, b = gpu_fields[name][q], np.asarray(ref[q])
+                    if n == "p":
+                        a, b = a - a.mean(), b - b.mean()
+                    acc[f"{name}_{n}_rel_l2"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+                    acc[f"{name}_{n}_rel_max"] = float(np.abs(a - b).max() / np.abs(b).max())
+                acc[f"div_max_{name}"] = gpu_div[name]
+            del ref
+        del gpu_fields
+        st = meta["step_seconds"][1:]
+        if not args.no_cpu_baseline:
+            cpu = {"value": len(st) / sum(st), "unit": "steps/s", "cores": meta["threads"], "kind": "port",
+                   "sample": f"steps 2-{len(st) + 1} of the {NX}x{NY}x{NZ} 100-step oracle run of the accuracy "
+                             f"check, {meta['threads']} OpenMP threads: {meta['what']}"}
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if cpu is None and rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             sps_cpu, threads, sample = cpu_reference_steps(2, 1, budget_s=25.0)
             cpu = {"value": sps_cpu, "unit": "steps/s", "cores": threads, "kind": "port", "sample": sample}
@@ -347,6 +361,26 @@ def run_b200(args):
         dist.destroy_process_group()
 
 
+def run_capture(args):
+    """One precision path only, no timing and no JSON line: the command a
+    profiler wraps.  Builds the channel, fills the seeded initial field and
+    runs --warmup then --steps steps (step 3 on is a steady-state step of the
+    mixed path: its pressure prediction and increment are live)."""
+    import torch
+    torch.cuda.set_device(0)
+    import powerllel_channel_b200 as plb
+    prec = plb.PL_MIXED if args.capture == "mixed" else plb.PL_FP64
+    cfg = plb.ChannelConfig(nx=NX, ny=NY, nz=NZ, stretch_ratio=STRETCH, re_tau=RE_TAU, dt=DT, precision=prec,
+                            trid_parts=args.trid_parts)
+    ch = plb.Channel(cfg)
+    ch.init_flow(SEED, NOISE)
+    ch.step(args.warmup + args.steps)
+    ch.synchronize()
+    print(json.dumps({"capture": args.capture, "grid": [NX, NY, NZ], "steps": args.warmup + args.steps,
+                      "diag": ch.diagnostics()}), flush=True)
+    ch.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -358,6 +392,9 @@ def main():
     ap.add_argument("--grid", type=int, nargs=3, default=None,
                     help="override the grid (profiling captures on a smaller case); the bench line is only "
                          "valid at the default 512 384 256")
+    ap.add_argument("--capture", choices=["fp64", "mixed"], default=None,
+                    help="run one precision path untimed (the command an ncu capture wraps)")
+    ap.add_argument("--trid-parts", type=int, default=0, help="--capture only: PDD partitions (0 = Thomas)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -365,7 +402,9 @@ def main():
         global NX, NY, NZ, WORKLOAD
         NX, NY, NZ = args.grid
         WORKLOAD = WORKLOAD.replace("512x384x256", f"{NX}x{NY}x{NZ}")
-    if args.impl == "reference":
+    if args.capture:
+        run_capture(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_b200(args)
