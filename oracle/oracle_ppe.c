@@ -3,9 +3,10 @@
  * (src/src_c/mod_poisson_solver.c) for one process.  TEST INFRASTRUCTURE ONLY.
  *
  * The reference solves  L p = rhs  with real FFTs in x and y (R2HC, FFTW
- * guru plans, mod_fft_fftw.inc:100-155) and one wall-normal tridiagonal
+ * guru plans, init_fft mod_fft_fftw.inc:35-90, execute_fft :92-95) and one wall-normal tridiagonal
  * system per half-complex slot (i,j), eigenvalue lambda_x(i)/dx^2 +
- * lambda_y(j)/dy^2 (mod_poisson_solver.c:226-242, mod_fft_fftw.inc:175-183).
+ * lambda_y(j)/dy^2 (mod_poisson_solver.c:226-242, get_eigen_values
+ * mod_fft_fftw.inc:110-133).
  * Thomas (ssolve_trid :311-359) in the default build; PDD (init_pdd_array
  * :105-176, psolve_trid :361-466) over p_col z-partitions in the _PDD build.
  * With p_row = 1 every pencil transpose is an identity, so the P partitions
@@ -77,7 +78,7 @@ static void set_trid_coeff_c_nn(int n, const double *dzf, int bottom, int top, d
     }
 }
 
-/* mod_fft_fftw.inc:175-183, "PP" */
+/* get_eigen_values, mod_fft_fftw.inc:115-118, "PP" */
 static void eigen_pp(int n, double *lambda)
 {
     const double pi = acos(-1.0);
@@ -101,7 +102,7 @@ orc_ppe *orc_ppe_init(int nx, int ny, int nz, double dx, double dy, const double
     for (int m = 0; m < P; m++) s->kst[m] -= 1;
     free(en);
 
-    /* init_fft: normfactor 1/(1*nx*1*ny) for PP,PP (mod_fft_fftw.inc:154) */
+    /* init_fft: normfactor 1/(1*nx*1*ny) for PP,PP (mod_fft_fftw.inc:89) */
     s->norm = 1.0 / (1.0 * nx * 1.0 * ny);
     s->px = hc_fft_plan_create(nx);
     s->py = hc_fft_plan_create(ny);
@@ -188,11 +189,15 @@ orc_ppe *orc_ppe_init(int nx, int ny, int nz, double dx, double dy, const double
  * only, so the PDD zeroing of a[0], c[ke-1] does not enter it). */
 static void thomas_chunk(size_t nxy, int ke, const double *a, const double *c, const double *b, double *x)
 {
+    /* the columns ij are independent: threads split them (same arithmetic per
+     * column as the serial loops) */
     for (int k = 1; k < ke; k++)
+#pragma omp parallel for schedule(static)
         for (size_t ij = 0; ij < nxy; ij++) {
             double a_tmp = a[k] / b[ij + nxy * (k - 1)];
             x[ij + nxy * k] -= a_tmp * x[ij + nxy * (k - 1)];
         }
+#pragma omp parallel for schedule(static)
     for (size_t ij = 0; ij < nxy; ij++) {
         double bb = b[ij + nxy * (ke - 1)];
         if (bb != 0)
@@ -201,6 +206,7 @@ static void thomas_chunk(size_t nxy, int ke, const double *a, const double *c, c
             x[ij + nxy * (ke - 1)] = 0;
     }
     for (int k = ke - 2; k >= 0; k--)
+#pragma omp parallel for schedule(static)
         for (size_t ij = 0; ij < nxy; ij++)
             x[ij + nxy * k] = (x[ij + nxy * k] - c[k] * x[ij + nxy * (k + 1)]) / b[ij + nxy * k];
 }
@@ -224,6 +230,7 @@ static void solve_trid(orc_ppe *s, double *x)
         const double *xt = x + nxy * (s->kst[m] + ke - 1);
         const double *tmp_var = x + nxy * s->kst[m + 1]; /* upper neighbour's var[k=0] */
         const double *tmp_v = s->tmp_v + nxy * m;
+#pragma omp parallel for schedule(static)
         for (size_t ij = 0; ij < nxy; ij++) {
             double det_pdd = wt[ij] * tmp_v[ij] - ((double)1.0);
             y2[nxy * m + ij] = (xt[ij] * tmp_v[ij] - tmp_var[ij]) / det_pdd;
@@ -234,6 +241,7 @@ static void solve_trid(orc_ppe *s, double *x)
     for (int m = 1; m < P; m++) memcpy(y1 + nxy * m, y3 + nxy * (m - 1), sizeof(double) * nxy);
     for (int m = 0; m < P; m++) {
         const int k0 = s->kst[m], ke = s->ksz[m];
+#pragma omp parallel for schedule(static)
         for (int k = 0; k < ke; k++)
             for (size_t ij = 0; ij < nxy; ij++) {
                 size_t g = ij + nxy * (size_t)(k0 + k);
@@ -251,6 +259,8 @@ void orc_ppe_execute(orc_ppe *s, double *var)
     const int nx = s->nx, ny = s->ny, nz = s->nz;
     const size_t gx = (size_t)nx + 2, gxy = gx * (ny + 2), nxy = (size_t)nx * ny;
     double *x = s->work;
+    /* every line transform is independent: threads split the lines */
+#pragma omp parallel for collapse(2) schedule(static)
     for (int k = 0; k < nz; k++) {
         for (int j = 0; j < ny; j++) {
             memcpy(&x[(size_t)k * nxy + (size_t)j * nx], &var[(size_t)(k + 1) * gxy + (size_t)(j + 1) * gx + 1],
@@ -258,11 +268,14 @@ void orc_ppe_execute(orc_ppe *s, double *var)
             hc_fft_r2hc(s->px, &x[(size_t)k * nxy + (size_t)j * nx], 1);
         }
     }
+#pragma omp parallel for collapse(2) schedule(static)
     for (int k = 0; k < nz; k++)
         for (int i = 0; i < nx; i++) hc_fft_r2hc(s->py, &x[(size_t)k * nxy + i], nx);
     solve_trid(s, x);
+#pragma omp parallel for collapse(2) schedule(static)
     for (int k = 0; k < nz; k++)
         for (int i = 0; i < nx; i++) hc_fft_hc2r(s->py, &x[(size_t)k * nxy + i], nx);
+#pragma omp parallel for collapse(2) schedule(static)
     for (int k = 0; k < nz; k++)
         for (int j = 0; j < ny; j++) {
             double *src = &x[(size_t)k * nxy + (size_t)j * nx];

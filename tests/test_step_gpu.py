@@ -190,6 +190,43 @@ def test_full_size_step_invariants(gpu):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("path", ["step", "phases"])
+def test_convecting_frame_matches_oracle(gpu, oracle_mod, precision, path):
+    """u_crf = 0.3: the convecting reference frame (transform2CRF,
+    mod_calcVel.f90:26-50; the u_crf advection terms of :93, 115, 137; the u
+    wall value -u_crf of imposeBCVel, mod_updateBound.f90:57-108).  "step"
+    runs pl_channel_step (the fused RK kernels' u_crf specialisations at
+    64x48x32); "phases" runs the separate RK1, RK2, calcRHS, Poisson and
+    correction kernels.  FP64 against the oracle at 1e-12; mixed at 1e-7
+    (FP32 stencils: 3 steps leave a few 1e-9)."""
+    plb, O = gpu, oracle_mod
+    nx, ny, nz, nsteps, u_crf = 64, 48, 32, 3, 0.3
+    prec = plb.PL_FP64 if precision == "fp64" else plb.PL_MIXED
+    cfg = plb.ChannelConfig(nx=nx, ny=ny, nz=nz, stretch_ratio=1.5, re_tau=180.0, u_crf=u_crf, precision=prec)
+    ch = plb.Channel(cfg)
+    ch.init_flow(42, 0.1)
+    for _ in range(nsteps):
+        if path == "step":
+            ch.step(1)
+        else:
+            for ph in ("rk1", "rk2", "calc_rhs", "poisson", "correct_force"):
+                ch.phase(ph)
+    g = O.Grid(nx, ny, nz, stretch=1.5, re_tau=180.0, u_crf=u_crf)
+    u, v, w, p = g.init_flow(42, 0.1)
+    ppe = O.PPE(nx, ny, nz, g.g.dx, g.g.dy, g.dzf_global)
+    u1, v1, w1 = g.zeros(), g.zeros(), g.zeros()
+    for _ in range(nsteps):
+        g.step(ppe, u, v, w, u1, v1, w1, p)
+    gu, gv, gw, _ = ch.get_fields()
+    errs = [rel(a, b) for a, b in ((gu, u), (gv, v), (gw, w))]
+    print(f"u_crf {u_crf} {precision} {path}: max rel err u v w", errs)
+    # the u wall ghosts hold 2*(-u_crf) - u(1): the frame velocity reached them
+    assert np.abs(gu[0, 1:-1, 1:-1] + gu[1, 1:-1, 1:-1] + 2 * u_crf).max() < 1e-12
+    assert max(errs) < (TOL64 if precision == "fp64" else 1e-7)
+    ch.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
 @pytest.mark.parametrize("nx,ny,nz", [(64, 48, 32), (192, 48, 24), (768, 16, 16)])
 def test_step_matches_phases(gpu, precision, nx, ny, nz):
     """pl_channel_step fuses calcRHS into the Poisson solve's forward x
