@@ -75,20 +75,24 @@ int pl_ppe_create(pl_ppe **out, int nx, int ny, int nz, double dx, double dy, co
 int pl_ppe_solve(pl_ppe *s, void *d_var, void *stream);
 int pl_ppe_destroy(pl_ppe *s);
 
-/* Allocation-free variant of pl_ppe_solve, for callers that cannot allocate
- * device memory while they solve: a driver capturing its time loop into a
- * CUDA graph (cudaMalloc is not permitted during stream capture) or a host
- * program whose device memory belongs to another allocator.  No counterpart
- * in the reference.  It runs the same kernels as pl_ppe_solve on a plan made
- * with PL_MIXED and nparts = 0 (Thomas), but the FP64 forward-sweep scratch of
- * the tridiagonal solve lives in a fixed 16 MiB device array inside the
- * library instead of in the plan; it calls no cudaMalloc or cudaFree.
+/* Allocation-free variant of pl_ppe_solve, for callers that cannot call
+ * cudaMalloc while they solve: a host program whose device memory is owned by
+ * another allocator (a pool that claimed the GPU's memory at start-up), or a
+ * loop that must not stall on cudaMalloc, which can wait for the device to go
+ * idle.  No counterpart in the reference.  The plan must be made with
+ * PL_MIXED and nparts = 0 (Thomas).  The solve runs the same x and y
+ * transforms as pl_ppe_solve, but always the tridiagonal kernel that keeps
+ * its FP64 forward-swept values in device memory (pl_ppe_solve keeps them in
+ * tensor memory where nz allows), and that memory is a fixed 16 MiB array
+ * inside the library instead of the plan's buffer; it calls no cudaMalloc or
+ * cudaFree.  The results equal pl_ppe_solve's (same arithmetic).
  * Limit: nx*ny*nz <= 2,097,152 (e.g. 128^3); larger plans are rejected with an
  * error.  The array's device address is looked up on the first call on each
- * device (make that first call before any stream capture).  Every call on a
- * device shares the array: calls that overlap on the GPU (other streams,
- * other threads) race; serialise them.  The plan's other tables are read-only
- * and are shared safely. */
+ * device (and again after the device's context is recreated): make that first
+ * call before any stream capture.  Every call on a device shares the array:
+ * calls that overlap on the GPU (other streams, other threads) race;
+ * serialise them.  The plan's other tables are read-only and are shared
+ * safely. */
 int pl_ppe_solve_noalloc(pl_ppe *s, void *d_var, void *stream);
 
 /* ======================================================================

@@ -2,7 +2,7 @@
 //
 // Reference: src/src_c/mod_poisson_solver.c (init :178-309, Thomas :311-359,
 // PDD :105-176/:361-466, execute :468-605), src/src_c/mod_fft_fftw.inc
-// (plans :100-155, eigenvalues :175-198).
+// (init_fft :35-90, execute_fft :92-95, get_eigen_values :110-133).
 //
 // Kernels (one launch each per solve):
 //   k_xfft<fwd>  rows of the k-plane, two rows per complex line (x: contiguous)
@@ -14,6 +14,7 @@
 // (ix <= nx/2, jy <= ny/2): a quarter of the reference's b array.
 #include <algorithm>
 #include <cstdint>
+#include <cuda.h> // CUcontext (the driver entry point is fetched through the runtime)
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -942,7 +943,7 @@ int ppe_create(Ppe *s, int nx, int ny, int nz, double dx, double dy, const doubl
     s->prec = prec;
     s->ncx = nx / 2 + 1;
     s->ncy = ny / 2 + 1;
-    s->norm = 1.0 / (1.0 * nx * 1.0 * ny); // mod_fft_fftw.inc:154, PP/PP
+    s->norm = 1.0 / (1.0 * nx * 1.0 * ny); // mod_fft_fftw.inc:89, PP/PP
     const int P = nparts >= 1 ? nparts : 1;
 
     int rx[FFT_MAX_STAGES], ry[FFT_MAX_STAGES], nsx = 0, nsy = 0;
@@ -1334,23 +1335,45 @@ int ppe_solve_fp32_from_x(Ppe *s, float *d_var, const double *mode0, cudaStream_
 // ------------------------------------------------------------------------
 // Allocation-free solve (pl_ppe_solve_noalloc in include/powerllel_b200.h).
 //
-// Some callers cannot call cudaMalloc while they solve: a driver that records
-// its time loop into a CUDA graph (allocation is not permitted while a stream
-// is being captured), or a host program whose device memory is owned by
-// another allocator.  For them the mixed-precision Thomas solve takes its FP64
-// forward-sweep scratch from this fixed device array instead of the buffer
-// pl_ppe_create allocates.  The array is file-scope device memory: every GPU
-// that loads the library holds it (16 MiB) until the process exits.
+// Some callers cannot call cudaMalloc while they solve: a host program whose
+// device memory is owned by another allocator (a pool that claimed the GPU's
+// memory at start-up), or a loop that must not stall on cudaMalloc, which can
+// wait for the device to go idle.  For them the mixed-precision Thomas solve
+// runs the HBM-scratch sweep kernel (k_thomas), whose FP64 forward-swept
+// values go to this fixed device array instead of the buffer pl_ppe_create
+// allocates.  The array is file-scope device memory: every GPU that loads
+// the library holds it (16 MiB) until the process exits.
 // ------------------------------------------------------------------------
 namespace pl {
 
 constexpr size_t NOALLOC_SCRATCH_DOUBLES = (size_t)1 << 21; // 16 MiB: nx*ny*nz <= 2,097,152
 static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_SCRATCH_DOUBLES];
 
-// device address of g_noalloc_scratch, looked up once per device: in host
-// code the symbol names a host-side stand-in, not device memory
+// Device address of g_noalloc_scratch.  In host code the symbol names a
+// host-side stand-in, not device memory, so the address is looked up with
+// cudaGetSymbolAddress once per device and context (with that device
+// current); a new context on the device (after cudaDeviceReset) looks it up
+// again, since the array then lives at a new address.
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+
+static CtxGetCurrentFn ctx_get_current()
+{
+    static CtxGetCurrentFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<CtxGetCurrentFn>(f);
+    }
+    return fn;
+}
+
 static std::mutex g_noalloc_mu;
 static double *g_noalloc_ptr[64] = {nullptr};
+static CUcontext g_noalloc_ctx[64] = {nullptr};
 
 static int noalloc_scratch(double **out)
 {
@@ -1361,14 +1384,22 @@ static int noalloc_scratch(double **out)
         return -1;
     }
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
+    CtxGetCurrentFn get = ctx_get_current();
+    auto current = [&]() {
+        CUcontext c = nullptr;
+        if (get && get(&c) != CUDA_SUCCESS) c = nullptr;
+        return c;
+    };
+    const CUcontext ctx = current(); // null: no context is current in this thread yet
+    if (!g_noalloc_ptr[dev] || ctx == nullptr || ctx != g_noalloc_ctx[dev]) {
         void *ptr = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch); // makes the device's context current
         if (e != cudaSuccess || ptr == nullptr) {
             set_error(std::string("pl_ppe_solve_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
             return -1;
         }
         g_noalloc_ptr[dev] = static_cast<double *>(ptr);
+        g_noalloc_ctx[dev] = current();
     }
     *out = g_noalloc_ptr[dev];
     return 0;

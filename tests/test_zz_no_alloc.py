@@ -1,10 +1,9 @@
 """GPU test of pl_ppe_solve_noalloc, the allocation-free PPE entry point.
 
-Callers that cannot allocate device memory while they solve (a driver that
-captures its time loop into a CUDA graph, where cudaMalloc is not permitted,
-or a host program whose device memory belongs to another allocator) use it:
-it takes the FP64 scratch of the tridiagonal sweeps from a fixed array inside
-the library.  This file sorts last so that a run stopping at the first failure
+Callers that cannot call cudaMalloc while they solve (a host program whose
+device memory belongs to another allocator, or a loop that must not stall on
+cudaMalloc) use it: it takes the FP64 scratch of the tridiagonal sweep from a
+fixed array inside the library.  This file sorts last so that a run stopping at the first failure
 has already run every other test; it also passes on its own."""
 import ctypes as C
 
