@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libpowerllel_b200.so")
-SOURCES = ["ppe.cu", "stencil.cu", "rk_fused.cu", "channel.cu", "adjoint.cu", "monitor.cu"]
+SOURCES = ["ppe.cu", "stencil.cu", "rk_fused.cu", "rk_mixed.cu", "channel.cu", "adjoint.cu", "monitor.cu"]
 HEADERS = ["common.cuh", "fft.cuh", "ppe.cuh", "stencil.cuh", "stencil_rhs.cuh", "tmem.cuh", "trid_tables.h", "channel.cuh"]
 
 NVCC_FLAGS = [

@@ -243,8 +243,10 @@ static void channel_free(pl_channel *c)
     cudaFree(c->ub);
     cudaFree(c->vb);
     cudaFree(c->wb);
-    cudaFree(c->pb);
-    cudaFree(c->pm);
+    cudaFree(c->p32);
+    cudaFree(c->pm32);
+    cudaFree(c->pb32);
+    cudaFree(c->mxtab);
     cudaFree(c->d1u);
     cudaFree(c->d1v);
     cudaFree(c->d1w);
@@ -321,12 +323,15 @@ extern "C" int pl_channel_create(pl_channel **out, const pl_channel_config *cfg)
         cudaMemset(*f, 0, sizeof(float) * n);
         return true;
     };
-    c->fused_rk = rk_fused_supported(c->sp);
+    // both RK stages in one kernel where the grid tiles: 32 x 8 (FP64
+    // kernel) or 32 x 16 (mixed kernel); else the two stage kernels
+    c->fused_rk = mixed ? rk_mixed_supported(c->sp) : rk_fused_supported(c->sp);
     bool ok = dalloc(&c->u, c->nf) && dalloc(&c->v, c->nf) && dalloc(&c->w, c->nf) && dalloc(&c->p, c->np) &&
               dalloc(&c->ub, c->nf) && dalloc(&c->vb, c->nf) && dalloc(&c->wb, c->nf);
     if (ok && !mixed) ok = dalloc(&c->u1, c->nf) && dalloc(&c->v1, c->nf) && dalloc(&c->w1, c->nf);
     if (ok && mixed)
-        ok = dalloc(&c->pb, c->np) && dalloc(&c->pm, c->np) && falloc(&c->d1u, c->nf) && falloc(&c->d1v, c->nf) &&
+        ok = falloc(&c->p32, c->np) && falloc(&c->pb32, c->np) && falloc(&c->pm32, c->np) &&
+             falloc(&c->mxtab, (size_t)12 * (c->nz + 2)) && falloc(&c->d1u, c->nf) && falloc(&c->d1v, c->nf) &&
              falloc(&c->d1w, c->nf) && falloc(&c->r32, c->np) && dalloc(&c->mode0, c->nz) &&
              dalloc(&c->plane_part, (size_t)std::max(warp_partials_per_plane(c->sp), c->sp.ny / 2) * c->nz);
     if (!ok) {
@@ -340,8 +345,16 @@ extern "C" int pl_channel_create(pl_channel **out, const pl_channel_config *cfg)
     if (ppe_create(&c->ppe, c->nx, c->ny, c->nz, dx, dy, c->dzf_global.data(), cfg->trid_parts,
                    mixed ? PREC_MIXED : PREC_FP64))
         return fail();
+    if (mixed) {
+        const std::vector<float> tab = rk_mixed_table(c->sp, c->dzf, c->dzf_inv, c->dzc_inv);
+        if (cudaMemcpy(c->mxtab, tab.data(), sizeof(float) * tab.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+            set_error("pl_channel_create: upload of the mixed RK coefficients failed");
+            return fail();
+        }
+    }
     c->max_blocks = ((c->nx + 63) / 64) * ((c->ny + 3) / 4) * c->nz;
-    if (c->fused_rk && rk_fused_blocks(c->sp) > c->max_blocks) c->max_blocks = rk_fused_blocks(c->sp);
+    if (c->fused_rk && !mixed && rk_fused_blocks(c->sp) > c->max_blocks) c->max_blocks = rk_fused_blocks(c->sp);
+    if (c->fused_rk && mixed && rk_mixed_blocks(c->sp) > c->max_blocks) c->max_blocks = rk_mixed_blocks(c->sp);
     c->rb.max_blocks = c->max_blocks;
     if (cudaMalloc(&c->rb.partial, sizeof(double) * 3 * c->max_blocks) != cudaSuccess ||
         cudaMalloc(&c->rb.scalar, sizeof(double) * 8) != cudaSuccess ||
@@ -389,8 +402,9 @@ extern "C" int pl_channel_init_flow(pl_channel *c, uint64_t seed, double noise)
     PL_CUDA_TRY(cudaMemsetAsync(c->v, 0, sizeof(double) * c->nf, c->stream));
     PL_CUDA_TRY(cudaMemsetAsync(c->w, 0, sizeof(double) * c->nf, c->stream));
     PL_CUDA_TRY(cudaMemsetAsync(c->p, 0, sizeof(double) * c->np, c->stream));
-    if (c->pb) PL_CUDA_TRY(cudaMemsetAsync(c->pb, 0, sizeof(double) * c->np, c->stream));
-    if (c->pm) PL_CUDA_TRY(cudaMemsetAsync(c->pm, 0, sizeof(double) * c->np, c->stream));
+    for (float *q : {c->p32, c->pb32, c->pm32})
+        if (q) PL_CUDA_TRY(cudaMemsetAsync(q, 0, sizeof(float) * c->np, c->stream));
+    c->p_stale = false;
     c->nsolve = 0;
     int rc = launch_init_fill(c->u, c->v, c->w, dprof, seed, noise, c->sp, c->stream);
     if (!rc) rc = launch_mean_sum(c->u, c->sp, c->m, c->rb, 0, c->stream);
@@ -401,6 +415,14 @@ extern "C" int pl_channel_init_flow(pl_channel *c, uint64_t seed, double noise)
 }
 
 static inline bool is_mixed(const pl_channel *c) { return c->cfg.precision == PL_MIXED; }
+
+const double *pl::channel_p64(pl_channel *c)
+{
+    if (c->p32 && c->p_stale) {
+        if (launch_widen(c->p32, c->p, c->np, c->stream) == 0) c->p_stale = false;
+    }
+    return c->p;
+}
 
 // mixed path pressure prediction: the first two projections after the
 // initial field solve for the full pressure (the first one removes the
@@ -425,7 +447,7 @@ extern "C" int pl_phase_rk2(pl_channel *c)
     int rc;
     if (is_mixed(c)) {
         rc = launch_rk2_mixed(c->u, c->v, c->w, c->d1u, c->d1v, c->d1w, c->ub, c->vb, c->wb, c->sp, c->m, c->ms,
-                              c->pm, mixed_incremental(c), c->stream);
+                              c->pm32, mixed_incremental(c), c->stream);
         std::swap(c->u, c->ub);
         std::swap(c->v, c->vb);
         std::swap(c->w, c->wb);
@@ -453,9 +475,9 @@ extern "C" int pl_phase_calc_rhs(pl_channel *c)
 static PressureUpdate mixed_pressure_update(const pl_channel *c)
 {
     PressureUpdate pu;
-    pu.q = c->pm;
-    pu.p = c->p;
-    pu.qnext = c->pb;
+    pu.q = c->pm32;
+    pu.p = c->p32;
+    pu.qnext = c->pb32;
     pu.incremental = mixed_incremental(c);
     pu.qmode = (c->nsolve + 1 >= 3) ? 1 : 0;
     return pu;
@@ -465,6 +487,7 @@ extern "C" int pl_phase_poisson(pl_channel *c)
 {
     if (is_mixed(c)) {
         const PressureUpdate pu = mixed_pressure_update(c);
+        c->p_stale = true;
         return ppe_solve_fp32(&c->ppe, c->r32, c->mode0, c->stream, &pu);
     }
     return ppe_solve_fp64(&c->ppe, c->p, c->stream);
@@ -492,6 +515,7 @@ static int phase_rhs_poisson(pl_channel *c)
             if (launch_plane_sums(c->plane_part, c->sp.ny / 2, c->nz, c->mode0, c->stream)) return -1;
             channel_mark(c, "rhs_xfft");
             const PressureUpdate pu = mixed_pressure_update(c);
+            c->p_stale = true;
             return ppe_solve_fp32_from_x(&c->ppe, c->r32, c->mode0, c->stream, &pu);
         }
     } else {
@@ -513,14 +537,15 @@ extern "C" int pl_phase_correct_force(pl_channel *c)
                                : launch_correct_force_fp64(c->p, c->u, c->v, c->w, c->sp, c->m, c->cfg.is_forced[0],
                                                            c->ms.scalar, c->stream);
     if (is_mixed(c)) {
-        std::swap(c->pm, c->pb); // the prediction written by the solve
+        std::swap(c->pm32, c->pb32); // the prediction written by the solve
         c->nsolve++;
     }
     channel_mark(c, "correct_force");
     return rc;
 }
 
-// both RK stages in one kernel (out of place), when the grid tiles by 32 x 8
+// both RK stages in one kernel (out of place) when the grid tiles (32 x 8 FP64,
+// 32 x 16 mixed), else the two stage kernels
 extern "C" int pl_phase_rk(pl_channel *c)
 {
     int rc;
@@ -529,8 +554,8 @@ extern "C" int pl_phase_rk(pl_channel *c)
         if (!rc) rc = pl_phase_rk2(c);
         return rc;
     }
-    rc = is_mixed(c) ? launch_rk_fused_mixed(c->u, c->v, c->w, c->ub, c->vb, c->wb, c->sp, c->m, c->ms, c->pm,
-                                             mixed_incremental(c), c->stream)
+    rc = is_mixed(c) ? launch_rk_mixed(c->u, c->v, c->w, c->ub, c->vb, c->wb, c->sp, c->m, c->mxtab, c->ms, c->pm32,
+                                       mixed_incremental(c), c->stream)
                      : launch_rk_fused_fp64(c->u, c->v, c->w, c->ub, c->vb, c->wb, c->sp, c->m, c->ms, c->stream);
     std::swap(c->u, c->ub);
     std::swap(c->v, c->vb);
@@ -649,6 +674,8 @@ extern "C" int pl_channel_get_fields(pl_channel *c, double *u, double *v, double
         expand_ghosted(c, tmp.data(), host[q], c->nz + 2, 0);
     }
     if (p) {
+        channel_p64(c);
+        PL_CUDA_TRY(cudaStreamSynchronize(c->stream));
         PL_CUDA_TRY(cudaMemcpy(tmp.data(), c->p, sizeof(double) * c->np, cudaMemcpyDeviceToHost));
         // interior planes 0..nz-1 become k = 1..nz; ghosts p(0) = p(1), p(nz+1) = p(nz)
         expand_ghosted(c, tmp.data(), p, c->nz, -1);
@@ -665,6 +692,8 @@ extern "C" int pl_channel_get_field(pl_channel *c, int which, double *host)
     }
     std::vector<double> tmp(c->nf);
     if (which == 3) {
+        channel_p64(c);
+        PL_CUDA_TRY(cudaStreamSynchronize(c->stream));
         PL_CUDA_TRY(cudaMemcpy(tmp.data(), c->p, sizeof(double) * c->np, cudaMemcpyDeviceToHost));
         expand_ghosted(c, tmp.data(), host, c->nz, -1);
         return 0;
@@ -730,7 +759,7 @@ extern "C" void *pl_channel_field(pl_channel *c, int which)
     case 0: return c->u;
     case 1: return c->v;
     case 2: return c->w;
-    case 3: return c->p;
+    case 3: return (void *)channel_p64(c);
     case 4: return is_mixed(c) ? (void *)c->d1u : (void *)c->u1;
     case 5: return is_mixed(c) ? (void *)c->d1v : (void *)c->v1;
     case 6: return is_mixed(c) ? (void *)c->d1w : (void *)c->w1;

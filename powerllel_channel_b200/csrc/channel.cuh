@@ -20,18 +20,23 @@ struct pl_channel {
     pl::MeshDev m{};
     // FP64 path: u,v,w = ua,va,wa; stage-1 fields u1,v1,w1; p
     // mixed path: u,v,w ping-pong between (ua,va,wa) and (ub,vb,wb); stage-1
-    // increments d1u,d1v,d1w (FP32); p = p_n (FP64, updated in place); the
-    // pressure prediction for the next projection in pm, written into pb by
-    // the correction and swapped (FP64); the PPE works in place on r32 (FP32)
+    // increments d1u,d1v,d1w (FP32, the per-phase entries only); p32 = p_n
+    // (FP32, updated in place by the solve); the pressure prediction for the
+    // next projection in pm32, written into pb32 by the solve and swapped;
+    // the PPE works in place on r32 (FP32); p (FP64) is p32 widened on demand
+    // for readers (channel_p64); mxtab: the mixed RK kernel's per-plane
+    // coefficients
     double *u = nullptr, *v = nullptr, *w = nullptr;
     double *u1 = nullptr, *v1 = nullptr, *w1 = nullptr;
     double *p = nullptr;
-    double *ub = nullptr, *vb = nullptr, *wb = nullptr, *pb = nullptr, *pm = nullptr;
+    double *ub = nullptr, *vb = nullptr, *wb = nullptr;
+    float *p32 = nullptr, *pm32 = nullptr, *pb32 = nullptr, *mxtab = nullptr;
+    bool p_stale = false; // mixed: p lags p32
     float *d1u = nullptr, *d1v = nullptr, *d1w = nullptr, *r32 = nullptr;
     double *plane_part = nullptr, *mode0 = nullptr;
     int incremental = 1;   // mixed path: solve for a pressure increment (Thomas)
     long long nsolve = 0;  // projections since the initial field (mixed prediction schedule)
-    bool fused_rk = false; // both RK stages in one kernel (rk_fused.cu)
+    bool fused_rk = false; // both RK stages in one kernel (rk_fused.cu, rk_mixed.cu)
     pl::Ppe ppe;
     pl::ReduceBuf rb;
     pl::MeanState ms;
@@ -46,3 +51,9 @@ struct pl_channel {
     std::vector<cudaEvent_t> *prof_events = nullptr;
     std::vector<std::string> *prof_names = nullptr;
 };
+
+namespace pl {
+// the FP64 pressure of the current state (the mixed path widens p32 into p
+// on the channel's stream when it has changed)
+const double *channel_p64(pl_channel *c);
+} // namespace pl

@@ -125,8 +125,9 @@ int host_scalar(pl_channel *c, const double *d, double *h)
     return 0;
 }
 
-// the pressure the monitors report: p of the current state (FP64 in both paths)
-const double *state_p(const pl_channel *c) { return c->p; }
+// the pressure the monitors report: p of the current state, FP64 in both
+// paths (the mixed path widens its FP32 pressure on demand)
+const double *state_p(pl_channel *c) { return pl::channel_p64(c); }
 
 } // namespace
 

@@ -197,21 +197,21 @@ __device__ __forceinline__ int opaque_tid()
 }
 
 // pressure update of one point o (PressureUpdate in ppe.cuh); dp is the
-// FP32 increment widened to FP64
-__device__ __forceinline__ void pressure_update(const PressureUpdate &pu, size_t o, double dp)
+// FP32 increment
+__device__ __forceinline__ void pressure_update(const PressureUpdate &pu, size_t o, float dp)
 {
-    const double pn = (pu.incremental ? __ldg(pu.q + o) : 0.0) + dp;
-    const double pold = __ldg(pu.p + o);
+    const float pn = (pu.incremental ? __ldg(pu.q + o) : 0.f) + dp;
+    const float pold = __ldg(pu.p + o);
     // the prediction first: storing over the just-read p before another
     // stream measured markedly slower on B200
-    pu.qnext[o] = pu.qmode ? 2.0 * pn - pold : pn;
+    pu.qnext[o] = pu.qmode ? 2.f * pn - pold : pn;
     pu.p[o] = pn;
 }
 
 __global__ void __launch_bounds__(256) k_pressure_update(const float *__restrict__ dp, PressureUpdate pu, size_t n)
 {
     for (size_t o = (size_t)blockIdx.x * 256 + threadIdx.x; o < n; o += (size_t)gridDim.x * 256)
-        pressure_update(pu, o, (double)__ldg(dp + o));
+        pressure_update(pu, o, __ldg(dp + o));
 }
 
 // Persistent versions on the compact layout [k][j][i] (the device solves).
@@ -319,8 +319,8 @@ __global__ void __launch_bounds__(pf_x_threads<T>()) k_xfft_pf(const T *__restri
                 dst[(size_t)(2 * b + 1) * N + m] = d1;
                 if (sizeof(T) == 4 && pu.p) {
                     const size_t o = (size_t)k * N * ny + (size_t)2 * p0 * N + (size_t)2 * b * N + m;
-                    pressure_update(pu, o, (double)d0);
-                    pressure_update(pu, o + N, (double)d1);
+                    pressure_update(pu, o, (float)d0);
+                    pressure_update(pu, o + N, (float)d1);
                 }
             };
             ct_last_stage<V, FWD, false, N, NB, 1, N, NT>(buf, nb, tw, tid, put);
@@ -861,6 +861,13 @@ __global__ void k_widen(const float *__restrict__ in, double *__restrict__ out, 
 {
     for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x)
         out[q] = (double)in[q];
+}
+
+int launch_widen(const float *in, double *out, size_t n, cudaStream_t st)
+{
+    k_widen<<<1184, 256, 0, st>>>(in, out, n);
+    PL_CHECK_LAUNCH();
+    return 0;
 }
 
 // ------------------------------------------------------------------------

@@ -63,7 +63,10 @@ int ppe_solve_fp64(Ppe *s, double *d_var, cudaStream_t st);
 // increment solve, fused into the inverse x transform where the layout
 // allows (one kernel otherwise): p_new = (incremental ? q : 0) + dp stored
 // in p (in place of p_n), and the next prediction qnext = qmode ?
-// 2 p_new - p_n : p_new (FP64, interior-only layout).
+// 2 p_new - p_n : p_new (FP32, interior-only layout).  The projection's
+// accuracy does not rest on these values: the RK kernel subtracts dt G q
+// from whatever q holds and the FP64 residual of the next increment solve
+// takes up the difference.
 // The ghosted velocity fields and factors of calcRHS
 // (rhs = (u_i - u_{i-1}) dt^-1 dx^-1 + (v_j - v_{j-1}) dt^-1 dy^-1
 //        + (w_k - w_{k-1}) dt^-1 dzf_k^-1, mod_calcRHS.f90:19-33) for the
@@ -84,8 +87,8 @@ template <typename T> int ppe_xfwd_div(Ppe *s, const DivIn &d, T *out, double *p
 int ppe_solve_fp64_from_x(Ppe *s, double *d_var, cudaStream_t st);
 
 struct PressureUpdate {
-    const double *q = nullptr;
-    double *p = nullptr, *qnext = nullptr;
+    const float *q = nullptr;
+    float *p = nullptr, *qnext = nullptr;
     int incremental = 0, qmode = 0;
 };
 int ppe_solve_fp32(Ppe *s, float *d_var, const double *mode0, cudaStream_t st, const PressureUpdate *pu = nullptr);
@@ -99,6 +102,9 @@ int ppe_solve_fp32_from_x(Ppe *s, float *d_var, const double *mode0, cudaStream_
 // j*sj + k*sk].  The interior-only work array receives the transform.
 int ppe_solve_fp64_strided(Ppe *s, const double *in, double *out, size_t off, size_t sj, size_t sk,
                            double *d_work, cudaStream_t st);
+
+// out[q] = (double)in[q], q < n
+int launch_widen(const float *in, double *out, size_t n, cudaStream_t st);
 
 } // namespace pl
 

@@ -1,5 +1,6 @@
 // rk_fused.cu -- both RK2 stages of timeIntVelRK1 / timeIntVelRK2
-// (mod_calcVel.f90:52-146, 240-334) with their wall fills in one kernel.
+// (mod_calcVel.f90:52-146, 240-334) with their wall fills in one kernel, FP64
+// (the parity path; the mixed path's kernel is rk_mixed.cu).
 //
 // 2.5D blocking: a CTA owns a 32 x 8 tile of (i, j) and marches up a chunk of
 // k-planes.  Shared-memory rings hold the last planes of u (halo 2 in x, y)
@@ -9,11 +10,8 @@
 // new u, v, w, instead of writing and re-reading u1, v1, w1 between two
 // kernels.
 //
-// FP64 path: the rings hold u and u1 in double, the expressions are the
-// reference's.  Mixed path: the rings hold u, the stage-1 increment
-// d1 = dt*RHS(u) and u1 = u + d1, all in float (FP32 stencil arithmetic); the
-// update u_new = ((u + d1) + dt*RHS(u1) + u)/2 uses the FP64 u of the centre
-// and is stored in FP64.
+// The rings hold u and u1 in double; the expressions are the reference's,
+// in the reference's order.
 #include "fft.cuh" // cp.async helpers
 #include "stencil.cuh"
 #include "stencil_rhs.cuh"
@@ -24,15 +22,7 @@ constexpr int FX = 32, FY = 8;          // tile
 constexpr int UW = FX + 4, UH = FY + 4; // ring plane with a halo of 2
 constexpr int UPS = UW * UH;            // 432 values per plane
 
-template <bool MIXED> struct RkTraits;
-template <> struct RkTraits<false> {
-    using R = double;       // ring and stencil arithmetic type
-    static constexpr int NS = 3; // planes per ring
-};
-template <> struct RkTraits<true> {
-    using R = float;
-    static constexpr int NS = 3;
-};
+constexpr int NS = 3; // planes per ring
 
 template <typename R> struct RingLoad {
     const R *a;
@@ -80,21 +70,18 @@ __device__ __forceinline__ Nb32 ring_nb(int x, int y, int s0, int sm, int sp)
     return n;
 }
 
-template <bool MIXED, bool CRF>
-__global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double *__restrict__ u, const double *__restrict__ v,
-                                                     const double *__restrict__ w, double *__restrict__ uo,
-                                                     double *__restrict__ vo, double *__restrict__ wo, StepParams p,
-                                                     MeshDev m, MeanRed red, int kchunk,
-                                                     const double *__restrict__ pq, int pinc)
+template <bool CRF>
+__global__ void __launch_bounds__(FX *FY, 3) k_rk_fused(const double *__restrict__ u, const double *__restrict__ v,
+                                                       const double *__restrict__ w, double *__restrict__ uo,
+                                                       double *__restrict__ vo, double *__restrict__ wo, StepParams p,
+                                                       MeshDev m, MeanRed red, int kchunk)
 {
-    using R = typename RkTraits<MIXED>::R;
-    constexpr int NS = RkTraits<MIXED>::NS;
+    using R = double;
     constexpr int FS = NS * UPS; // ring size per field
     static_assert(NS == 3, "the ring slot rotation of the march assumes three-plane rings");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R *ur = reinterpret_cast<R *>(smem_raw); // u, v, w rings
-    R *qr = ur + 3 * FS;                     // u1 (FP64) or d1 (mixed) rings
-    R *sr = qr + 3 * FS;                     // mixed: u1 = u + d1 in FP32 (the stage-2 stencil input)
+    R *qr = ur + 3 * FS;                     // u1 rings
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int i0 = blockIdx.x * FX, j0 = blockIdx.y * FY;
     const int kbeg = blockIdx.z * kchunk + 1, kend = min(kbeg + kchunk - 1, p.nz);
@@ -141,22 +128,8 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
             lxy[sl] = ly[sl] * UW + lx[sl];
         }
     }
-    auto load_u_plane = [&](int kq, int s) { // kq in [0, nz+1], into ring slot s = kq % NS
-        const size_t gk = sk * kq;
-#pragma unroll
-        for (int sl = 0; sl < 2; sl++) {
-            if (sl == 0 || lval1) {
-                const size_t g = gk + loff[sl];
-                const int q = s * UPS + lxy[sl];
-                ur[0 * FS + q] = (R)__ldg(u + g);
-                ur[1 * FS + q] = (R)__ldg(v + g);
-                ur[2 * FS + q] = (R)__ldg(w + g);
-            }
-        }
-    };
-
-    // FP64 rings hold the fields as loaded: the plane can be copied
-    // asynchronously (cp.async), in flight while stage 2 runs
+    // the rings hold the fields as loaded: a plane is copied asynchronously
+    // (cp.async), in flight while stage 2 runs
     auto load_u_plane_async = [&](int kq, int s) {
         const size_t gk = sk * kq;
 #pragma unroll
@@ -194,19 +167,10 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
                                    RingLoad3<R>{ur + FS + om, ur + FS + oc, ur + FS + op},
                                    RingLoad3<R>{ur + 2 * FS + om, ur + 2 * FS + oc, ur + 2 * FS + op}, RingNbC{}, cst,
                                    ru, rv, rw);
-            if (MIXED) { // increments, and u1 = u + d1 for the stage-2 stencils
-                const R du = dt * ru, dv = dt * rv, dw = (mq == p.nz) ? (R)0 : dt * rw; // w1(nz) = 0 = w(nz)
-                qr[oc] = du;
-                qr[FS + oc] = dv;
-                qr[2 * FS + oc] = dw;
-                sr[oc] = ur[oc] + du;
-                sr[FS + oc] = ur[FS + oc] + dv;
-                sr[2 * FS + oc] = ur[2 * FS + oc] + dw;
-            } else {      // u1 = u + dt*(visc - conv)
-                qr[oc] = ur[oc] + dt * (ru + (R)p.fb[0]);
-                qr[FS + oc] = ur[FS + oc] + dt * (rv + (R)p.fb[1]);
-                qr[2 * FS + oc] = (mq == p.nz) ? (R)0 : ur[2 * FS + oc] + dt * (rw + (R)p.fb[2]);
-            }
+            // u1 = u + dt*(visc - conv); w1(nz) = 0, the wall
+            qr[oc] = ur[oc] + dt * (ru + (R)p.fb[0]);
+            qr[FS + oc] = ur[FS + oc] + dt * (rv + (R)p.fb[1]);
+            qr[2 * FS + oc] = (mq == p.nz) ? (R)0 : ur[2 * FS + oc] + dt * (rw + (R)p.fb[2]);
         }
     };
 
@@ -217,19 +181,9 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
         for (int sl = 0; sl < HSLOTS; sl++) {
             if (sl == 1 && !hval1) break;
             const int xy = hxy[sl];
-            if (MIXED) { // u1(g) = 2bc - u1(i) and u(g) = 2bc - u(i)  =>  d1(g) = -d1(i)
-                const R du = -qr[si * UPS + xy], dv = -qr[FS + si * UPS + xy];
-                qr[sg * UPS + xy] = du;
-                qr[FS + sg * UPS + xy] = dv;
-                qr[2 * FS + sg * UPS + xy] = (R)0;
-                sr[sg * UPS + xy] = ur[sg * UPS + xy] + du;
-                sr[FS + sg * UPS + xy] = ur[FS + sg * UPS + xy] + dv;
-                sr[2 * FS + sg * UPS + xy] = ur[2 * FS + sg * UPS + xy];
-            } else {
-                qr[sg * UPS + xy] = (R)2 * bcu - qr[si * UPS + xy];
-                qr[FS + sg * UPS + xy] = -qr[FS + si * UPS + xy];
-                qr[2 * FS + sg * UPS + xy] = (R)0;
-            }
+            qr[sg * UPS + xy] = (R)2 * bcu - qr[si * UPS + xy];
+            qr[FS + sg * UPS + xy] = -qr[FS + si * UPS + xy];
+            qr[2 * FS + sg * UPS + xy] = (R)0;
         }
     };
 
@@ -240,40 +194,19 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
         // global loads first, so their latency overlaps the stencil
         const size_t g = (size_t)(i0 + tx) + (size_t)p.nx * (j0 + ty) + sk * kq;
         const double uc = __ldg(u + g), vc = __ldg(v + g), wc = __ldg(w + g);
-        double q0 = 0.0, qxp = 0.0, qyp = 0.0, qzp = 0.0;
-        if (MIXED && pinc) { // u_hat = u* - dt G p_pred (FP64): its divergence is the increment's residual
-            const int ip = (i0 + tx == p.nx - 1) ? 0 : i0 + tx + 1, jp = (j0 + ty == p.ny - 1) ? 0 : j0 + ty + 1;
-            const size_t pc = g - sk;
-            q0 = __ldg(pq + pc);
-            qxp = __ldg(pq + (size_t)ip + (size_t)p.nx * (j0 + ty) + sk * (kq - 1));
-            qyp = __ldg(pq + (size_t)(i0 + tx) + (size_t)p.nx * jp + sk * (kq - 1));
-            qzp = (kq < p.nz) ? __ldg(pq + pc + sk) : q0;
-        }
         R ru, rv, rw;
         {
             const int xy = (ty + 2) * UW + tx + 2;
             const int om = sm * UPS + xy, oc = s0 * UPS + xy, op = sp * UPS + xy;
-            const R *b = MIXED ? sr : qr;
+            const R *b = qr;
             momentum_rhs_c<R, CRF>(RingLoad3<R>{b + om, b + oc, b + op},
                                    RingLoad3<R>{b + FS + om, b + FS + oc, b + FS + op},
                                    RingLoad3<R>{b + 2 * FS + om, b + 2 * FS + oc, b + 2 * FS + op}, RingNbC{}, cst, ru,
                                    rv, rw);
         }
-        double nu, nv, nw;
-        if (MIXED) {
-            nu = ((uc + (double)qr[n.c]) + (double)(dt * ru) + uc) * 0.5;
-            nv = ((vc + (double)qr[FS + n.c]) + (double)(dt * rv) + vc) * 0.5;
-            nw = ((wc + (double)qr[2 * FS + n.c]) + (double)(dt * rw) + wc) * 0.5;
-            if (pinc) {
-                nu = nu - (qxp - q0) * (p.dt * p.dx_inv);
-                nv = nv - (qyp - q0) * (p.dt * p.dy_inv);
-                nw = nw - (qzp - q0) * p.dt * __ldg(m.dzc_inv + kq);
-            }
-        } else {
-            nu = ((double)qr[n.c] + p.dt * ((double)ru + p.fb[0]) + uc) * 0.5;
-            nv = ((double)qr[FS + n.c] + p.dt * ((double)rv + p.fb[1]) + vc) * 0.5;
-            nw = ((double)qr[2 * FS + n.c] + p.dt * ((double)rw + p.fb[2]) + wc) * 0.5;
-        }
+        const double nu = ((double)qr[n.c] + p.dt * ((double)ru + p.fb[0]) + uc) * 0.5;
+        const double nv = ((double)qr[FS + n.c] + p.dt * ((double)rv + p.fb[1]) + vc) * 0.5;
+        const double nw = ((double)qr[2 * FS + n.c] + p.dt * ((double)rw + p.fb[2]) + wc) * 0.5;
         uo[g] = nu;
         vo[g] = nv;
         if (kq != p.nz) wo[g] = nw;
@@ -294,17 +227,18 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
     RhsConst<R> cur = rhs_const<R>(p, m, mstart), prev = cur; // prev is unused until mq = mstart + 1
     // ring slots of the planes mq-1, mq, mq+1, rotated once per plane
     int sa = (mstart - 1) % NS, sb = mstart % NS, sc = (mstart + 1) % NS;
-    load_u_plane(mstart - 1, sa);
-    load_u_plane(mstart, sb);
-    load_u_plane(mstart + 1, sc);
+    load_u_plane_async(mstart - 1, sa);
+    load_u_plane_async(mstart, sb);
+    load_u_plane_async(mstart + 1, sc);
+    cp_async_wait<0>();
     __syncthreads();
     for (int mq = mstart; mq <= mend; mq++) {
         produce(mq, sa, sb, sc, cur);
         __syncthreads();
         const bool next = mq + 2 <= mend + 1;
-        // FP64: the copy of u plane mq+2 into the slot of plane mq-1 (which
+        // the copy of u plane mq+2 into the slot of plane mq-1 (which
         // nothing reads after produce(mq)) overlaps stage 2
-        if (!MIXED && next) load_u_plane_async(mq + 2, sa);
+        if (next) load_u_plane_async(mq + 2, sa);
         if (mq == 1) {
             wall(0, 1);
             __syncthreads();
@@ -319,8 +253,7 @@ __global__ void __launch_bounds__(FX *FY, MIXED ? 4 : 3) k_rk_fused(const double
             __syncthreads();
             if (p.nz >= kbeg && p.nz <= kend) stage2(p.nz, sa, sb, sc, cur);
         }
-        if (MIXED && next) load_u_plane(mq + 2, sa); // (mq + 2) % 3 == (mq - 1) % 3
-        if (!MIXED && next) cp_async_wait<0>();
+        if (next) cp_async_wait<0>(); // (mq + 2) % 3 == (mq - 1) % 3
         if (mq < mend) { // constants of plane mq + 1 <= nz: indices up to mq + 2 <= nz + 1
             prev = cur;
             cur.dzf_km = cur.dzf_k;
@@ -371,19 +304,16 @@ static int sm_count_rk()
     return n;
 }
 
-template <bool MIXED>
-static int launch_rk_fused_t(const double *u, const double *v, const double *w, double *uo, double *vo, double *wo,
-                             const StepParams &p, const MeshDev &m, MeanState &ms, cudaStream_t st,
-                             const double *pq = nullptr, int pinc = 0)
+int launch_rk_fused_fp64(const double *u, const double *v, const double *w, double *uo, double *vo, double *wo,
+                         const StepParams &p, const MeshDev &m, MeanState &ms, cudaStream_t st)
 {
     if (!rk_fused_supported(p)) {
         set_error("fused RK kernel needs nx % 32 == 0 and ny % 8 == 0");
         return -1;
     }
-    using R = typename RkTraits<MIXED>::R;
-    const size_t shm = sizeof(R) * (MIXED ? 9 : 6) * RkTraits<MIXED>::NS * UPS;
+    const size_t shm = sizeof(double) * 6 * NS * UPS;
     // u_crf == 0 (the channel's usual frame) drops the frame-velocity terms
-    auto kern = (p.u_crf != 0.0) ? k_rk_fused<MIXED, true> : k_rk_fused<MIXED, false>;
+    auto kern = (p.u_crf != 0.0) ? k_rk_fused<true> : k_rk_fused<false>;
     PL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
     // prefer the largest shared-memory carve-out: several CTAs per SM
     PL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
@@ -399,22 +329,9 @@ static int launch_rk_fused_t(const double *u, const double *v, const double *w, 
         return -1;
     }
     MeanRed r{ms.partial, ms.counter, ms.scalar, (double)p.nx, (double)p.ny, ms.vel_force};
-    kern<<<grid, dim3(FX, FY), shm, st>>>(u, v, w, uo, vo, wo, p, m, r, kchunk, pq, pinc);
+    kern<<<grid, dim3(FX, FY), shm, st>>>(u, v, w, uo, vo, wo, p, m, r, kchunk);
     PL_CHECK_LAUNCH();
     return 0;
-}
-
-int launch_rk_fused_fp64(const double *u, const double *v, const double *w, double *uo, double *vo, double *wo,
-                         const StepParams &p, const MeshDev &m, MeanState &ms, cudaStream_t st)
-{
-    return launch_rk_fused_t<false>(u, v, w, uo, vo, wo, p, m, ms, st);
-}
-
-int launch_rk_fused_mixed(const double *u, const double *v, const double *w, double *uo, double *vo, double *wo,
-                          const StepParams &p, const MeshDev &m, MeanState &ms, const double *pq, int pinc,
-                          cudaStream_t st)
-{
-    return launch_rk_fused_t<true>(u, v, w, uo, vo, wo, p, m, ms, st, pq, pinc);
 }
 
 } // namespace pl

@@ -1,0 +1,685 @@
+// rk_mixed.cu -- the mixed-precision path's fused RK2 kernel: both stages of
+// timeIntVelRK1 / timeIntVelRK2 (mod_calcVel.f90:52-146, 240-334) with their
+// wall fills, in FP32 flux form.
+//
+// 2.5D blocking as in the FP64 kernel (rk_fused.cu), on a 32 x 16 tile of
+// (i, j) whose 256 threads own two y-adjacent points each: a CTA marches up a
+// chunk of k-planes; shared-memory rings hold
+// the last three planes of u, v, w (FP32, halo 2) and of the stage-1 field
+// u1 = u + d1 (FP32, halo 1); HBM sees u, v, w read once, the new fields
+// written once and the FP32 pressure prediction read once.  The FP64 planes
+// arrive through a three-slot staging ring filled by cp.async two planes
+// ahead of their conversion to FP32, and each thread converts only the
+// points it copied itself, so no load latency and no extra barrier sits on
+// the march's critical path; the stage-2 centre values of the next plane are
+// loaded into registers before stage 1, so their latency hides behind it.
+//
+// The arithmetic is the reference's stencil rearranged into fluxes, which
+// the FP64 path (the parity path) does not do:
+//   * every convective edge product is formed once per point and serves the
+//     two equations that share the edge: (u_c + u_yp)(v_c + v_xp) is the
+//     north flux of u and the east flux of v (:84 un*vn, :107 ue*ve); the
+//     u-to-w-face interpolation times (w_c + w_xp) is the top flux of u and
+//     the east flux of w (:85 ut*wt, :129 ue*we); likewise v and w;
+//   * the top fluxes of plane k are the bottom fluxes of plane k+1, so they
+//     ride in registers up the march instead of being recomputed;
+//   * (q_c + q_xp)^2 - (q_xm + q_c)^2 = (q_xp - q_xm)(q_xp + q_xm + 2 q_c), and
+//     the viscous terms are one five-point combination per direction with
+//     dt, 0.25, 1/Re and the mesh factors folded into per-plane coefficients;
+//   * each thread evaluates its two points together: 41 shared-memory loads
+//     instead of 50, and the upper point's south fluxes are the lower
+//     point's north fluxes;
+//   * the stage-1 increment d1 = dt RHS(u) of the tile's own points stays in
+//     the thread's registers from stage 1 of plane k to stage 2 of plane k
+//     (the thread that forms it consumes it), so only u1 goes through
+//     shared memory.
+// About 70 FP32 operations and 25 shared-memory loads per stencil
+// evaluation, against about 135 and 27 for the reference's form.
+//
+// Stage 2 forms u_hat = u + [ (d1 + d2)/2 - dt G p_pred ] with the bracket in
+// FP32 and the sum in FP64: u, v, w stay FP64, and the projection residual of
+// the increment solve is the FP64 divergence of the stored u_hat, whatever
+// rounding the bracket carries.
+#include <vector>
+
+#include "fft.cuh" // cp.async helpers
+#include "stencil.cuh"
+#include "stencil_rhs.cuh"
+
+namespace pl {
+
+namespace {
+
+constexpr int MX = 32, MY = 16;         // tile; each thread owns the points (x, 2t) and (x, 2t+1)
+constexpr int MW = MX + 4, MH = MY + 4; // ring plane with a halo of 2
+constexpr int MPS = MW * MH;            // 720 values per plane
+constexpr int MNS = 3;                  // planes per ring
+constexpr int MFS = MNS * MPS;          // ring size per field
+constexpr int MT = 256;                 // threads
+constexpr int MX_KCHUNK = 80;           // longest z-chunk (planes)
+
+// rolling top fluxes of one point: E_uw(k+1/2), E_vw(k+1/2) and (w_k + w_{k+1})^2
+struct Carry {
+    float euw, evw, cw;
+};
+
+// the top fluxes of plane k at one point from the planes k (oc) and k+1 (op)
+// of a ring (u, v, w at R, R + MFS, R + 2 MFS); a, b: plane k's weights of
+// the face interpolation q_{k+1/2} = q_k a + q_{k+1} b
+__device__ __forceinline__ Carry mx_top(const float *R, int oc, int op, float a, float b)
+{
+    const float *u = R, *v = R + MFS, *w = R + 2 * MFS;
+    Carry c;
+    const float wc = w[oc];
+    c.euw = (u[oc] * a + u[op] * b) * (wc + w[oc + 1]);
+    c.evw = (v[oc] * a + v[op] * b) * (wc + w[oc + MW]);
+    const float wt = wc + w[op];
+    c.cw = wt * wt;
+    return c;
+}
+
+// dt * (momentum right-hand side) at one point from the planes k-1 (om), k
+// (oc), k+1 (op) of a ring; cy holds the bottom fluxes on entry and the top
+// fluxes on return.  Plane coefficients (dt folded in, MxPlane): a, b face
+// weights; hzuv = dt/4 dzf_inv(k); azp, azm = dt/Re dzf_inv(k) dzc_inv(k),
+// dzc_inv(k-1); ccuv = 2 cxx + 2 cyy + azp + azm; hzw = dt/4 dzc_inv(k);
+// bzp, bzm = dt/Re dzc_inv(k) dzf_inv(k+1), dzf_inv(k); ccw likewise.
+template <bool CRF>
+__device__ __forceinline__ void mx_rhs(const float *R, int om, int oc, int op, const MxPlane &P, const MxConst &K,
+                                       Carry &cy, float &du, float &dv, float &dw)
+{
+    const float *u = R, *v = R + MFS, *w = R + 2 * MFS;
+    const float uc = u[oc], uxp = u[oc + 1], uxm = u[oc - 1], uyp = u[oc + MW], uym = u[oc - MW];
+    const float uzp = u[op], uzm = u[om], uxmyp = u[oc - 1 + MW], uxmzp = u[op - 1];
+    const float vc = v[oc], vxp = v[oc + 1], vxm = v[oc - 1], vyp = v[oc + MW], vym = v[oc - MW];
+    const float vzp = v[op], vzm = v[om], vxpym = v[oc + 1 - MW], vymzp = v[op - MW];
+    const float wc = w[oc], wxp = w[oc + 1], wxm = w[oc - 1], wyp = w[oc + MW], wym = w[oc - MW];
+    const float wzp = w[op], wzm = w[om];
+
+    // edge fluxes (products of face sums), each shared by two equations
+    const float euv_n = (uc + uyp) * (vc + vxp);                // (i+1/2, j+1/2): u north, v east
+    const float euv_s = (uym + uc) * (vym + vxpym);             // (i+1/2, j-1/2): u south
+    const float euv_w = (uxm + uxmyp) * (vxm + vc);             // (i-1/2, j+1/2): v west
+    const float euw_t = (uc * P.a + uzp * P.b) * (wc + wxp);    // (i+1/2, k+1/2): u top, w east
+    const float euw_w = (uxm * P.a + uxmzp * P.b) * (wxm + wc); // (i-1/2, k+1/2): w west
+    const float evw_t = (vc * P.a + vzp * P.b) * (wc + wyp);    // (j+1/2, k+1/2): v top, w north
+    const float evw_s = (vym * P.a + vymzp * P.b) * (wym + wc); // (j-1/2, k+1/2): w south
+    const float wt = wc + wzp;
+    const float cw_t = wt * wt;
+
+    // u: x self-flux difference (u_xp - u_xm)(u_xp + u_xm + 2 u_c)
+    const float sxu = uxp + uxm, syu = uyp + uym, dxu = uxp - uxm;
+    float r = K.cxx * sxu;
+    r = fmaf(K.cyy, syu, r);
+    r = fmaf(P.azp, uzp, r);
+    r = fmaf(P.azm, uzm, r);
+    r = fmaf(-P.ccuv, uc, r);
+    r = fmaf(-K.hx, dxu * fmaf(2.f, uc, sxu), r);
+    r = fmaf(-K.hy, euv_n - euv_s, r);
+    r = fmaf(-P.hzuv, euw_t - cy.euw, r);
+    if (CRF) r = fmaf(-K.ucx, dxu, r);
+    du = r;
+
+    // v: y self-flux difference
+    const float sxv = vxp + vxm, syv = vyp + vym, dyv = vyp - vym;
+    r = K.cxx * sxv;
+    r = fmaf(K.cyy, syv, r);
+    r = fmaf(P.azp, vzp, r);
+    r = fmaf(P.azm, vzm, r);
+    r = fmaf(-P.ccuv, vc, r);
+    r = fmaf(-K.hx, euv_n - euv_w, r);
+    r = fmaf(-K.hy, dyv * fmaf(2.f, vc, syv), r);
+    r = fmaf(-P.hzuv, evw_t - cy.evw, r);
+    if (CRF) r = fmaf(-K.ucx, vxp - vxm, r);
+    dv = r;
+
+    // w: z self-flux from the carried bottom square
+    const float sxw = wxp + wxm, syw = wyp + wym;
+    r = K.cxx * sxw;
+    r = fmaf(K.cyy, syw, r);
+    r = fmaf(P.bzp, wzp, r);
+    r = fmaf(P.bzm, wzm, r);
+    r = fmaf(-P.ccw, wc, r);
+    r = fmaf(-K.hx, euw_t - euw_w, r);
+    r = fmaf(-K.hy, evw_t - evw_s, r);
+    r = fmaf(-P.hzw, cw_t - cy.cw, r);
+    if (CRF) r = fmaf(-K.ucx, wxp - wxm, r);
+    dw = r;
+
+    cy.euw = euw_t;
+    cy.evw = evw_t;
+    cy.cw = cw_t;
+}
+
+// plane k's coefficients from the chunk's copy in shared memory (tab points
+// at the first plane of the chunk's copy, k relative to it)
+__device__ __forceinline__ MxPlane mx_plane(const float4 *tab, int k)
+{
+    const float4 x = tab[3 * k], y = tab[3 * k + 1], z = tab[3 * k + 2];
+    MxPlane P;
+    P.a = x.x;
+    P.b = x.y;
+    P.hzuv = x.z;
+    P.azp = x.w;
+    P.azm = y.x;
+    P.ccuv = y.y;
+    P.hzw = y.z;
+    P.bzp = y.w;
+    P.bzm = z.x;
+    P.ccw = z.y;
+    P.gz = z.z;
+    return P;
+}
+
+
+// dt * (momentum right-hand side) at the points A (oc) and B = A + y (oc + MW)
+// of a ring, sharing their loads and the edge products of their common face:
+// A's north fluxes are B's south fluxes.  cA, cB: the carried bottom fluxes
+// of A and B (top fluxes on return).
+template <bool CRF>
+__device__ __forceinline__ void mx_rhs2(const float *R, int om, int oc, int op, const MxPlane &P, const MxConst &K,
+                                        Carry &cA, Carry &cB, float &duA, float &dvA, float &dwA, float &duB,
+                                        float &dvB, float &dwB)
+{
+    const float *u = R, *v = R + MFS, *w = R + 2 * MFS;
+    // u: the centre column y-1 .. y+2, the +x and -x columns, the planes above and below
+    const float uym = u[oc - MW], uA = u[oc], uB = u[oc + MW], uyp2 = u[oc + 2 * MW];
+    const float uxpA = u[oc + 1], uxpB = u[oc + 1 + MW];
+    const float uxmA = u[oc - 1], uxmB = u[oc - 1 + MW], uxm2 = u[oc - 1 + 2 * MW];
+    const float uzpA = u[op], uzpB = u[op + MW], uzmA = u[om], uzmB = u[om + MW];
+    const float uxmzpA = u[op - 1], uxmzpB = u[op - 1 + MW];
+    const float vym = v[oc - MW], vA = v[oc], vB = v[oc + MW], vyp2 = v[oc + 2 * MW];
+    const float vxpym = v[oc + 1 - MW], vxpA = v[oc + 1], vxpB = v[oc + 1 + MW];
+    const float vxmA = v[oc - 1], vxmB = v[oc - 1 + MW];
+    const float vzpA = v[op], vzpB = v[op + MW], vzmA = v[om], vzmB = v[om + MW];
+    const float vymzp = v[op - MW];
+    const float wym = w[oc - MW], wA = w[oc], wB = w[oc + MW], wyp2 = w[oc + 2 * MW];
+    const float wxpA = w[oc + 1], wxpB = w[oc + 1 + MW], wxmA = w[oc - 1], wxmB = w[oc - 1 + MW];
+    const float wzpA = w[op], wzpB = w[op + MW], wzmA = w[om], wzmB = w[om + MW];
+
+    // edge fluxes
+    const float euv_nA = (uA + uB) * (vA + vxpA); // = south flux of B
+    const float euv_nB = (uB + uyp2) * (vB + vxpB);
+    const float euv_sA = (uym + uA) * (vym + vxpym);
+    const float euv_wA = (uxmA + uxmB) * (vxmA + vA);
+    const float euv_wB = (uxmB + uxm2) * (vxmB + vB);
+    const float euw_tA = (uA * P.a + uzpA * P.b) * (wA + wxpA);
+    const float euw_tB = (uB * P.a + uzpB * P.b) * (wB + wxpB);
+    const float euw_wA = (uxmA * P.a + uxmzpA * P.b) * (wxmA + wA);
+    const float euw_wB = (uxmB * P.a + uxmzpB * P.b) * (wxmB + wB);
+    const float evw_tA = (vA * P.a + vzpA * P.b) * (wA + wB); // = south flux of B
+    const float evw_tB = (vB * P.a + vzpB * P.b) * (wB + wyp2);
+    const float evw_sA = (vym * P.a + vymzp * P.b) * (wym + wA);
+    const float wtA = wA + wzpA, wtB = wB + wzpB;
+    const float cw_tA = wtA * wtA, cw_tB = wtB * wtB;
+
+    float r;
+    // u at A and B
+    {
+        const float sx = uxpA + uxmA, sy = uB + uym, dx = uxpA - uxmA;
+        r = K.cxx * sx;
+        r = fmaf(K.cyy, sy, r);
+        r = fmaf(P.azp, uzpA, r);
+        r = fmaf(P.azm, uzmA, r);
+        r = fmaf(-P.ccuv, uA, r);
+        r = fmaf(-K.hx, dx * fmaf(2.f, uA, sx), r);
+        r = fmaf(-K.hy, euv_nA - euv_sA, r);
+        r = fmaf(-P.hzuv, euw_tA - cA.euw, r);
+        if (CRF) r = fmaf(-K.ucx, dx, r);
+        duA = r;
+    }
+    {
+        const float sx = uxpB + uxmB, sy = uyp2 + uA, dx = uxpB - uxmB;
+        r = K.cxx * sx;
+        r = fmaf(K.cyy, sy, r);
+        r = fmaf(P.azp, uzpB, r);
+        r = fmaf(P.azm, uzmB, r);
+        r = fmaf(-P.ccuv, uB, r);
+        r = fmaf(-K.hx, dx * fmaf(2.f, uB, sx), r);
+        r = fmaf(-K.hy, euv_nB - euv_nA, r);
+        r = fmaf(-P.hzuv, euw_tB - cB.euw, r);
+        if (CRF) r = fmaf(-K.ucx, dx, r);
+        duB = r;
+    }
+    // v at A and B
+    {
+        const float sx = vxpA + vxmA, sy = vB + vym, dy = vB - vym;
+        r = K.cxx * sx;
+        r = fmaf(K.cyy, sy, r);
+        r = fmaf(P.azp, vzpA, r);
+        r = fmaf(P.azm, vzmA, r);
+        r = fmaf(-P.ccuv, vA, r);
+        r = fmaf(-K.hx, euv_nA - euv_wA, r);
+        r = fmaf(-K.hy, dy * fmaf(2.f, vA, sy), r);
+        r = fmaf(-P.hzuv, evw_tA - cA.evw, r);
+        if (CRF) r = fmaf(-K.ucx, vxpA - vxmA, r);
+        dvA = r;
+    }
+    {
+        const float sx = vxpB + vxmB, sy = vyp2 + vA, dy = vyp2 - vA;
+        r = K.cxx * sx;
+        r = fmaf(K.cyy, sy, r);
+        r = fmaf(P.azp, vzpB, r);
+        r = fmaf(P.azm, vzmB, r);
+        r = fmaf(-P.ccuv, vB, r);
+        r = fmaf(-K.hx, euv_nB - euv_wB, r);
+        r = fmaf(-K.hy, dy * fmaf(2.f, vB, sy), r);
+        r = fmaf(-P.hzuv, evw_tB - cB.evw, r);
+        if (CRF) r = fmaf(-K.ucx, vxpB - vxmB, r);
+        dvB = r;
+    }
+    // w at A and B
+    {
+        const float sx = wxpA + wxmA, sy = wB + wym;
+        r = K.cxx * sx;
+        r = fmaf(K.cyy, sy, r);
+        r = fmaf(P.bzp, wzpA, r);
+        r = fmaf(P.bzm, wzmA, r);
+        r = fmaf(-P.ccw, wA, r);
+        r = fmaf(-K.hx, euw_tA - euw_wA, r);
+        r = fmaf(-K.hy, evw_tA - evw_sA, r);
+        r = fmaf(-P.hzw, cw_tA - cA.cw, r);
+        if (CRF) r = fmaf(-K.ucx, wxpA - wxmA, r);
+        dwA = r;
+    }
+    {
+        const float sx = wxpB + wxmB, sy = wyp2 + wA;
+        r = K.cxx * sx;
+        r = fmaf(K.cyy, sy, r);
+        r = fmaf(P.bzp, wzpB, r);
+        r = fmaf(P.bzm, wzmB, r);
+        r = fmaf(-P.ccw, wB, r);
+        r = fmaf(-K.hx, euw_tB - euw_wB, r);
+        r = fmaf(-K.hy, evw_tB - evw_tA, r);
+        r = fmaf(-P.hzw, cw_tB - cB.cw, r);
+        if (CRF) r = fmaf(-K.ucx, wxpB - wxmB, r);
+        dwB = r;
+    }
+    cA.euw = euw_tA;
+    cA.evw = evw_tA;
+    cA.cw = cw_tA;
+    cB.euw = euw_tB;
+    cB.evw = evw_tB;
+    cB.cw = cw_tB;
+}
+} // namespace
+
+template <bool CRF>
+__global__ void __launch_bounds__(MT, 2) k_rk_mixed(const double *__restrict__ u, const double *__restrict__ v,
+                                                   const double *__restrict__ w, double *__restrict__ uo,
+                                                   double *__restrict__ vo, double *__restrict__ wo, StepParams p,
+                                                   MeshDev m, const float4 *__restrict__ tab, MxConst K, MeanRed red,
+                                                   int kchunk, const float *__restrict__ pq, int pinc)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *stg = reinterpret_cast<double *>(smem_raw);      // FP64 staging: plane k in slot k % 3, [slot][field][MPS]
+    float *ur = reinterpret_cast<float *>(stg + 3 * 3 * MPS); // u, v, w rings
+    float *sr = ur + 3 * MFS;                                 // u1 = u + d1 rings
+    // the chunk's plane coefficients (planes kbeg - 2 .. kbeg + kchunk + 1,
+    // 3 float4 each) and dzf/lz: used every plane, so they live on chip
+    // instead of in global loads whose latency would sit on the march
+    float4 *ptab = reinterpret_cast<float4 *>(sr + 3 * MFS);
+    double *pzl = reinterpret_cast<double *>(ptab + 3 * (kchunk + 4));
+    const int lane = threadIdx.x, wid = threadIdx.y;
+    const int i0 = blockIdx.x * MX, j0 = blockIdx.y * MY;
+    const int kbeg = blockIdx.z * kchunk + 1, kend = min(kbeg + kchunk - 1, p.nz);
+    const size_t sk = (size_t)p.nx * p.ny;
+
+    // ring-plane loads (36 x 20): slot 0 = x 2..33 of rows 0..7 (warp = row),
+    // slot 1 = rows 8..15, slot 2 = rows 16..19 (warps 0-3) and x 0, 1, 34,
+    // 35 of rows 0..19 (warps 4, 5 and half of warp 6: 80 points).  Whole
+    // 32-value row segments per warp: coalesced loads, conflict-free stores.
+    static_assert(MX == 32 && MY == 16 && MW == 36 && MH == 20, "slot maps of the 32 x 16 tile");
+    int loff[3], lxy[3];
+    const bool lval2 = wid < 6 || (wid == 6 && lane < 16);
+    {
+        int lx[3], ly[3];
+        lx[0] = lx[1] = 2 + lane;
+        ly[0] = wid;
+        ly[1] = 8 + wid;
+        if (wid < 4) {
+            lx[2] = 2 + lane;
+            ly[2] = 16 + wid;
+        } else {
+            const int e = (wid - 4) * 32 + lane, c = e % 4; // e < 80 on the valid lanes
+            lx[2] = c < 2 ? c : 32 + c;
+            ly[2] = min(e / 4, MH - 1);
+        }
+#pragma unroll
+        for (int sl = 0; sl < 3; sl++) {
+            int gi = i0 - 2 + lx[sl], gj = j0 - 2 + ly[sl];
+            gi += (gi < 0) ? p.nx : 0;
+            gi -= (gi >= p.nx) ? p.nx : 0;
+            gj += (gj < 0) ? p.ny : 0;
+            gj -= (gj >= p.ny) ? p.ny : 0;
+            loff[sl] = gi + p.nx * gj;
+            lxy[sl] = ly[sl] * MW + lx[sl];
+        }
+    }
+    // copy plane kq (in [0, nz+1]; none past last) into its staging slot; one
+    // commit group per call, empty or not, so the wait counts stay uniform
+    auto issue = [&](int kq, int last) {
+        if (kq <= last) {
+            const size_t gk = sk * kq;
+            double *d = stg + (kq % 3) * 3 * MPS;
+#pragma unroll
+            for (int sl = 0; sl < 3; sl++) {
+                if (sl < 2 || lval2) {
+                    const size_t g = gk + loff[sl];
+                    cp_async_8(d + lxy[sl], u + g);
+                    cp_async_8(d + MPS + lxy[sl], v + g);
+                    cp_async_8(d + 2 * MPS + lxy[sl], w + g);
+                }
+            }
+        }
+        cp_async_commit();
+    };
+    // this thread's staged points of plane kq -> FP32 ring slot s
+    auto convert = [&](int kq, int s) {
+        const double *d = stg + (kq % 3) * 3 * MPS;
+#pragma unroll
+        for (int sl = 0; sl < 3; sl++) {
+            if (sl < 2 || lval2) {
+                const int q = s * MPS + lxy[sl];
+                ur[0 * MFS + q] = (float)d[lxy[sl]];
+                ur[1 * MFS + q] = (float)d[MPS + lxy[sl]];
+                ur[2 * MFS + q] = (float)d[2 * MPS + lxy[sl]];
+            }
+        }
+    };
+
+    // stage-1 points (halo-1 region, x 1..34, y 1..18 of the ring plane):
+    // the pair = the thread's own points (x 2 + lane, y 2 + 2 wid and the row
+    // above: its stage-2 points); the halo = rows 1 and 18 (warps 0, 1) and
+    // columns 1, 34 of rows 1..18 (warp 2 and 4 lanes of warp 3)
+    const int hxy0 = (2 + 2 * wid) * MW + 2 + lane;
+    int hxy1;
+    if (wid < 2) {
+        hxy1 = (wid == 0 ? 1 : 18) * MW + 2 + lane;
+    } else {
+        const int e = (wid - 2) * 32 + lane; // < 36 on the valid lanes
+        hxy1 = (1 + e % 18) * MW + (e < 18 ? 1 : 34);
+    }
+    const bool hval1 = wid < 3 || (wid == 3 && lane < 4);
+
+    // the global points of the thread's stage-2 pair and their
+    // pressure-prediction neighbours (+x, +y periodic)
+    const int gi = i0 + lane, gjA = j0 + 2 * wid;
+    const int gxp = (gi == p.nx - 1) ? 0 : gi + 1, gjB2 = (gjA + 2 >= p.ny) ? gjA + 2 - p.ny : gjA + 2;
+    const size_t gA = (size_t)gi + (size_t)p.nx * gjA;
+
+    const int mstart = max(kbeg - 1, 1), mend = min(kend + 1, p.nz);
+    const int last = mend + 1; // the last u plane the march reads
+    int sa = (mstart - 1) % MNS, sb = mstart % MNS, sc = (mstart + 1) % MNS;
+    {
+        const int k0 = max(kbeg - 2, 0), np = min(kbeg + kchunk + 1, p.nz + 1) - k0 + 1;
+        const int t = threadIdx.x + MX * threadIdx.y;
+        for (int q = t; q < 3 * np; q += MT) ptab[q] = __ldg(tab + 3 * k0 + q);
+        for (int q = t; q < np; q += MT) pzl[q] = __ldg(m.dzflzi + k0 + q);
+        ptab -= 3 * k0; // indexable by the global plane
+        pzl -= k0;
+    }
+    issue(mstart - 1, last);
+    issue(mstart, last);
+    issue(mstart + 1, last);
+    cp_async_wait<0>();
+    convert(mstart - 1, sa);
+    convert(mstart, sb);
+    convert(mstart + 1, sc);
+    issue(mstart + 2, last); // into the slots of mstart - 1 and mstart, converted above
+    issue(mstart + 3, last);
+    __syncthreads();
+
+    // bottom fluxes of the first stage-1 plane (the top fluxes of mstart - 1)
+    const Carry zero = {0.f, 0.f, 0.f};
+    Carry cA, cB, cH, c2A = zero, c2B = zero;
+    {
+        const MxPlane Pm = mx_plane(ptab, mstart - 1);
+        cA = mx_top(ur, sa * MPS + hxy0, sb * MPS + hxy0, Pm.a, Pm.b);
+        cB = mx_top(ur, sa * MPS + hxy0 + MW, sb * MPS + hxy0 + MW, Pm.a, Pm.b);
+        cH = hval1 ? mx_top(ur, sa * MPS + hxy1, sb * MPS + hxy1, Pm.a, Pm.b) : zero;
+    }
+    // d1 of the own pair at plane mq (this iteration) and at mq - 1
+    float d1[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, e1[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    bool first2 = true;
+    double su = 0.0;
+    const float bcu2 = (float)(2.0 * (0.0 - p.u_crf));
+
+    // the stage-2 centre values of the pair at plane kq: u, v, w (FP64) and
+    // the pressure prediction at A, B and their +x, +y, +z neighbours (A's +y
+    // neighbour is B)
+    struct Centre {
+        double u[2], v[2], w[2];
+        float qA, qB, qxA, qxB, qyB, qzA, qzB;
+    };
+    auto centre = [&](int kq) {
+        Centre c;
+        const size_t g = gA + sk * kq;
+        c.u[0] = __ldg(u + g);
+        c.u[1] = __ldg(u + g + p.nx);
+        c.v[0] = __ldg(v + g);
+        c.v[1] = __ldg(v + g + p.nx);
+        c.w[0] = __ldg(w + g);
+        c.w[1] = __ldg(w + g + p.nx);
+        c.qA = c.qB = c.qxA = c.qxB = c.qyB = c.qzA = c.qzB = 0.f;
+        if (pinc) {
+            const size_t pl = sk * (kq - 1);
+            const size_t rowA = (size_t)p.nx * gjA + pl, rowB = rowA + p.nx;
+            c.qA = __ldg(pq + rowA + gi);
+            c.qB = __ldg(pq + rowB + gi);
+            c.qxA = __ldg(pq + rowA + gxp);
+            c.qxB = __ldg(pq + rowB + gxp);
+            c.qyB = __ldg(pq + (size_t)p.nx * gjB2 + pl + gi);
+            c.qzA = (kq < p.nz) ? __ldg(pq + rowA + sk + gi) : c.qA;
+            c.qzB = (kq < p.nz) ? __ldg(pq + rowB + sk + gi) : c.qB;
+        }
+        return c;
+    };
+
+    // stage 2 at interior plane kq from the stage-1 planes kq-1 (sm), kq (s0),
+    // kq+1 (sp); e: the pair's d1 at kq (uA, vA, wA, uB, vB, wB)
+    auto stage2 = [&](int kq, int sm, int s0, int sp, const float *e, const Centre &cv) {
+        const MxPlane P = mx_plane(ptab, kq);
+        if (first2) { // bottom fluxes of u1 at kq: the top fluxes of plane kq - 1
+            const MxPlane Pm = mx_plane(ptab, kq - 1);
+            c2A = mx_top(sr, sm * MPS + hxy0, s0 * MPS + hxy0, Pm.a, Pm.b);
+            c2B = mx_top(sr, sm * MPS + hxy0 + MW, s0 * MPS + hxy0 + MW, Pm.a, Pm.b);
+            first2 = false;
+        }
+        float d[6];
+        mx_rhs2<CRF>(sr, sm * MPS + hxy0, s0 * MPS + hxy0, sp * MPS + hxy0, P, K, c2A, c2B, d[0], d[1], d[2], d[3],
+                     d[4], d[5]);
+        float iu[2], iv[2], iw[2];
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            iu[q] = 0.5f * (e[3 * q] + d[3 * q]);
+            iv[q] = 0.5f * (e[3 * q + 1] + d[3 * q + 1]);
+            iw[q] = 0.5f * (e[3 * q + 2] + d[3 * q + 2]);
+        }
+        if (pinc) {
+            iu[0] = fmaf(-K.gx, cv.qxA - cv.qA, iu[0]);
+            iu[1] = fmaf(-K.gx, cv.qxB - cv.qB, iu[1]);
+            iv[0] = fmaf(-K.gy, cv.qB - cv.qA, iv[0]);
+            iv[1] = fmaf(-K.gy, cv.qyB - cv.qB, iv[1]);
+            iw[0] = fmaf(-P.gz, cv.qzA - cv.qA, iw[0]);
+            iw[1] = fmaf(-P.gz, cv.qzB - cv.qB, iw[1]);
+        }
+        const size_t g = gA + sk * kq;
+        const double zl = pzl[kq];
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            const size_t gq = g + (size_t)q * p.nx;
+            const double nu = cv.u[q] + (double)iu[q], nv = cv.v[q] + (double)iv[q], nw = cv.w[q] + (double)iw[q];
+            uo[gq] = nu;
+            vo[gq] = nv;
+            if (kq != p.nz) wo[gq] = nw;
+            wall_fill<double>(uo, vo, wo, gq, kq, sk, p.nz, 0.0 - p.u_crf, nu, nv);
+            su += nu * zl;
+        }
+    };
+
+    // u1 = u + d1 at ring offset o (FP32), and its wall image at plane 0
+    auto put1 = [&](int s, int sw, int xy, float du, float dv, float dw, bool bottom) {
+        const float a = ur[s * MPS + xy] + du, b = ur[MFS + s * MPS + xy] + dv;
+        sr[s * MPS + xy] = a;
+        sr[MFS + s * MPS + xy] = b;
+        sr[2 * MFS + s * MPS + xy] = ur[2 * MFS + s * MPS + xy] + dw;
+        if (bottom) { // imposeNoSlipBC on u1: u1(0) = 2bc - u1(1), v1(0) = -v1(1), w1(0) = 0
+            sr[sw * MPS + xy] = bcu2 - a;
+            sr[MFS + sw * MPS + xy] = -b;
+            sr[2 * MFS + sw * MPS + xy] = 0.f;
+        }
+    };
+    // the top wall plane of u1 at ring slot st from plane nz at slot sn
+    auto top1 = [&](int st, int sn, int xy) {
+        sr[st * MPS + xy] = bcu2 - sr[sn * MPS + xy];
+        sr[MFS + st * MPS + xy] = -sr[MFS + sn * MPS + xy];
+        sr[2 * MFS + st * MPS + xy] = 0.f;
+    };
+
+    // Two barriers per plane: stage 1 at plane mq reads u planes mq-1..mq+1
+    // and writes u1 plane mq; then stage 2 at mq-1 reads u1 planes mq-2..mq,
+    // and the staged u plane mq+2 is converted into the slot of plane mq-1.
+    for (int mq = mstart; mq <= mend; mq++) {
+        const bool do2 = (mq - 1 >= kbeg && mq - 1 <= kend);
+        Centre cv;
+        if (do2) cv = centre(mq - 1); // in flight during stage 1
+        {
+            const MxPlane P = mx_plane(ptab, mq);
+            const bool top = (mq == p.nz), bottom = (mq == 1);
+            mx_rhs2<CRF>(ur, sa * MPS + hxy0, sb * MPS + hxy0, sc * MPS + hxy0, P, K, cA, cB, d1[0], d1[1], d1[2],
+                         d1[3], d1[4], d1[5]);
+            if (top) d1[2] = d1[5] = 0.f; // w1(nz) = 0, the wall
+            put1(sb, sa, hxy0, d1[0], d1[1], d1[2], bottom);
+            put1(sb, sa, hxy0 + MW, d1[3], d1[4], d1[5], bottom);
+            if (hval1) {
+                float du, dv, dw;
+                mx_rhs<CRF>(ur, sa * MPS + hxy1, sb * MPS + hxy1, sc * MPS + hxy1, P, K, cH, du, dv, dw);
+                if (top) dw = 0.f;
+                put1(sb, sa, hxy1, du, dv, dw, bottom);
+            }
+        }
+        __syncthreads();
+        // plane mq-2 sits in slot sc
+        if (do2) stage2(mq - 1, sc, sa, sb, e1, cv);
+        if (mq == p.nz) {
+            // the top wall plane of u1 takes the slot of plane nz-2, which
+            // stage 2 at nz-1 has just consumed
+            __syncthreads();
+            top1(sc, sb, hxy0);
+            top1(sc, sb, hxy0 + MW);
+            if (hval1) top1(sc, sb, hxy1);
+            __syncthreads();
+            if (p.nz >= kbeg && p.nz <= kend) stage2(p.nz, sa, sb, sc, d1, centre(p.nz));
+        }
+        if (mq + 2 <= last) {
+            // plane mq+2 was issued two iterations ago; mq+3 may still be in
+            // flight.  Its FP32 slot is plane mq-1's ((mq + 2) % 3 == (mq - 1) % 3),
+            // which stage 1 above has finished with.
+            cp_async_wait<1>();
+            convert(mq + 2, sa);
+        }
+        issue(mq + 4, last); // into the staging slot of plane mq + 1, converted last iteration
+#pragma unroll
+        for (int q = 0; q < 6; q++) e1[q] = d1[q];
+        const int st = sa;
+        sa = sb;
+        sb = sc;
+        sc = st;
+        __syncthreads();
+    }
+    cp_async_wait<0>();
+    mean_reduce(su, red);
+}
+
+// z-chunks per tile column, as for the FP64 kernel: chunks of about 52
+// planes, more where tiles x chunks would not fill one wave of resident CTAs
+static int mx_chunks(const StepParams &p, long resident)
+{
+    const int tiles = (p.nx / MX) * (p.ny / MY);
+    const int maxch = p.nz / 16 > 1 ? p.nz / 16 : 1;
+    int nch = (p.nz + 26) / 52;
+    if (nch < 1) nch = 1;
+    while (nch < maxch && (long)tiles * nch < resident) nch++;
+    return nch < maxch ? nch : maxch;
+}
+
+std::vector<float> rk_mixed_table(const StepParams &p, const std::vector<double> &dzf,
+                                  const std::vector<double> &dzf_inv, const std::vector<double> &dzc_inv)
+{
+    const int nz = p.nz;
+    std::vector<float> t((size_t)(nz + 2) * 12, 0.f);
+    const double dt = p.dt, re = p.re_inv;
+    const double cxx = dt * re * p.dx_inv * p.dx_inv, cyy = dt * re * p.dy_inv * p.dy_inv;
+    for (int k = 0; k <= nz; k++) {
+        float *r = t.data() + (size_t)12 * k;
+        r[0] = (float)(dzf[k + 1] * dzc_inv[k]); // a
+        r[1] = (float)(dzf[k] * dzc_inv[k]);     // b
+        if (k == 0) continue;
+        const double azp = dt * re * dzf_inv[k] * dzc_inv[k], azm = dt * re * dzf_inv[k] * dzc_inv[k - 1];
+        const double bzp = dt * re * dzc_inv[k] * dzf_inv[k + 1], bzm = dt * re * dzc_inv[k] * dzf_inv[k];
+        r[2] = (float)(0.25 * dt * dzf_inv[k]); // hzuv
+        r[3] = (float)azp;
+        r[4] = (float)azm;
+        r[5] = (float)(2.0 * cxx + 2.0 * cyy + azp + azm); // ccuv
+        r[6] = (float)(0.25 * dt * dzc_inv[k]);            // hzw
+        r[7] = (float)bzp;
+        r[8] = (float)bzm;
+        r[9] = (float)(2.0 * cxx + 2.0 * cyy + bzp + bzm); // ccw
+        r[10] = (float)(dt * dzc_inv[k]);                  // gz
+    }
+    return t;
+}
+
+bool rk_mixed_supported(const StepParams &p) { return p.nx % MX == 0 && p.ny % MY == 0 && p.nz >= 2; }
+
+int rk_mixed_blocks(const StepParams &p) { return (p.nx / MX) * (p.ny / MY) * (p.nz / 16 > 1 ? p.nz / 16 : 1); }
+
+int launch_rk_mixed(const double *u, const double *v, const double *w, double *uo, double *vo, double *wo,
+                    const StepParams &p, const MeshDev &m, const float *tab, MeanState &ms, const float *pq, int pinc,
+                    cudaStream_t st)
+{
+    if (!rk_mixed_supported(p)) {
+        set_error("mixed fused RK kernel needs nx % 32 == 0 and ny % 16 == 0");
+        return -1;
+    }
+    // staging + rings + the chunk's coefficient table (room for chunks of up
+    // to MX_KCHUNK planes; mx_chunks gives at most 78)
+    const size_t shm = sizeof(double) * 3 * 3 * MPS + sizeof(float) * 2 * 3 * MFS +
+                       (sizeof(float4) * 3 + sizeof(double)) * (MX_KCHUNK + 4);
+    auto kern = (p.u_crf != 0.0) ? k_rk_mixed<true> : k_rk_mixed<false>;
+    PL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+    PL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     (int)cudaSharedmemCarveoutMaxShared));
+    int per_sm = 0, dev = 0, nsm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, MT, shm) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int nch = mx_chunks(p, (long)per_sm * (nsm > 0 ? nsm : 1));
+    const int kchunk = (p.nz + nch - 1) / nch;
+    if (kchunk > MX_KCHUNK) {
+        set_error("mixed fused RK kernel: z-chunk longer than its coefficient table");
+        return -1;
+    }
+    dim3 grid(p.nx / MX, p.ny / MY, (p.nz + kchunk - 1) / kchunk);
+    if ((int)(grid.x * grid.y * grid.z) > ms.max_blocks) {
+        set_error("mean buffer too small for the mixed fused RK kernel");
+        return -1;
+    }
+    MxConst K;
+    K.hx = (float)(0.25 * p.dt * p.dx_inv);
+    K.hy = (float)(0.25 * p.dt * p.dy_inv);
+    K.cxx = (float)(p.dt * p.re_inv * p.dx_inv * p.dx_inv);
+    K.cyy = (float)(p.dt * p.re_inv * p.dy_inv * p.dy_inv);
+    K.ucx = (float)(0.5 * p.dt * p.u_crf * p.dx_inv);
+    K.gx = (float)(p.dt * p.dx_inv);
+    K.gy = (float)(p.dt * p.dy_inv);
+    MeanRed r{ms.partial, ms.counter, ms.scalar, (double)p.nx, (double)p.ny, ms.vel_force};
+    kern<<<grid, dim3(MX, MT / MX), shm, st>>>(u, v, w, uo, vo, wo, p, m, reinterpret_cast<const float4 *>(tab), K, r,
+                                          kchunk, pq, pinc);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
+} // namespace pl

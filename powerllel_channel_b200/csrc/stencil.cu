@@ -402,7 +402,7 @@ __global__ void __launch_bounds__(256) k_rk2_mixed(const double *__restrict__ u,
                                                    const float *__restrict__ dv, const float *__restrict__ dw,
                                                    double *__restrict__ uo, double *__restrict__ vo,
                                                    double *__restrict__ wo, StepParams p, MeshDev m, MeanRed red,
-                                                   const double *__restrict__ pq, int pinc)
+                                                   const float *__restrict__ pq, int pinc)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -421,7 +421,7 @@ __global__ void __launch_bounds__(256) k_rk2_mixed(const double *__restrict__ u,
         if (pinc) { // u_hat = u* - dt G p_pred (FP64): its divergence is the increment's residual
             const size_t pc = n.c - sk;
             const double q0 = __ldg(pq + pc), qxp = __ldg(pq + n.xp - sk), qyp = __ldg(pq + n.yp - sk);
-            const double qzp = (k < p.nz) ? __ldg(pq + pc + sk) : q0;
+            const double qzp = (k < p.nz) ? (double)__ldg(pq + pc + sk) : q0;
             nu = nu - (qxp - q0) * (p.dt * p.dx_inv);
             nv = nv - (qyp - q0) * (p.dt * p.dy_inv);
             nw = nw - (qzp - q0) * p.dt * __ldg(m.dzc_inv + k);
@@ -723,7 +723,7 @@ int launch_rk1_mixed(const double *u, const double *v, const double *w, float *d
 
 int launch_rk2_mixed(const double *u, const double *v, const double *w, const float *d1u, const float *d1v,
                      const float *d1w, double *uo, double *vo, double *wo, const StepParams &p, const MeshDev &m,
-                     MeanState &ms, const double *pq, int pinc, cudaStream_t st)
+                     MeanState &ms, const float *pq, int pinc, cudaStream_t st)
 {
     if (nblocks(p) > ms.max_blocks) {
         set_error("mean buffer too small");

@@ -3,6 +3,8 @@
 // src/mod_calcRHS.f90, src/mod_updateBound.f90, src/mod_utils.f90).
 #pragma once
 
+#include <vector>
+
 #include "common.cuh"
 
 namespace pl {
@@ -54,12 +56,28 @@ bool rk_fused_supported(const StepParams &p);
 int rk_fused_blocks(const StepParams &p);
 int launch_rk_fused_fp64(const double *u, const double *v, const double *w, double *uo, double *vo, double *wo,
                          const StepParams &p, const MeshDev &m, MeanState &ms, cudaStream_t st);
-// mixed: with pinc, u_hat = u* - dt G pq (pq: the pressure prediction,
-// interior-only layout) is stored, whose divergence / dt is the increment's
-// residual
-int launch_rk_fused_mixed(const double *u, const double *v, const double *w, double *uo, double *vo, double *wo,
-                          const StepParams &p, const MeshDev &m, MeanState &ms, const double *pq, int pinc,
-                          cudaStream_t st);
+
+// mixed path: both RK stages in FP32 flux form (rk_mixed.cu); with pinc,
+// u_hat = u* - dt G pq is stored (pq: the FP32 pressure prediction,
+// interior-only layout), whose divergence / dt is the increment's residual.
+// tab: the per-plane coefficients of rk_mixed_table, 12 floats per plane
+// k = 0..nz+1, on the device.
+struct MxPlane {
+    float a, b;                 // face weights: q_{k+1/2} = q_k a + q_{k+1} b
+    float hzuv, azp, azm, ccuv; // u, v equations (dt folded in)
+    float hzw, bzp, bzm, ccw;   // w equation
+    float gz;                   // dt dzc_inv(k)
+};
+struct MxConst {
+    float hx, hy, cxx, cyy, ucx, gx, gy;
+};
+bool rk_mixed_supported(const StepParams &p);
+int rk_mixed_blocks(const StepParams &p);
+std::vector<float> rk_mixed_table(const StepParams &p, const std::vector<double> &dzf,
+                                  const std::vector<double> &dzf_inv, const std::vector<double> &dzc_inv);
+int launch_rk_mixed(const double *u, const double *v, const double *w, double *uo, double *vo, double *wo,
+                    const StepParams &p, const MeshDev &m, const float *tab, MeanState &ms, const float *pq, int pinc,
+                    cudaStream_t st);
 
 int launch_rk2m_fp64(double *u, double *v, double *w, const double *u1, const double *v1, const double *w1,
                      const StepParams &p, const MeshDev &m, MeanState &ms, cudaStream_t st);
@@ -74,7 +92,7 @@ int launch_rk1_mixed(const double *u, const double *v, const double *w, float *d
                      const StepParams &p, const MeshDev &m, cudaStream_t st);
 int launch_rk2_mixed(const double *u, const double *v, const double *w, const float *d1u, const float *d1v,
                      const float *d1w, double *uo, double *vo, double *wo, const StepParams &p, const MeshDev &m,
-                     MeanState &ms, const double *pq, int pinc, cudaStream_t st);
+                     MeanState &ms, const float *pq, int pinc, cudaStream_t st);
 int launch_rhs_mixed(const double *u, const double *v, const double *w, float *r, double *warp_part, double *mode0,
                      const StepParams &p, const MeshDev &m, cudaStream_t st);
 int warp_partials_per_plane(const StepParams &p);
