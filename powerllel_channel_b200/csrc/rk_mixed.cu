@@ -8,11 +8,11 @@
 // the last three planes of u, v, w (FP32, halo 2) and of the stage-1 field
 // u1 = u + d1 (FP32, halo 1); HBM sees u, v, w read once, the new fields
 // written once and the FP32 pressure prediction read once.  The FP64 planes
-// arrive through a three-slot staging ring filled by cp.async two planes
-// ahead of their conversion to FP32, and each thread converts only the
-// points it copied itself, so no load latency and no extra barrier sits on
-// the march's critical path; the stage-2 centre values of the next plane are
-// loaded into registers before stage 1, so their latency hides behind it.
+// arrive through a three-slot staging ring filled by 16-byte cp.async copies
+// two planes ahead of their conversion to FP32, so no load latency and no
+// extra barrier sits on the march's critical path; the stage-2 centre values
+// of the next plane are loaded into registers before stage 1, so their
+// latency hides behind it.
 //
 // The arithmetic is the reference's stencil rearranged into fluxes, which
 // the FP64 path (the parity path) does not do:
@@ -325,65 +325,55 @@ __global__ void __launch_bounds__(MT, 2) k_rk_mixed(const double *__restrict__ u
     const int kbeg = blockIdx.z * kchunk + 1, kend = min(kbeg + kchunk - 1, p.nz);
     const size_t sk = (size_t)p.nx * p.ny;
 
-    // ring-plane loads (36 x 20): slot 0 = x 2..33 of rows 0..7 (warp = row),
-    // slot 1 = rows 8..15, slot 2 = rows 16..19 (warps 0-3) and x 0, 1, 34,
-    // 35 of rows 0..19 (warps 4, 5 and half of warp 6: 80 points).  Whole
-    // 32-value row segments per warp: coalesced loads, conflict-free stores.
-    static_assert(MX == 32 && MY == 16 && MW == 36 && MH == 20, "slot maps of the 32 x 16 tile");
-    int loff[3], lxy[3];
-    const bool lval2 = wid < 6 || (wid == 6 && lane < 16);
-    {
-        int lx[3], ly[3];
-        lx[0] = lx[1] = 2 + lane;
-        ly[0] = wid;
-        ly[1] = 8 + wid;
-        if (wid < 4) {
-            lx[2] = 2 + lane;
-            ly[2] = 16 + wid;
-        } else {
-            const int e = (wid - 4) * 32 + lane, c = e % 4; // e < 80 on the valid lanes
-            lx[2] = c < 2 ? c : 32 + c;
-            ly[2] = min(e / 4, MH - 1);
-        }
+    // Ring-plane loads (36 x 20 of u, v, w): 1080 aligned pairs of doubles
+    // per plane, pair q = t + 256 s of thread t (s < 5; the fifth only for
+    // t < 56), pair q = field f, row r, x pair c (q = 360 f + 18 r + c).  Each
+    // pair is one 16-byte copy (cp.async.cg: L2 only, no L1 pollution) into
+    // the FP64 staging slot, and one 16-byte shared load, two conversions and
+    // an 8-byte store into the FP32 ring.  The pair's global source (periodic
+    // in x and y; a pair never straddles the wrap, nx being even) and both
+    // shared offsets are fixed for the whole march.
+    static_assert(MX == 32 && MY == 16 && MW == 36 && MH == 20, "pair maps of the 32 x 16 tile");
+    constexpr int NPAIR = 3 * MH * (MW / 2); // 1080
+    const int tid = lane + MX * wid;
+    const double *src[5];
+    int soff[5], roff[5];
 #pragma unroll
-        for (int sl = 0; sl < 3; sl++) {
-            int gi = i0 - 2 + lx[sl], gj = j0 - 2 + ly[sl];
-            gi += (gi < 0) ? p.nx : 0;
-            gi -= (gi >= p.nx) ? p.nx : 0;
-            gj += (gj < 0) ? p.ny : 0;
-            gj -= (gj >= p.ny) ? p.ny : 0;
-            loff[sl] = gi + p.nx * gj;
-            lxy[sl] = ly[sl] * MW + lx[sl];
-        }
+    for (int sl = 0; sl < 5; sl++) {
+        int q = tid + MT * sl;
+        if (q >= NPAIR) q = 0; // unused slot (sl = 4, tid >= 56)
+        const int fld = q / 360, r = (q % 360) / 18, c = q % 18;
+        int gx = i0 - 2 + 2 * c, gy = j0 - 2 + r;
+        gx += (gx < 0) ? p.nx : 0;
+        gx -= (gx >= p.nx) ? p.nx : 0;
+        gy += (gy < 0) ? p.ny : 0;
+        gy -= (gy >= p.ny) ? p.ny : 0;
+        src[sl] = (fld == 0 ? u : (fld == 1 ? v : w)) + (size_t)gy * p.nx + gx;
+        soff[sl] = fld * MPS + r * MW + 2 * c;
+        roff[sl] = fld * MFS + r * MW + 2 * c;
     }
+    const bool pv4 = tid + MT * 4 < NPAIR;
     // copy plane kq (in [0, nz+1]; none past last) into its staging slot; one
     // commit group per call, empty or not, so the wait counts stay uniform
     auto issue = [&](int kq, int last) {
         if (kq <= last) {
-            const size_t gk = sk * kq;
+            const size_t off = sk * kq;
             double *d = stg + (kq % 3) * 3 * MPS;
 #pragma unroll
-            for (int sl = 0; sl < 3; sl++) {
-                if (sl < 2 || lval2) {
-                    const size_t g = gk + loff[sl];
-                    cp_async_8(d + lxy[sl], u + g);
-                    cp_async_8(d + MPS + lxy[sl], v + g);
-                    cp_async_8(d + 2 * MPS + lxy[sl], w + g);
-                }
-            }
+            for (int sl = 0; sl < 5; sl++)
+                if (sl < 4 || pv4) cp_async_16(d + soff[sl], src[sl] + off);
         }
         cp_async_commit();
     };
-    // this thread's staged points of plane kq -> FP32 ring slot s
+    // staged plane kq (every thread's copies landed and a barrier passed) ->
+    // FP32 ring slot s
     auto convert = [&](int kq, int s) {
         const double *d = stg + (kq % 3) * 3 * MPS;
 #pragma unroll
-        for (int sl = 0; sl < 3; sl++) {
-            if (sl < 2 || lval2) {
-                const int q = s * MPS + lxy[sl];
-                ur[0 * MFS + q] = (float)d[lxy[sl]];
-                ur[1 * MFS + q] = (float)d[MPS + lxy[sl]];
-                ur[2 * MFS + q] = (float)d[2 * MPS + lxy[sl]];
+        for (int sl = 0; sl < 5; sl++) {
+            if (sl < 4 || pv4) {
+                const double2 x = *reinterpret_cast<const double2 *>(d + soff[sl]);
+                *reinterpret_cast<float2 *>(ur + s * MPS + roff[sl]) = make_float2((float)x.x, (float)x.y);
             }
         }
     };
@@ -423,11 +413,14 @@ __global__ void __launch_bounds__(MT, 2) k_rk_mixed(const double *__restrict__ u
     issue(mstart, last);
     issue(mstart + 1, last);
     cp_async_wait<0>();
+    __syncthreads();
     convert(mstart - 1, sa);
     convert(mstart, sb);
     convert(mstart + 1, sc);
-    issue(mstart + 2, last); // into the slots of mstart - 1 and mstart, converted above
+    __syncthreads();
+    issue(mstart + 2, last); // into the staging slots of mstart - 1 and mstart, converted above
     issue(mstart + 3, last);
+    cp_async_wait<1>(); // plane mstart + 2 landed; the barrier below publishes it
     __syncthreads();
 
     // bottom fluxes of the first stage-1 plane (the top fluxes of mstart - 1)
@@ -572,14 +565,12 @@ __global__ void __launch_bounds__(MT, 2) k_rk_mixed(const double *__restrict__ u
             __syncthreads();
             if (p.nz >= kbeg && p.nz <= kend) stage2(p.nz, sa, sb, sc, d1, centre(p.nz));
         }
-        if (mq + 2 <= last) {
-            // plane mq+2 was issued two iterations ago; mq+3 may still be in
-            // flight.  Its FP32 slot is plane mq-1's ((mq + 2) % 3 == (mq - 1) % 3),
-            // which stage 1 above has finished with.
-            cp_async_wait<1>();
-            convert(mq + 2, sa);
-        }
+        // staged plane mq+2 (landed and published by the last iteration's
+        // wait and barrier) into the FP32 slot of plane mq-1
+        // ((mq + 2) % 3 == (mq - 1) % 3), which stage 1 above has finished with
+        if (mq + 2 <= last) convert(mq + 2, sa);
         issue(mq + 4, last); // into the staging slot of plane mq + 1, converted last iteration
+        cp_async_wait<1>();  // plane mq + 3 landed (mq + 4 may be in flight)
 #pragma unroll
         for (int q = 0; q < 6; q++) e1[q] = d1[q];
         const int st = sa;
