@@ -45,9 +45,13 @@ WORKLOAD = "channel 512x384x256, Re_tau 1000, tanh stretch 2.0, Thomas, dt 1e-4,
 ALG_BYTES = {
     "fp64": {"rk_fused": 48, "rk1": 48, "rk2": 72, "calc_rhs": 32, "rhs_xfft": 32, "ppe_xfft_fwd": 16, "ppe_yfft_fwd": 16,
              "ppe_thomas": 20, "ppe_pdd": 40, "ppe_yfft_bwd": 16, "ppe_xfft_bwd": 16, "correct_force": 56},
-    "mixed": {"rk_fused": 56, "rk1": 36, "rk2": 68, "calc_rhs": 28, "rhs_xfft": 28, "ppe_xfft_fwd": 8, "ppe_yfft_fwd": 8,
-              "ppe_thomas": 12, "ppe_pdd": 32, "ppe_yfft_bwd": 8, "ppe_xfft_bwd": 40, "correct_force": 52},
+    "mixed": {"rk_fused": 52, "rk1": 36, "rk2": 64, "calc_rhs": 28, "rhs_xfft": 28, "ppe_xfft_fwd": 8, "ppe_yfft_fwd": 8,
+              "ppe_thomas": 12, "ppe_pdd": 32, "ppe_yfft_bwd": 8, "ppe_xfft_bwd": 24, "correct_force": 52},
 }
+# mixed: rk_fused reads u (FP64) and the FP32 pressure prediction and writes
+# u_hat (FP64): 24 + 4 + 24; ppe_xfft_bwd reads the FP32 half-complex line and
+# writes the FP32 increment, plus the FP32 pressure update (reads the
+# prediction and p_n, writes p_n+1 and the next prediction): 4 + 4 + 16
 # kernel launches per step (this library's kernels only)
 LAUNCHES = {"fp64": 7, "mixed": 8}
 

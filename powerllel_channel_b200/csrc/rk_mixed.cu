@@ -54,7 +54,8 @@ constexpr int MX = 32, MY = 16;         // tile; each thread owns the points (x,
 constexpr int MW = MX + 4, MH = MY + 4; // ring plane with a halo of 2
 constexpr int MPS = MW * MH;            // 720 values per plane
 constexpr int MNS = 3;                  // planes per ring
-constexpr int MFS = MNS * MPS;          // ring size per field
+constexpr int FST = MPS;                // ring layout [slot][field][xy]: field stride
+constexpr int SST = 3 * MPS;            // ... and plane (slot) stride
 constexpr int MT = 256;                 // threads
 constexpr int MX_KCHUNK = 80;           // longest z-chunk (planes)
 
@@ -64,11 +65,11 @@ struct Carry {
 };
 
 // the top fluxes of plane k at one point from the planes k (oc) and k+1 (op)
-// of a ring (u, v, w at R, R + MFS, R + 2 MFS); a, b: plane k's weights of
+// of a ring (u, v, w at R, R + FST, R + 2 FST); a, b: plane k's weights of
 // the face interpolation q_{k+1/2} = q_k a + q_{k+1} b
 __device__ __forceinline__ Carry mx_top(const float *R, int oc, int op, float a, float b)
 {
-    const float *u = R, *v = R + MFS, *w = R + 2 * MFS;
+    const float *u = R, *v = R + FST, *w = R + 2 * FST;
     Carry c;
     const float wc = w[oc];
     c.euw = (u[oc] * a + u[op] * b) * (wc + w[oc + 1]);
@@ -88,7 +89,7 @@ template <bool CRF>
 __device__ __forceinline__ void mx_rhs(const float *R, int om, int oc, int op, const MxPlane &P, const MxConst &K,
                                        Carry &cy, float &du, float &dv, float &dw)
 {
-    const float *u = R, *v = R + MFS, *w = R + 2 * MFS;
+    const float *u = R, *v = R + FST, *w = R + 2 * FST;
     const float uc = u[oc], uxp = u[oc + 1], uxm = u[oc - 1], uyp = u[oc + MW], uym = u[oc - MW];
     const float uzp = u[op], uzm = u[om], uxmyp = u[oc - 1 + MW], uxmzp = u[op - 1];
     const float vc = v[oc], vxp = v[oc + 1], vxm = v[oc - 1], vyp = v[oc + MW], vym = v[oc - MW];
@@ -181,7 +182,7 @@ __device__ __forceinline__ void mx_rhs2(const float *R, int om, int oc, int op, 
                                         Carry &cA, Carry &cB, float &duA, float &dvA, float &dwA, float &duB,
                                         float &dvB, float &dwB)
 {
-    const float *u = R, *v = R + MFS, *w = R + 2 * MFS;
+    const float *u = R, *v = R + FST, *w = R + 2 * FST;
     // u: the centre column y-1 .. y+2, the +x and -x columns, the planes above and below
     const float uym = u[oc - MW], uA = u[oc], uB = u[oc + MW], uyp2 = u[oc + 2 * MW];
     const float uxpA = u[oc + 1], uxpB = u[oc + 1 + MW];
@@ -311,33 +312,34 @@ __global__ void __launch_bounds__(MT, 2) k_rk_mixed(const double *__restrict__ u
                                                    MeshDev m, const float4 *__restrict__ tab, MxConst K, MeanRed red,
                                                    int kchunk, const float *__restrict__ pq, int pinc)
 {
+    constexpr int NSTG = 3; // FP64 staging slots
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *stg = reinterpret_cast<double *>(smem_raw);      // FP64 staging: plane k in slot k % 3, [slot][field][MPS]
-    float *ur = reinterpret_cast<float *>(stg + 3 * 3 * MPS); // u, v, w rings
-    float *sr = ur + 3 * MFS;                                 // u1 = u + d1 rings
+    double *stg = reinterpret_cast<double *>(smem_raw);    // FP64 staging, [slot][field][MPS]
+    float *ur = reinterpret_cast<float *>(stg + NSTG * SST); // u, v, w rings, [plane slot][field][MPS]
+    float *sr = ur + 3 * SST;                               // u1 = u + d1 rings
     // the chunk's plane coefficients (planes kbeg - 2 .. kbeg + kchunk + 1,
     // 3 float4 each) and dzf/lz: used every plane, so they live on chip
     // instead of in global loads whose latency would sit on the march
-    float4 *ptab = reinterpret_cast<float4 *>(sr + 3 * MFS);
+    float4 *ptab = reinterpret_cast<float4 *>(sr + 3 * SST);
     double *pzl = reinterpret_cast<double *>(ptab + 3 * (kchunk + 4));
     const int lane = threadIdx.x, wid = threadIdx.y;
     const int i0 = blockIdx.x * MX, j0 = blockIdx.y * MY;
     const int kbeg = blockIdx.z * kchunk + 1, kend = min(kbeg + kchunk - 1, p.nz);
     const size_t sk = (size_t)p.nx * p.ny;
+    const int tid = lane + MX * wid;
 
     // Ring-plane loads (36 x 20 of u, v, w): 1080 aligned pairs of doubles
     // per plane, pair q = t + 256 s of thread t (s < 5; the fifth only for
     // t < 56), pair q = field f, row r, x pair c (q = 360 f + 18 r + c).  Each
     // pair is one 16-byte copy (cp.async.cg: L2 only, no L1 pollution) into
     // the FP64 staging slot, and one 16-byte shared load, two conversions and
-    // an 8-byte store into the FP32 ring.  The pair's global source (periodic
-    // in x and y; a pair never straddles the wrap, nx being even) and both
-    // shared offsets are fixed for the whole march.
+    // an 8-byte store into the FP32 ring, at the same offset within the slot.
+    // The pair's global source (periodic in x and y; a pair never straddles
+    // the wrap, nx being even) and offset are fixed for the whole march.
     static_assert(MX == 32 && MY == 16 && MW == 36 && MH == 20, "pair maps of the 32 x 16 tile");
     constexpr int NPAIR = 3 * MH * (MW / 2); // 1080
-    const int tid = lane + MX * wid;
     const double *src[5];
-    int soff[5], roff[5];
+    int pk[5]; // offset of the pair in a staging slot and in a ring slot
 #pragma unroll
     for (int sl = 0; sl < 5; sl++) {
         int q = tid + MT * sl;
@@ -349,31 +351,34 @@ __global__ void __launch_bounds__(MT, 2) k_rk_mixed(const double *__restrict__ u
         gy += (gy < 0) ? p.ny : 0;
         gy -= (gy >= p.ny) ? p.ny : 0;
         src[sl] = (fld == 0 ? u : (fld == 1 ? v : w)) + (size_t)gy * p.nx + gx;
-        soff[sl] = fld * MPS + r * MW + 2 * c;
-        roff[sl] = fld * MFS + r * MW + 2 * c;
+        pk[sl] = fld * MPS + r * MW + 2 * c;
     }
     const bool pv4 = tid + MT * 4 < NPAIR;
-    // copy plane kq (in [0, nz+1]; none past last) into its staging slot; one
-    // commit group per call, empty or not, so the wait counts stay uniform
+
+    // copy u, v, w plane kq (in [0, nz+1]; none past last) into its staging
+    // slot; one commit group per call, empty or not, so the wait counts stay
+    // uniform
     auto issue = [&](int kq, int last) {
         if (kq <= last) {
             const size_t off = sk * kq;
-            double *d = stg + (kq % 3) * 3 * MPS;
+            double *d = stg + (kq % NSTG) * SST;
 #pragma unroll
             for (int sl = 0; sl < 5; sl++)
-                if (sl < 4 || pv4) cp_async_16(d + soff[sl], src[sl] + off);
+                if (sl < 4 || pv4) cp_async_16(d + pk[sl], src[sl] + off);
         }
         cp_async_commit();
     };
+
     // staged plane kq (every thread's copies landed and a barrier passed) ->
     // FP32 ring slot s
     auto convert = [&](int kq, int s) {
-        const double *d = stg + (kq % 3) * 3 * MPS;
+        const double *d = stg + (kq % NSTG) * SST;
+        float *o = ur + s * SST;
 #pragma unroll
         for (int sl = 0; sl < 5; sl++) {
             if (sl < 4 || pv4) {
-                const double2 x = *reinterpret_cast<const double2 *>(d + soff[sl]);
-                *reinterpret_cast<float2 *>(ur + s * MPS + roff[sl]) = make_float2((float)x.x, (float)x.y);
+                const double2 x = *reinterpret_cast<const double2 *>(d + pk[sl]);
+                *reinterpret_cast<float2 *>(o + pk[sl]) = make_float2((float)x.x, (float)x.y);
             }
         }
     };
@@ -403,12 +408,13 @@ __global__ void __launch_bounds__(MT, 2) k_rk_mixed(const double *__restrict__ u
     int sa = (mstart - 1) % MNS, sb = mstart % MNS, sc = (mstart + 1) % MNS;
     {
         const int k0 = max(kbeg - 2, 0), np = min(kbeg + kchunk + 1, p.nz + 1) - k0 + 1;
-        const int t = threadIdx.x + MX * threadIdx.y;
-        for (int q = t; q < 3 * np; q += MT) ptab[q] = __ldg(tab + 3 * k0 + q);
-        for (int q = t; q < np; q += MT) pzl[q] = __ldg(m.dzflzi + k0 + q);
+        for (int q = tid; q < 3 * np; q += MT) ptab[q] = __ldg(tab + 3 * k0 + q);
+        for (int q = tid; q < np; q += MT) pzl[q] = __ldg(m.dzflzi + k0 + q);
         ptab -= 3 * k0; // indexable by the global plane
         pzl -= k0;
     }
+    // a plane is issued two iterations before its conversion at the end of
+    // an iteration
     issue(mstart - 1, last);
     issue(mstart, last);
     issue(mstart + 1, last);
@@ -428,9 +434,9 @@ __global__ void __launch_bounds__(MT, 2) k_rk_mixed(const double *__restrict__ u
     Carry cA, cB, cH, c2A = zero, c2B = zero;
     {
         const MxPlane Pm = mx_plane(ptab, mstart - 1);
-        cA = mx_top(ur, sa * MPS + hxy0, sb * MPS + hxy0, Pm.a, Pm.b);
-        cB = mx_top(ur, sa * MPS + hxy0 + MW, sb * MPS + hxy0 + MW, Pm.a, Pm.b);
-        cH = hval1 ? mx_top(ur, sa * MPS + hxy1, sb * MPS + hxy1, Pm.a, Pm.b) : zero;
+        cA = mx_top(ur, sa * SST + hxy0, sb * SST + hxy0, Pm.a, Pm.b);
+        cB = mx_top(ur, sa * SST + hxy0 + MW, sb * SST + hxy0 + MW, Pm.a, Pm.b);
+        cH = hval1 ? mx_top(ur, sa * SST + hxy1, sb * SST + hxy1, Pm.a, Pm.b) : zero;
     }
     // d1 of the own pair at plane mq (this iteration) and at mq - 1
     float d1[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, e1[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -454,15 +460,15 @@ __global__ void __launch_bounds__(MT, 2) k_rk_mixed(const double *__restrict__ u
         c.v[1] = __ldg(v + g + p.nx);
         c.w[0] = __ldg(w + g);
         c.w[1] = __ldg(w + g + p.nx);
+        const size_t pl = sk * (kq - 1);
+        const size_t rowA = (size_t)p.nx * gjA + pl, rowB = rowA + p.nx, rowB2 = (size_t)p.nx * gjB2 + pl;
         c.qA = c.qB = c.qxA = c.qxB = c.qyB = c.qzA = c.qzB = 0.f;
         if (pinc) {
-            const size_t pl = sk * (kq - 1);
-            const size_t rowA = (size_t)p.nx * gjA + pl, rowB = rowA + p.nx;
             c.qA = __ldg(pq + rowA + gi);
             c.qB = __ldg(pq + rowB + gi);
             c.qxA = __ldg(pq + rowA + gxp);
             c.qxB = __ldg(pq + rowB + gxp);
-            c.qyB = __ldg(pq + (size_t)p.nx * gjB2 + pl + gi);
+            c.qyB = __ldg(pq + rowB2 + gi);
             c.qzA = (kq < p.nz) ? __ldg(pq + rowA + sk + gi) : c.qA;
             c.qzB = (kq < p.nz) ? __ldg(pq + rowB + sk + gi) : c.qB;
         }
@@ -475,12 +481,12 @@ __global__ void __launch_bounds__(MT, 2) k_rk_mixed(const double *__restrict__ u
         const MxPlane P = mx_plane(ptab, kq);
         if (first2) { // bottom fluxes of u1 at kq: the top fluxes of plane kq - 1
             const MxPlane Pm = mx_plane(ptab, kq - 1);
-            c2A = mx_top(sr, sm * MPS + hxy0, s0 * MPS + hxy0, Pm.a, Pm.b);
-            c2B = mx_top(sr, sm * MPS + hxy0 + MW, s0 * MPS + hxy0 + MW, Pm.a, Pm.b);
+            c2A = mx_top(sr, sm * SST + hxy0, s0 * SST + hxy0, Pm.a, Pm.b);
+            c2B = mx_top(sr, sm * SST + hxy0 + MW, s0 * SST + hxy0 + MW, Pm.a, Pm.b);
             first2 = false;
         }
         float d[6];
-        mx_rhs2<CRF>(sr, sm * MPS + hxy0, s0 * MPS + hxy0, sp * MPS + hxy0, P, K, c2A, c2B, d[0], d[1], d[2], d[3],
+        mx_rhs2<CRF>(sr, sm * SST + hxy0, s0 * SST + hxy0, sp * SST + hxy0, P, K, c2A, c2B, d[0], d[1], d[2], d[3],
                      d[4], d[5]);
         float iu[2], iv[2], iw[2];
 #pragma unroll
@@ -513,21 +519,21 @@ __global__ void __launch_bounds__(MT, 2) k_rk_mixed(const double *__restrict__ u
 
     // u1 = u + d1 at ring offset o (FP32), and its wall image at plane 0
     auto put1 = [&](int s, int sw, int xy, float du, float dv, float dw, bool bottom) {
-        const float a = ur[s * MPS + xy] + du, b = ur[MFS + s * MPS + xy] + dv;
-        sr[s * MPS + xy] = a;
-        sr[MFS + s * MPS + xy] = b;
-        sr[2 * MFS + s * MPS + xy] = ur[2 * MFS + s * MPS + xy] + dw;
+        const float a = ur[s * SST + xy] + du, b = ur[s * SST + FST + xy] + dv;
+        sr[s * SST + xy] = a;
+        sr[s * SST + FST + xy] = b;
+        sr[s * SST + 2 * FST + xy] = ur[s * SST + 2 * FST + xy] + dw;
         if (bottom) { // imposeNoSlipBC on u1: u1(0) = 2bc - u1(1), v1(0) = -v1(1), w1(0) = 0
-            sr[sw * MPS + xy] = bcu2 - a;
-            sr[MFS + sw * MPS + xy] = -b;
-            sr[2 * MFS + sw * MPS + xy] = 0.f;
+            sr[sw * SST + xy] = bcu2 - a;
+            sr[sw * SST + FST + xy] = -b;
+            sr[sw * SST + 2 * FST + xy] = 0.f;
         }
     };
     // the top wall plane of u1 at ring slot st from plane nz at slot sn
     auto top1 = [&](int st, int sn, int xy) {
-        sr[st * MPS + xy] = bcu2 - sr[sn * MPS + xy];
-        sr[MFS + st * MPS + xy] = -sr[MFS + sn * MPS + xy];
-        sr[2 * MFS + st * MPS + xy] = 0.f;
+        sr[st * SST + xy] = bcu2 - sr[sn * SST + xy];
+        sr[st * SST + FST + xy] = -sr[sn * SST + FST + xy];
+        sr[st * SST + 2 * FST + xy] = 0.f;
     };
 
     // Two barriers per plane: stage 1 at plane mq reads u planes mq-1..mq+1
@@ -540,14 +546,14 @@ __global__ void __launch_bounds__(MT, 2) k_rk_mixed(const double *__restrict__ u
         {
             const MxPlane P = mx_plane(ptab, mq);
             const bool top = (mq == p.nz), bottom = (mq == 1);
-            mx_rhs2<CRF>(ur, sa * MPS + hxy0, sb * MPS + hxy0, sc * MPS + hxy0, P, K, cA, cB, d1[0], d1[1], d1[2],
+            mx_rhs2<CRF>(ur, sa * SST + hxy0, sb * SST + hxy0, sc * SST + hxy0, P, K, cA, cB, d1[0], d1[1], d1[2],
                          d1[3], d1[4], d1[5]);
             if (top) d1[2] = d1[5] = 0.f; // w1(nz) = 0, the wall
             put1(sb, sa, hxy0, d1[0], d1[1], d1[2], bottom);
             put1(sb, sa, hxy0 + MW, d1[3], d1[4], d1[5], bottom);
             if (hval1) {
                 float du, dv, dw;
-                mx_rhs<CRF>(ur, sa * MPS + hxy1, sb * MPS + hxy1, sc * MPS + hxy1, P, K, cH, du, dv, dw);
+                mx_rhs<CRF>(ur, sa * SST + hxy1, sb * SST + hxy1, sc * SST + hxy1, P, K, cH, du, dv, dw);
                 if (top) dw = 0.f;
                 put1(sb, sa, hxy1, du, dv, dw, bottom);
             }
@@ -636,7 +642,7 @@ int launch_rk_mixed(const double *u, const double *v, const double *w, double *u
     }
     // staging + rings + the chunk's coefficient table (room for chunks of up
     // to MX_KCHUNK planes; mx_chunks gives at most 78)
-    const size_t shm = sizeof(double) * 3 * 3 * MPS + sizeof(float) * 2 * 3 * MFS +
+    const size_t shm = sizeof(double) * 3 * SST + sizeof(float) * 6 * SST +
                        (sizeof(float4) * 3 + sizeof(double)) * (MX_KCHUNK + 4);
     auto kern = (p.u_crf != 0.0) ? k_rk_mixed<true> : k_rk_mixed<false>;
     PL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
@@ -668,7 +674,7 @@ int launch_rk_mixed(const double *u, const double *v, const double *w, double *u
     K.gy = (float)(p.dt * p.dy_inv);
     MeanRed r{ms.partial, ms.counter, ms.scalar, (double)p.nx, (double)p.ny, ms.vel_force};
     kern<<<grid, dim3(MX, MT / MX), shm, st>>>(u, v, w, uo, vo, wo, p, m, reinterpret_cast<const float4 *>(tab), K, r,
-                                          kchunk, pq, pinc);
+                                               kchunk, pq, pinc);
     PL_CHECK_LAUNCH();
     return 0;
 }
