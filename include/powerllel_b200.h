@@ -245,6 +245,53 @@ int pl_monitor_probe(pl_channel *c, int i, int j, int k, double out[4]);
  * other, each [k][j][i] over the clipped region */
 int pl_monitor_region(pl_channel *c, const int ijk[6], double *host_uvwp);
 
+/* ======================================================================
+ * 5. z slabs: one GPU per slab of a multi-GPU run
+ *
+ * The reference decomposes the domain over p_row x p_col MPI ranks
+ * (decomp_2d.c:45-130); with p_row = 1 the x- and y-pencils coincide, the x
+ * and y transforms stay local and the tridiagonal systems are solved by PDD
+ * with one partition per rank (mod_poisson_solver.c:105-176, 361-466).  A
+ * slab holds planes kst+1 .. kst+nz of the global grid (distributed as
+ * decomp_2d.c:261-283 distributes them), its walls where it touches one, and
+ * two halo planes of u, v, w beyond each interface.  Every entry below is one
+ * phase of the step between two exchanges; the host moves the planes
+ * pl_slab_plane names between the ranks (in order, see
+ * powerllel_channel_b200/slab.py):
+ *   pl_slab_rk; sum plane 8 over the ranks; pl_slab_mean_finish;
+ *   w plane nz -> upper neighbour's plane 0;  pl_slab_rhs_sweep;
+ *   plane 4 (0) -> lower neighbour's 5;      pl_slab_pdd_iface;
+ *   plane 6 -> upper neighbour's 7;          pl_slab_finish;
+ *   plane 3 (0) -> lower neighbour's 3 (nz); pl_slab_correct;
+ *   u, v, w planes 1, 2 -> lower's nz+1, nz+2 and nz-1, nz -> upper's -1, 0.
+ * Counterparts: the MPI_Sendrecv calls of psolve_trid (:415-417, 444-446),
+ * updateHalo (mod_updateBound.f90:364-396) and the MPI_ALLREDUCE of Mean_h
+ * (mod_utils.f90:127); the plane tmp_v exchanged once in init_pdd_array
+ * (:172-174) is computed by every rank from the global tables instead.
+ * ====================================================================== */
+
+/* cfg describes the global problem; trid_parts must equal z_ranks */
+int pl_channel_create_slab(pl_channel **out, const pl_channel_config *cfg, int z_rank, int z_ranks);
+/* out = {kst, nz (the slab's planes), z_rank, z_ranks} */
+int pl_slab_info(pl_channel *c, int out[4]);
+/* device address of an exchanged plane, *bytes its size: field 0, 1, 2 = u,
+ * v, w plane k (-1 .. nz+2); 3 = the pressure the correction reads (FP64 p,
+ * or the mixed path's FP32 solution), interior plane k (0 .. nz; nz is the
+ * upper neighbour's first); 4 = the PDD sweep buffer, plane k; 5 = the upper
+ * neighbour's first swept plane (received); 6 = y3 (sent up); 7 = y1
+ * (received from below); 8 = the RK's sum of u dzf/lz; 9 = the initial
+ * field's sum of u dzf/lz (both one double, summed over the ranks in place) */
+void *pl_slab_plane(pl_channel *c, int field, int k, size_t *bytes);
+/* initFlow in two halves around the cross-rank sum of plane 9 */
+int pl_slab_init_fill(pl_channel *c, uint64_t seed, double noise);
+int pl_slab_init_finish(pl_channel *c);
+int pl_slab_rk(pl_channel *c);
+int pl_slab_mean_finish(pl_channel *c);
+int pl_slab_rhs_sweep(pl_channel *c);
+int pl_slab_pdd_iface(pl_channel *c);
+int pl_slab_finish(pl_channel *c);
+int pl_slab_correct(pl_channel *c);
+
 #ifdef __cplusplus
 }
 #endif

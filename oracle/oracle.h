@@ -81,6 +81,11 @@ const double *orc_ppe_pivots(const orc_ppe *s);
 /* ---- one time step of main.f90:131-208 ------------------------------ */
 typedef void (*orc_ppe_fn)(void *ctx, double *var);
 void orc_ppe_execute_cb(void *ctx, double *var); /* ctx = orc_ppe* */
+/* one PDD partition m, as the rank holding it runs it (see oracle_ppe.c) */
+void orc_slab_forward(orc_ppe *s, int m, const double *x, double *xs);
+void orc_slab_iface(orc_ppe *s, int m, const double *xs, const double *tvar, double *y2, double *y3);
+void orc_slab_finish(orc_ppe *s, int m, double *xs, const double *y1, const double *y2, double *out);
+void orc_slab_extent(const orc_ppe *s, int m, int *kst, int *ksz);
 void orc_step(const orc_grid *g, orc_ppe_fn ppe, void *ppe_ctx, double *u, double *v, double *w, double *u1,
               double *v1, double *w1, double *p);
 

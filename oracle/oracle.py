@@ -93,6 +93,10 @@ def lib():
         L.orc_ppe_init.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, _dp, C.c_int]
         L.orc_ppe_init.restype = C.c_void_p
         L.orc_ppe_execute.argtypes = [C.c_void_p, _dp]
+        L.orc_slab_forward.argtypes = [C.c_void_p, C.c_int, _dp, _dp]
+        L.orc_slab_iface.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp]
+        L.orc_slab_finish.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp]
+        L.orc_slab_extent.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.orc_ppe_free.argtypes = [C.c_void_p]
         L.orc_ppe_pivots.argtypes = [C.c_void_p]
         L.orc_ppe_pivots.restype = _dp
@@ -197,6 +201,7 @@ class PPE:
         self.dzf = np.ascontiguousarray(dzf_global, dtype=np.float64)
         self.h = lib().orc_ppe_init(nx, ny, nz, dx, dy, _ptr(self.dzf), nparts)
         self.n = (nx, ny, nz)
+        self.nparts = max(1, nparts)
 
     def execute(self, var):
         lib().orc_ppe_execute(self.h, _ptr(var))
@@ -214,6 +219,47 @@ class PPE:
             lib().orc_ppe_free(self.h)
         except Exception:
             pass
+
+
+class SlabPPE:
+    """CPU stand-in of one GPU's z slab for the PDD part of the slab schedule
+    (powerllel_channel_b200.slab.pdd_solve): partition m of the restated PDD
+    solve, with the same phase names and exchanged planes as the library's
+    slab.  rhs: the partition's planes of the right-hand side ([k][j][i])."""
+
+    def __init__(self, ppe: "PPE", m: int, rhs: np.ndarray):
+        import torch
+        nx, ny, _ = ppe.n
+        kst, ksz = C.c_int(), C.c_int()
+        lib().orc_slab_extent(ppe.h, m, C.byref(kst), C.byref(ksz))
+        self.ppe, self.rank, self.kst, self.nz = ppe, m, kst.value, ksz.value
+        self.ranks = ppe.nparts
+        self.x = np.ascontiguousarray(rhs, dtype=np.float64)
+        self.xs = np.zeros_like(self.x)
+        self.out = np.zeros_like(self.x)
+        self.planes = {5: torch.zeros(nx * ny, dtype=torch.float64), 6: torch.zeros(nx * ny, dtype=torch.float64),
+                       7: torch.zeros(nx * ny, dtype=torch.float64), 2: torch.zeros(nx * ny, dtype=torch.float64)}
+        self.nxy = nx * ny
+
+    def tensor(self, field, k=0):
+        import torch
+        if field == 4:  # the sweep buffer's plane k, shared with self.xs
+            return torch.from_numpy(self.xs.reshape(self.nz, -1)[k])
+        return self.planes[field]
+
+    def rhs_sweep(self):
+        lib().orc_slab_forward(self.ppe.h, self.rank, _ptr(self.x), _ptr(self.xs))
+
+    def pdd_iface(self):
+        if self.rank + 1 < self.ranks:
+            y2 = self.planes[2].numpy()
+            lib().orc_slab_iface(self.ppe.h, self.rank, _ptr(self.xs), _ptr(self.planes[5].numpy()), _ptr(y2),
+                                 _ptr(self.planes[6].numpy()))
+
+    def finish(self):
+        y1 = _ptr(self.planes[7].numpy()) if self.rank > 0 else None
+        y2 = _ptr(self.planes[2].numpy()) if self.rank + 1 < self.ranks else None
+        lib().orc_slab_finish(self.ppe.h, self.rank, _ptr(self.xs), y1, y2, _ptr(self.out))
 
 
 def ref_available() -> bool:

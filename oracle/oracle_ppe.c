@@ -287,6 +287,73 @@ void orc_ppe_execute(orc_ppe *s, double *var)
 
 void orc_ppe_execute_cb(void *ctx, double *var) { orc_ppe_execute((orc_ppe *)ctx, var); }
 
+/* One partition m of the PDD solve, as the rank that holds it runs it
+ * (psolve_trid, mod_poisson_solver.c:361-466, on p_col ranks with p_row = 1):
+ * the three parts between the two MPI_Sendrecv calls.  x is the partition's
+ * ksz[m] planes (layout [k][j][i], no ghosts); xs its FP64 sweep buffer;
+ * planes tvar, y1, y2, y3 are nx*ny.  Same operations, in the same order, as
+ * orc_ppe_execute's transforms and solve_trid for that partition. */
+void orc_slab_forward(orc_ppe *s, int m, const double *x, double *xs)
+{
+    const int nx = s->nx, ny = s->ny, ke = s->ksz[m];
+    const size_t nxy = (size_t)nx * ny;
+    memcpy(xs, x, sizeof(double) * nxy * ke);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < ke; k++)
+        for (int j = 0; j < ny; j++) hc_fft_r2hc(s->px, &xs[(size_t)k * nxy + (size_t)j * nx], 1);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < ke; k++)
+        for (int i = 0; i < nx; i++) hc_fft_r2hc(s->py, &xs[(size_t)k * nxy + i], nx);
+    thomas_chunk(nxy, ke, s->a + s->kst[m], s->c + s->kst[m], s->b + nxy * s->kst[m], xs);
+}
+
+void orc_slab_iface(orc_ppe *s, int m, const double *xs, const double *tvar, double *y2, double *y3)
+{
+    const size_t nxy = (size_t)s->nx * s->ny;
+    const int ke = s->ksz[m];
+    const double *wt = s->w + nxy * (s->kst[m] + ke - 1);
+    const double *xt = xs + nxy * (ke - 1);
+    const double *tmp_v = s->tmp_v + nxy * m;
+#pragma omp parallel for schedule(static)
+    for (size_t ij = 0; ij < nxy; ij++) {
+        double det_pdd = wt[ij] * tmp_v[ij] - ((double)1.0);
+        y2[ij] = (xt[ij] * tmp_v[ij] - tvar[ij]) / det_pdd;
+        y3[ij] = (tvar[ij] * wt[ij] - xt[ij]) / det_pdd;
+    }
+}
+
+/* y1 (NULL: no lower neighbour) and y2 (NULL: no upper one) are zero there */
+void orc_slab_finish(orc_ppe *s, int m, double *xs, const double *y1, const double *y2, double *out)
+{
+    const int nx = s->nx, ny = s->ny, k0 = s->kst[m], ke = s->ksz[m];
+    const size_t nxy = (size_t)nx * ny;
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < ke; k++)
+        for (size_t ij = 0; ij < nxy; ij++) {
+            const size_t g = ij + nxy * (size_t)k, gg = ij + nxy * (size_t)(k0 + k);
+            const double a1 = y1 ? y1[ij] : 0.0, a2 = y2 ? y2[ij] : 0.0;
+            xs[g] = xs[g] - s->v[gg] * a1 - s->w[gg] * a2;
+        }
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < ke; k++)
+        for (int i = 0; i < nx; i++) hc_fft_hc2r(s->py, &xs[(size_t)k * nxy + i], nx);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < ke; k++)
+        for (int j = 0; j < ny; j++) {
+            double *src = &xs[(size_t)k * nxy + (size_t)j * nx];
+            hc_fft_hc2r(s->px, src, 1);
+            double *dst = &out[(size_t)k * nxy + (size_t)j * nx];
+            for (int i = 0; i < nx; i++) dst[i] = src[i] * s->norm;
+        }
+}
+
+void orc_slab_extent(const orc_ppe *s, int m, int *kst, int *ksz)
+{
+    *kst = s->kst[m];
+    *ksz = s->ksz[m];
+}
+
+
 const double *orc_ppe_pivots(const orc_ppe *s) { return s->b; }
 
 void orc_ppe_free(orc_ppe *s)

@@ -14,6 +14,7 @@
 
 #include "../../include/powerllel_b200.h"
 #include "channel.cuh"
+#include "trid_tables.h"
 
 namespace pl {
 
@@ -233,20 +234,15 @@ static void channel_free(pl_channel *c)
 {
     pl_stat_disable(c);
     cudaFree(c->d_mesh);
-    cudaFree(c->u);
-    cudaFree(c->v);
-    cudaFree(c->w);
-    cudaFree(c->u1);
-    cudaFree(c->v1);
-    cudaFree(c->w1);
+    // velocity-like fields start hx planes before their plane 0
+    const size_t hoff = (size_t)c->hx * c->nx * c->ny;
+    for (double *f : {c->u, c->v, c->w, c->u1, c->v1, c->w1, c->ub, c->vb, c->wb})
+        if (f) cudaFree(f - hoff);
     cudaFree(c->p);
-    cudaFree(c->ub);
-    cudaFree(c->vb);
-    cudaFree(c->wb);
     cudaFree(c->p32);
     cudaFree(c->pm32);
     cudaFree(c->pb32);
-    cudaFree(c->mxtab);
+    if (c->mxtab) cudaFree(c->mxtab - (size_t)12 * c->hx);
     cudaFree(c->d1u);
     cudaFree(c->d1v);
     cudaFree(c->d1w);
@@ -265,7 +261,8 @@ static void channel_free(pl_channel *c)
     if (c->stream) cudaStreamDestroy(c->stream);
 }
 
-extern "C" int pl_channel_create(pl_channel **out, const pl_channel_config *cfg)
+// one GPU holding the whole domain (zn = 1), or z slab zr of zn
+static int channel_create(pl_channel **out, const pl_channel_config *cfg, int zr, int zn)
 {
     *out = nullptr;
     if (cfg->precision != PL_FP64 && cfg->precision != PL_MIXED) {
@@ -276,14 +273,37 @@ extern "C" int pl_channel_create(pl_channel **out, const pl_channel_config *cfg)
         set_error("pl_channel_create: nx, ny, nz must be even (mod_parameters.f90:264-267)");
         return -1;
     }
+    int kst = 0, nzl = cfg->nz;
+    if (zn > 1) {
+        // p_row = 1, p_col = zn: the z planes distributed as decomp_2d.c:261-283
+        // distributes them, and the PDD partitions are the slabs
+        if (zr < 0 || zr >= zn || cfg->trid_parts != zn) {
+            set_error("pl_channel_create_slab: needs 0 <= z_rank < z_ranks and trid_parts == z_ranks (PDD across "
+                      "the slabs, one partition per GPU)");
+            return -1;
+        }
+        std::vector<int> st, sz;
+        trid_distribute(cfg->nz, zn, st, sz);
+        for (int q = 0; q < zn; q++)
+            if (sz[q] < 2) {
+                set_error("pl_channel_create_slab: every slab needs at least 2 planes");
+                return -1;
+            }
+        kst = st[zr];
+        nzl = sz[zr];
+    }
     pl_channel *c = new pl_channel();
     c->cfg = *cfg;
     c->nx = cfg->nx;
     c->ny = cfg->ny;
-    c->nz = cfg->nz;
+    c->nz = nzl;
+    c->zrank = zn > 1 ? zr : 0;
+    c->zranks = zn > 1 ? zn : 1;
+    c->kst = kst;
+    c->hx = zn > 1 ? 1 : 0;
     c->nf = (size_t)c->nx * c->ny * (c->nz + 2);
     c->np = (size_t)c->nx * c->ny * c->nz;
-    build_mesh(c);
+    build_mesh(c); // the global mesh (cfg->nz planes)
     c->sp.nx = c->nx;
     c->sp.ny = c->ny;
     c->sp.nz = c->nz;
@@ -292,6 +312,10 @@ extern "C" int pl_channel_create(pl_channel **out, const pl_channel_config *cfg)
     c->sp.re_inv = cfg->u_ref * cfg->l_ref / cfg->re;
     c->sp.dt = cfg->dt;
     c->sp.u_crf = cfg->u_crf;
+    c->sp.wlo = c->zrank == 0;
+    c->sp.whi = c->zrank == c->zranks - 1;
+    c->sp.kofs = kst;
+    c->sp.nzg = cfg->nz;
     const double dx = cfg->lx / cfg->nx, dy = cfg->ly / cfg->ny;
     auto fail = [&](void) {
         channel_free(c);
@@ -302,16 +326,28 @@ extern "C" int pl_channel_create(pl_channel **out, const pl_channel_config *cfg)
         set_error("pl_channel_create: stream creation failed");
         return fail();
     }
-    const size_t n1 = c->nz + 2;
-    if (cudaMalloc(&c->d_mesh, sizeof(double) * n1 * 4) != cudaSuccess) return fail();
-    cudaMemcpy(c->d_mesh, c->dzf.data(), sizeof(double) * n1, cudaMemcpyHostToDevice);
-    cudaMemcpy(c->d_mesh + n1, c->dzf_inv.data(), sizeof(double) * n1, cudaMemcpyHostToDevice);
-    cudaMemcpy(c->d_mesh + 2 * n1, c->dzc_inv.data(), sizeof(double) * n1, cudaMemcpyHostToDevice);
-    cudaMemcpy(c->d_mesh + 3 * n1, c->dzflzi.data(), sizeof(double) * n1, cudaMemcpyHostToDevice);
-    c->m.dzf = c->d_mesh;
-    c->m.dzf_inv = c->d_mesh + n1;
-    c->m.dzc_inv = c->d_mesh + 2 * n1;
-    c->m.dzflzi = c->d_mesh + 3 * n1;
+    // the device mesh over the local planes -hx .. nz+1+hx (global plane
+    // kst + k; beyond the global range only at a wall, where nothing reads it)
+    const int hx = c->hx;
+    const size_t n1 = c->nz + 2 + 2 * hx;
+    {
+        std::vector<double> loc(4 * n1);
+        const int nzg = cfg->nz;
+        for (size_t q = 0; q < n1; q++) {
+            int kg = kst + (int)q - hx;
+            kg = kg < 0 ? 0 : (kg > nzg + 1 ? nzg + 1 : kg);
+            loc[q] = c->dzf[kg];
+            loc[n1 + q] = c->dzf_inv[kg];
+            loc[2 * n1 + q] = c->dzc_inv[kg];
+            loc[3 * n1 + q] = c->dzflzi[kg];
+        }
+        if (cudaMalloc(&c->d_mesh, sizeof(double) * n1 * 4) != cudaSuccess) return fail();
+        cudaMemcpy(c->d_mesh, loc.data(), sizeof(double) * 4 * n1, cudaMemcpyHostToDevice);
+    }
+    c->m.dzf = c->d_mesh + hx;
+    c->m.dzf_inv = c->d_mesh + n1 + hx;
+    c->m.dzc_inv = c->d_mesh + 2 * n1 + hx;
+    c->m.dzflzi = c->d_mesh + 3 * n1 + hx;
     const bool mixed = cfg->precision == PL_MIXED;
     auto dalloc = [&](double **f, size_t n) {
         if (cudaMalloc(f, sizeof(double) * n) != cudaSuccess) return false;
@@ -326,14 +362,29 @@ extern "C" int pl_channel_create(pl_channel **out, const pl_channel_config *cfg)
     // both RK stages in one kernel where the grid tiles: 32 x 8 (FP64
     // kernel) or 32 x 16 (mixed kernel); else the two stage kernels
     c->fused_rk = mixed ? rk_mixed_supported(c->sp) : rk_fused_supported(c->sp);
-    bool ok = dalloc(&c->u, c->nf) && dalloc(&c->v, c->nf) && dalloc(&c->w, c->nf) && dalloc(&c->p, c->np) &&
-              dalloc(&c->ub, c->nf) && dalloc(&c->vb, c->nf) && dalloc(&c->wb, c->nf);
-    if (ok && !mixed) ok = dalloc(&c->u1, c->nf) && dalloc(&c->v1, c->nf) && dalloc(&c->w1, c->nf);
-    if (ok && mixed)
+    if (zn > 1 && !c->fused_rk) {
+        set_error("pl_channel_create_slab: the slab step needs the fused RK kernel: nx % 32 == 0 and ny % 8 == 0 "
+                  "(FP64) or ny % 16 == 0 (mixed)");
+        return fail();
+    }
+    // velocity-like fields with hx halo planes beyond each wall plane
+    const size_t sk = (size_t)c->nx * c->ny;
+    auto valloc = [&](double **f) {
+        if (!dalloc(f, c->nf + 2 * hx * sk)) return false;
+        *f += hx * sk;
+        return true;
+    };
+    const size_t npx = c->np + hx * sk; // pressure with the upper neighbour's first plane
+    bool ok = valloc(&c->u) && valloc(&c->v) && valloc(&c->w) && dalloc(&c->p, npx) && valloc(&c->ub) &&
+              valloc(&c->vb) && valloc(&c->wb);
+    if (ok && !mixed && zn == 1) ok = valloc(&c->u1) && valloc(&c->v1) && valloc(&c->w1);
+    if (ok && mixed) {
         ok = falloc(&c->p32, c->np) && falloc(&c->pb32, c->np) && falloc(&c->pm32, c->np) &&
-             falloc(&c->mxtab, (size_t)12 * (c->nz + 2)) && falloc(&c->d1u, c->nf) && falloc(&c->d1v, c->nf) &&
-             falloc(&c->d1w, c->nf) && falloc(&c->r32, c->np) && dalloc(&c->mode0, c->nz) &&
+             falloc(&c->mxtab, (size_t)12 * n1) && falloc(&c->r32, npx) && dalloc(&c->mode0, c->nz) &&
              dalloc(&c->plane_part, (size_t)std::max(warp_partials_per_plane(c->sp), c->sp.ny / 2) * c->nz);
+        if (ok) c->mxtab += (size_t)12 * hx;
+        if (ok && zn == 1) ok = falloc(&c->d1u, c->nf) && falloc(&c->d1v, c->nf) && falloc(&c->d1w, c->nf);
+    }
     if (!ok) {
         set_error("pl_channel_create: out of device memory for the fields");
         return fail();
@@ -342,12 +393,14 @@ extern "C" int pl_channel_create(pl_channel **out, const pl_channel_config *cfg)
     // reference's truncated solve is not an exact inverse, so the full
     // pressure is solved each step as in the reference
     c->incremental = (cfg->trid_parts == 0) ? 1 : 0;
-    if (ppe_create(&c->ppe, c->nx, c->ny, c->nz, dx, dy, c->dzf_global.data(), cfg->trid_parts,
-                   mixed ? PREC_MIXED : PREC_FP64))
+    const int pprec = mixed ? PREC_MIXED : PREC_FP64;
+    if (zn > 1 ? ppe_create_slab(&c->ppe, c->nx, c->ny, cfg->nz, dx, dy, c->dzf_global.data(), zn, c->zrank, pprec)
+               : ppe_create(&c->ppe, c->nx, c->ny, c->nz, dx, dy, c->dzf_global.data(), cfg->trid_parts, pprec))
         return fail();
     if (mixed) {
-        const std::vector<float> tab = rk_mixed_table(c->sp, c->dzf, c->dzf_inv, c->dzc_inv);
-        if (cudaMemcpy(c->mxtab, tab.data(), sizeof(float) * tab.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+        const std::vector<float> tab = rk_mixed_table(c->sp, c->dzf, c->dzf_inv, c->dzc_inv, kst - hx, n1);
+        if (cudaMemcpy(c->mxtab - (size_t)12 * hx, tab.data(), sizeof(float) * tab.size(), cudaMemcpyHostToDevice) !=
+            cudaSuccess) {
             set_error("pl_channel_create: upload of the mixed RK coefficients failed");
             return fail();
         }
@@ -384,6 +437,20 @@ extern "C" int pl_channel_create(pl_channel **out, const pl_channel_config *cfg)
     return 0;
 }
 
+extern "C" int pl_channel_create(pl_channel **out, const pl_channel_config *cfg)
+{
+    return channel_create(out, cfg, 0, 1);
+}
+
+extern "C" int pl_channel_create_slab(pl_channel **out, const pl_channel_config *cfg, int z_rank, int z_ranks)
+{
+    if (z_ranks < 2) {
+        set_error("pl_channel_create_slab: z_ranks must be >= 2 (pl_channel_create holds the whole domain)");
+        return -1;
+    }
+    return channel_create(out, cfg, z_rank, z_ranks);
+}
+
 extern "C" int pl_channel_destroy(pl_channel *c)
 {
     if (!c) return 0;
@@ -393,11 +460,14 @@ extern "C" int pl_channel_destroy(pl_channel *c)
     return 0;
 }
 
-extern "C" int pl_channel_init_flow(pl_channel *c, uint64_t seed, double noise)
+// initFlow (mod_initFlow.f90:28-78) up to the Mean_h normalisation: the
+// Poiseuille profile plus the seeded noise (global-index counters), and the
+// plane-weighted sum of u in rb.scalar[6]
+static int init_fill(pl_channel *c, uint64_t seed, double noise)
 {
     double *dprof = nullptr;
     PL_CUDA_TRY(cudaMalloc(&dprof, sizeof(double) * (c->nz + 2)));
-    PL_CUDA_TRY(cudaMemcpy(dprof, c->prof.data(), sizeof(double) * (c->nz + 2), cudaMemcpyHostToDevice));
+    PL_CUDA_TRY(cudaMemcpy(dprof, c->prof.data() + c->kst, sizeof(double) * (c->nz + 2), cudaMemcpyHostToDevice));
     PL_CUDA_TRY(cudaMemsetAsync(c->u, 0, sizeof(double) * c->nf, c->stream));
     PL_CUDA_TRY(cudaMemsetAsync(c->v, 0, sizeof(double) * c->nf, c->stream));
     PL_CUDA_TRY(cudaMemsetAsync(c->w, 0, sizeof(double) * c->nf, c->stream));
@@ -408,9 +478,22 @@ extern "C" int pl_channel_init_flow(pl_channel *c, uint64_t seed, double noise)
     c->nsolve = 0;
     int rc = launch_init_fill(c->u, c->v, c->w, dprof, seed, noise, c->sp, c->stream);
     if (!rc) rc = launch_mean_sum(c->u, c->sp, c->m, c->rb, 0, c->stream);
-    if (!rc) rc = launch_init_finish(c->u, c->v, c->w, c->sp, c->cfg.u_ref, c->rb, c->stream);
+    if (!rc) rc = launch_mean_partials(c->sp, c->rb, c->stream);
     PL_CUDA_TRY(cudaStreamSynchronize(c->stream));
     cudaFree(dprof);
+    return rc;
+}
+
+extern "C" int pl_channel_init_flow(pl_channel *c, uint64_t seed, double noise)
+{
+    if (c->zranks > 1) {
+        set_error("pl_channel_init_flow: a z slab needs the cross-rank Mean_h: pl_slab_init_fill, the sum of "
+                  "pl_slab_plane(c, 9, 0) over the ranks, pl_slab_init_finish");
+        return -1;
+    }
+    int rc = init_fill(c, seed, noise);
+    if (!rc) rc = launch_init_finish(c->u, c->v, c->w, c->sp, c->cfg.u_ref, c->rb, c->stream);
+    PL_CUDA_TRY(cudaStreamSynchronize(c->stream));
     return rc;
 }
 
@@ -768,3 +851,112 @@ extern "C" void *pl_channel_field(pl_channel *c, int which)
 }
 
 extern "C" void *pl_channel_stream(pl_channel *c) { return (void *)c->stream; }
+
+// ------------------------------------------------------------------------
+// 4. z slabs of a multi-GPU run: the phases of one step between the
+//    exchanges, which the host performs (powerllel_channel_b200/slab.py)
+// ------------------------------------------------------------------------
+extern "C" int pl_slab_info(pl_channel *c, int out[4])
+{
+    out[0] = c->kst;
+    out[1] = c->nz;
+    out[2] = c->zrank;
+    out[3] = c->zranks;
+    return 0;
+}
+
+extern "C" void *pl_slab_plane(pl_channel *c, int field, int k, size_t *bytes)
+{
+    const size_t sk = (size_t)c->nx * c->ny;
+    const bool mixed = is_mixed(c);
+    if (bytes) *bytes = sizeof(double) * sk;
+    switch (field) {
+    case 0: return c->u + sk * (k + 1) - sk;
+    case 1: return c->v + sk * (k + 1) - sk;
+    case 2: return c->w + sk * (k + 1) - sk;
+    case 3: // the pressure the correction reads (plane k of the interior, nz = the halo)
+        if (mixed) {
+            if (bytes) *bytes = sizeof(float) * sk;
+            return c->r32 + sk * k;
+        }
+        return c->p + sk * k;
+    case 4: return c->ppe.d_scratch + sk * k;
+    case 5: return c->ppe.d_tvar;
+    case 6: return c->ppe.d_y3;
+    case 7: return c->ppe.d_y1;
+    case 8:
+        if (bytes) *bytes = sizeof(double);
+        return c->ms.scalar + 6;
+    case 9:
+        if (bytes) *bytes = sizeof(double);
+        return c->rb.scalar + 6;
+    default: set_error("pl_slab_plane: field must be 0..9"); return nullptr;
+    }
+}
+
+extern "C" int pl_slab_init_fill(pl_channel *c, uint64_t seed, double noise) { return init_fill(c, seed, noise); }
+
+extern "C" int pl_slab_init_finish(pl_channel *c)
+{
+    const int rc = launch_init_finish_sum(c->u, c->v, c->w, c->sp, c->cfg.u_ref, c->rb, c->stream);
+    PL_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return rc;
+}
+
+extern "C" int pl_slab_rk(pl_channel *c)
+{
+    if (!c->fused_rk) {
+        set_error("pl_slab_rk: the slab step needs the fused RK kernel");
+        return -1;
+    }
+    return pl_phase_rk(c);
+}
+
+extern "C" int pl_slab_mean_finish(pl_channel *c)
+{
+    return launch_mean_from_sum(c->ms.scalar, c->sp, c->ms.vel_force, c->stream);
+}
+
+// calcRHS fused into the forward x transform, the y transform, the local PDD sweep
+extern "C" int pl_slab_rhs_sweep(pl_channel *c)
+{
+    DivIn d;
+    d.u = c->u;
+    d.v = c->v;
+    d.w = c->w;
+    d.dzf_inv = c->m.dzf_inv;
+    d.dti = 1.0 / c->sp.dt;
+    d.dtidxi = d.dti * c->sp.dx_inv;
+    d.dtidyi = d.dti * c->sp.dy_inv;
+    int rc = is_mixed(c) ? ppe_xfwd_div<float>(&c->ppe, d, c->r32, c->plane_part, c->stream)
+                         : ppe_xfwd_div<double>(&c->ppe, d, c->p, nullptr, c->stream);
+    if (rc < 0) return -1;
+    if (rc > 0) {
+        // no fused divergence + x transform for this nx: calcRHS, then the
+        // solve's own forward x transform
+        if (pl_phase_calc_rhs(c)) return -1;
+        return is_mixed(c) ? ppe_slab_forward<float>(&c->ppe, c->r32, c->stream, c->mode0)
+                           : ppe_slab_forward<double>(&c->ppe, c->p, c->stream, nullptr);
+    }
+    if (is_mixed(c) && launch_plane_sums(c->plane_part, c->sp.ny / 2, c->nz, c->mode0, c->stream)) return -1;
+    channel_mark(c, "rhs_xfft");
+    return is_mixed(c) ? ppe_slab_forward_from_x<float>(&c->ppe, c->r32, c->stream, c->mode0)
+                       : ppe_slab_forward_from_x<double>(&c->ppe, c->p, c->stream, nullptr);
+}
+
+extern "C" int pl_slab_pdd_iface(pl_channel *c)
+{
+    return ppe_slab_iface(&c->ppe, c->stream, is_mixed(c) && c->zranks == 2);
+}
+
+extern "C" int pl_slab_finish(pl_channel *c)
+{
+    if (is_mixed(c)) {
+        const PressureUpdate pu = mixed_pressure_update(c);
+        c->p_stale = true;
+        return ppe_slab_backward<float>(&c->ppe, c->r32, c->stream, &pu);
+    }
+    return ppe_slab_backward<double>(&c->ppe, c->p, c->stream, nullptr);
+}
+
+extern "C" int pl_slab_correct(pl_channel *c) { return pl_phase_correct_force(c); }

@@ -12,6 +12,12 @@
 struct pl_channel {
     pl_channel_config cfg{};
     int nx = 0, ny = 0, nz = 0;
+    // z slab of a multi-GPU run (pl_channel_create_slab): nz above is the
+    // slab's plane count, kst its first plane in the global grid (0-based);
+    // hx = 1 extra halo plane below plane 0 and above nz+1 of every
+    // velocity-like field (the fused RK kernels read two planes beyond the
+    // slab), and one extra pressure plane (nz: the upper neighbour's first)
+    int zrank = 0, zranks = 1, kst = 0, hx = 0;
     size_t nf = 0;  // elements of a velocity-like field, nx*ny*(nz+2)
     size_t np = 0;  // elements of p, nx*ny*nz
     pl::StepParams sp{};

@@ -824,13 +824,30 @@ struct PddDev {
 // (:444-446), and the correction x -= v*y1 + w*y2 (:452-464).  The bottom
 // partition keeps y1 = 0 and the top one y2 = 0, as in the reference where
 // those arrays are zeroed at init and never received.
+//
+// Mixed path (mode0 given): the (0,0) column takes its FP64 right-hand side
+// from the plane sums, as in k_thomas.  Its matrix has zero row sums, so a
+// partition's spike towards a wall-bounded neighbour is the constant -1; with
+// two partitions both spikes of the one interface are, its reduced system is
+// singular (det = wt tv - 1 is round-off) and the reference's division leaves
+// x with an arbitrary constant far above FP32's resolution of x.  There the
+// system's free parameter is fixed by y3 = 0 (x moves by a constant only)
+// and y2 comes from its second row, y2 + tv y3 = tvar.  With three or more
+// partitions every truncated interface system is regular.
+__device__ __forceinline__ bool pdd_gauge00(const double *mode0, size_t col, int nparts)
+{
+    return mode0 != nullptr && col == 0 && nparts == 2;
+}
+
 template <typename T>
-__global__ void __launch_bounds__(128) k_pdd(double *xs, T *xout, TridDev t, PddDev p)
+__global__ void __launch_bounds__(128) k_pdd(double *xs, T *xout, TridDev t, PddDev p, const double *mode0)
 {
     const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y;
     if (px >= t.nx) return;
     const size_t col = (size_t)px + (size_t)t.nx * py, stride = (size_t)t.nx * t.ny;
     const size_t cls = trid_class(px, py, t), cstride = (size_t)t.ncx * t.ncy;
+    if (mode0 != nullptr && col == 0)
+        for (int k = 0; k < t.nz; k++) xs[(size_t)k * stride] = mode0[k];
     // local solves in FP64, in place in xs
     for (int m = 0; m < p.nparts; m++)
         thomas_column<double>(xs, xs, xs, col, cls, stride, cstride, p.kst[m], p.ksz[m], t);
@@ -846,6 +863,10 @@ __global__ void __launch_bounds__(128) k_pdd(double *xs, T *xout, TridDev t, Pdd
             const double det = wt * tv - 1.0;
             y2 = (xt * tv - tvar) / det;
             y3 = (tvar * wt - xt) / det;
+            if (pdd_gauge00(mode0, col, p.nparts)) {
+                y2 = tvar;
+                y3 = 0.0;
+            }
         }
         for (int k = p.kst[m]; k < p.kst[m] + p.ksz[m]; k++) {
             const size_t g = col + (size_t)k * stride;
@@ -853,6 +874,66 @@ __global__ void __launch_bounds__(128) k_pdd(double *xs, T *xout, TridDev t, Pdd
             xout[g] = (T)(xs[g] - __ldg(p.v + gc) * y1 - __ldg(p.w + gc) * y2);
         }
         y1 = y3;
+    }
+}
+
+// PDD of one z slab per GPU (psolve_trid, mod_poisson_solver.c:361-466, for
+// the rank that holds the partition): the local sweep, the interface solve
+// with the upper neighbour, and the correction, as three kernels around the
+// two plane exchanges.  Per column the arithmetic is k_pdd's for that
+// partition, operation for operation, the mixed path's (0,0) column included
+// (mode0: this slab's plane sums; gauge on the lower rank of two).
+__global__ void __launch_bounds__(128) k_pdd_sweep(double *xs, TridDev t, const double *mode0)
+{
+    const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y;
+    if (px >= t.nx) return;
+    const size_t col = (size_t)px + (size_t)t.nx * py, stride = (size_t)t.nx * t.ny;
+    const size_t cls = trid_class(px, py, t), cstride = (size_t)t.ncx * t.ncy;
+    if (mode0 != nullptr && col == 0)
+        for (int k = 0; k < t.nz; k++) xs[(size_t)k * stride] = mode0[k];
+    thomas_column<double>(xs, xs, xs, col, cls, stride, cstride, 0, t.nz, t);
+}
+
+// the reduced 2x2 system at the top interface (:423-438): tvar is the upper
+// neighbour's first swept row, tmpv its v at that row
+__global__ void __launch_bounds__(256) k_pdd_iface(const double *xs, const double *tvar, const double *w,
+                                                   const double *tmpv, double *y2, double *y3, TridDev t,
+                                                   int gauge00)
+{
+    const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y;
+    if (px >= t.nx) return;
+    const size_t col = (size_t)px + (size_t)t.nx * py, stride = (size_t)t.nx * t.ny;
+    const size_t cls = trid_class(px, py, t), cstride = (size_t)t.ncx * t.ncy;
+    const int kt = t.nz - 1;
+    const double wt = __ldg(w + cls + (size_t)kt * cstride);
+    const double tv = __ldg(tmpv + cls);
+    const double xt = xs[col + (size_t)kt * stride];
+    const double tva = tvar[col];
+    const double det = wt * tv - 1.0;
+    y2[col] = (xt * tv - tva) / det;
+    y3[col] = (tva * wt - xt) / det;
+    if (gauge00 && col == 0) {
+        y2[col] = tva;
+        y3[col] = 0.0;
+    }
+}
+
+// x = xs - v y1 - w y2 (:454-465); y1 = 0 without a lower neighbour, y2 = 0
+// without an upper one (the reference's zero-initialised arrays)
+template <typename T>
+__global__ void __launch_bounds__(128) k_pdd_fix(const double *xs, T *xout, const double *v, const double *w,
+                                                 const double *y1, const double *y2, int has_down, int has_up,
+                                                 TridDev t)
+{
+    const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y;
+    if (px >= t.nx) return;
+    const size_t col = (size_t)px + (size_t)t.nx * py, stride = (size_t)t.nx * t.ny;
+    const size_t cls = trid_class(px, py, t), cstride = (size_t)t.ncx * t.ncy;
+    const double a1 = has_down ? y1[col] : 0.0, a2 = has_up ? y2[col] : 0.0;
+    for (int k = 0; k < t.nz; k++) {
+        const size_t g = col + (size_t)k * stride;
+        const size_t gc = cls + (size_t)k * cstride;
+        xout[g] = (T)(xs[g] - __ldg(v + gc) * a1 - __ldg(w + gc) * a2);
     }
 }
 
@@ -1007,6 +1088,68 @@ int ppe_create(Ppe *s, int nx, int ny, int nz, double dx, double dy, const doubl
     return 0;
 }
 
+int ppe_create_slab(Ppe *s, int nx, int ny, int nz_global, double dx, double dy, const double *dzf_global,
+                    int nranks, int rank, int prec)
+{
+    if (nranks < 2 || rank < 0 || rank >= nranks) {
+        set_error("ppe_create_slab: needs 2 or more slabs and 0 <= rank < nranks");
+        return -1;
+    }
+    // the FFT plans and every table of the global PDD system, then this
+    // partition's rows of them
+    Ppe g;
+    if (ppe_create(&g, nx, ny, nz_global, dx, dy, dzf_global, nranks, prec)) {
+        ppe_destroy(&g);
+        return -1;
+    }
+    const int k0 = g.kst[rank], nzl = g.ksz[rank];
+    if (nzl < 2) {
+        ppe_destroy(&g);
+        set_error("ppe_create_slab: every slab needs at least 2 planes");
+        return -1;
+    }
+    *s = g; // plans, twiddles and sizes; the tables are replaced below
+    s->nz = nzl;
+    s->nparts = 1;
+    s->kst.assign(1, 0);
+    s->ksz.assign(1, nzl);
+    s->slab = 1;
+    s->has_down = rank > 0;
+    s->has_up = rank < nranks - 1;
+    s->d_mult = s->d_rb = s->d_c = s->d_a = s->d_bt = s->d_v = s->d_w = s->d_tmpv = s->d_scratch = nullptr;
+    const size_t ncls = (size_t)s->ncx * s->ncy, nxy = (size_t)nx * ny;
+    auto slice = [&](const double *src, size_t per_plane, int k_from, int nk, double **dst) -> int {
+        PL_CUDA_TRY(cudaMalloc(dst, sizeof(double) * per_plane * nk));
+        PL_CUDA_TRY(cudaMemcpy(*dst, src + per_plane * k_from, sizeof(double) * per_plane * nk,
+                               cudaMemcpyDeviceToDevice));
+        return 0;
+    };
+    int rc = slice(g.d_mult, ncls, k0, nzl, &s->d_mult) || slice(g.d_rb, ncls, k0, nzl, &s->d_rb) ||
+             slice(g.d_c, 1, k0, nzl, &s->d_c) || slice(g.d_a, 1, k0, nzl, &s->d_a) ||
+             slice(g.d_bt, 1, k0, nzl, &s->d_bt) || slice(g.d_v, ncls, k0, nzl, &s->d_v) ||
+             slice(g.d_w, ncls, k0, nzl, &s->d_w) || slice(g.d_tmpv, ncls, rank, 1, &s->d_tmpv);
+    // the global plan's own tables and scratch go; its plans and twiddles stay in s
+    cudaFree(g.d_mult);
+    cudaFree(g.d_rb);
+    cudaFree(g.d_c);
+    cudaFree(g.d_a);
+    cudaFree(g.d_bt);
+    cudaFree(g.d_v);
+    cudaFree(g.d_w);
+    cudaFree(g.d_tmpv);
+    cudaFree(g.d_scratch);
+    if (rc) return -1;
+    s->scratch_elems = nxy * nzl;
+    PL_CUDA_TRY(cudaMalloc(&s->d_scratch, sizeof(double) * s->scratch_elems));
+    PL_CUDA_TRY(cudaMalloc(&s->d_tvar, sizeof(double) * nxy * 4));
+    s->d_y1 = s->d_tvar + nxy;
+    s->d_y2 = s->d_y1 + nxy;
+    s->d_y3 = s->d_y2 + nxy;
+    PL_CUDA_TRY(cudaMemset(s->d_tvar, 0, sizeof(double) * nxy * 4));
+    return 0;
+}
+
+
 void ppe_destroy(Ppe *s)
 {
     cudaFree(s->d_twx64);
@@ -1023,6 +1166,7 @@ void ppe_destroy(Ppe *s)
     cudaFree(s->d_tmpv);
     cudaFree(s->d_scratch);
     cudaFree(s->d_mode0);
+    cudaFree(s->d_tvar);
     *s = Ppe();
 }
 
@@ -1238,7 +1382,7 @@ template <typename T> static int launch_trid(Ppe *s, T *x, cudaStream_t st, cons
         p.v = s->d_v;
         p.w = s->d_w;
         p.tmpv = s->d_tmpv;
-        k_pdd<T><<<grid, 128, 0, st>>>(xs, x, t, p);
+        k_pdd<T><<<grid, 128, 0, st>>>(xs, x, t, p, sizeof(T) == 4 ? mode0 : nullptr);
     }
     PL_CHECK_LAUNCH();
     return 0;
@@ -1328,7 +1472,7 @@ int ppe_solve_fp32_from_x(Ppe *s, float *d_var, const double *mode0, cudaStream_
     const size_t nxl = s->nx, nxy = (size_t)s->nx * s->ny;
     if (launch_y<float>(s, true, d_var, st)) return -1;
     mark(s, "ppe_yfft_fwd");
-    if (launch_trid<float>(s, d_var, st, s->nparts == 0 ? mode0 : nullptr)) return -1;
+    if (launch_trid<float>(s, d_var, st, mode0)) return -1;
     mark(s, s->nparts ? "ppe_pdd" : "ppe_thomas");
     if (launch_y<float>(s, false, d_var, st)) return -1;
     mark(s, "ppe_yfft_bwd");
@@ -1336,6 +1480,63 @@ int ppe_solve_fp32_from_x(Ppe *s, float *d_var, const double *mode0, cudaStream_
     mark(s, "ppe_xfft_bwd");
     return 0;
 }
+
+template <typename T> int ppe_slab_forward_from_x(Ppe *s, T *d_var, cudaStream_t st, const double *mode0)
+{
+    if (launch_y<T>(s, true, d_var, st)) return -1;
+    mark(s, "ppe_yfft_fwd");
+    if (sizeof(T) == 4) {
+        k_widen<<<1184, 256, 0, st>>>(reinterpret_cast<const float *>(d_var), s->d_scratch, s->scratch_elems);
+        PL_CHECK_LAUNCH();
+    } else {
+        PL_CUDA_TRY(cudaMemcpyAsync(s->d_scratch, d_var, sizeof(double) * s->scratch_elems, cudaMemcpyDeviceToDevice,
+                                    st));
+    }
+    TridDev t{s->nx, s->ny, s->nz, s->ncx, s->ncy, s->d_mult, s->d_rb, s->d_c};
+    k_pdd_sweep<<<dim3((s->nx + 127) / 128, s->ny), 128, 0, st>>>(s->d_scratch, t, mode0);
+    PL_CHECK_LAUNCH();
+    mark(s, "ppe_pdd_sweep");
+    return 0;
+}
+template int ppe_slab_forward_from_x<double>(Ppe *, double *, cudaStream_t, const double *);
+template int ppe_slab_forward_from_x<float>(Ppe *, float *, cudaStream_t, const double *);
+
+template <typename T> int ppe_slab_forward(Ppe *s, T *d_var, cudaStream_t st, const double *mode0)
+{
+    const size_t nxl = s->nx, nxy = (size_t)s->nx * s->ny;
+    if (launch_x<T>(s, true, d_var, 0, nxl, nxy, d_var, 0, nxl, nxy, (T)1, st)) return -1;
+    mark(s, "ppe_xfft_fwd");
+    return ppe_slab_forward_from_x<T>(s, d_var, st, mode0);
+}
+template int ppe_slab_forward<double>(Ppe *, double *, cudaStream_t, const double *);
+template int ppe_slab_forward<float>(Ppe *, float *, cudaStream_t, const double *);
+
+int ppe_slab_iface(Ppe *s, cudaStream_t st, int gauge00)
+{
+    if (!s->has_up) return 0;
+    TridDev t{s->nx, s->ny, s->nz, s->ncx, s->ncy, s->d_mult, s->d_rb, s->d_c};
+    k_pdd_iface<<<dim3((s->nx + 255) / 256, s->ny), 256, 0, st>>>(s->d_scratch, s->d_tvar, s->d_w, s->d_tmpv, s->d_y2,
+                                                                   s->d_y3, t, gauge00);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
+template <typename T> int ppe_slab_backward(Ppe *s, T *d_var, cudaStream_t st, const PressureUpdate *pu)
+{
+    const size_t nxl = s->nx, nxy = (size_t)s->nx * s->ny;
+    TridDev t{s->nx, s->ny, s->nz, s->ncx, s->ncy, s->d_mult, s->d_rb, s->d_c};
+    k_pdd_fix<T><<<dim3((s->nx + 127) / 128, s->ny), 128, 0, st>>>(s->d_scratch, d_var, s->d_v, s->d_w, s->d_y1,
+                                                                   s->d_y2, s->has_down, s->has_up, t);
+    PL_CHECK_LAUNCH();
+    mark(s, "ppe_pdd_fix");
+    if (launch_y<T>(s, false, d_var, st)) return -1;
+    mark(s, "ppe_yfft_bwd");
+    if (launch_x<T>(s, false, d_var, 0, nxl, nxy, d_var, 0, nxl, nxy, (T)s->norm, st, pu)) return -1;
+    mark(s, "ppe_xfft_bwd");
+    return 0;
+}
+template int ppe_slab_backward<double>(Ppe *, double *, cudaStream_t, const PressureUpdate *);
+template int ppe_slab_backward<float>(Ppe *, float *, cudaStream_t, const PressureUpdate *);
 
 } // namespace pl
 

@@ -45,6 +45,16 @@ struct Ppe {
     // (0,0) mode (mixed path): FP64 plane sums of the right-hand side
     double *d_mode0 = nullptr;
 
+    // z slab of a multi-GPU run: this plan holds partition `rank` of the
+    // global PDD system over `nranks` partitions (one per GPU); the tables
+    // above are that partition's rows (nz = its plane count), d_tmpv its
+    // interface plane (the upper neighbour's v at its first row).  Per-column
+    // interface values: tvar (the upper neighbour's first swept row,
+    // received), y2, y3 (the interface solve), y1 (the lower neighbour's y3,
+    // received); nx*ny doubles each.
+    int slab = 0, has_up = 0, has_down = 0;
+    double *d_tvar = nullptr, *d_y1 = nullptr, *d_y2 = nullptr, *d_y3 = nullptr;
+
     // optional per-launch marker (profiling): called after every kernel launch
     void (*mark)(void *ctx, const char *name) = nullptr;
     void *mark_ctx = nullptr;
@@ -52,13 +62,15 @@ struct Ppe {
 
 int ppe_create(Ppe *s, int nx, int ny, int nz, double dx, double dy, const double *dzf_global, int nparts,
                int prec);
+
 void ppe_destroy(Ppe *s);
 
 // In-place solve on the interior-only device array (layout [k][j][i]).
 int ppe_solve_fp64(Ppe *s, double *d_var, cudaStream_t st);
 // mode0 (optional, FP64 [nz]): the plane sums of the right-hand side; when
-// given, the (kx,ky) = (0,0) system is solved from them in FP64 with the
-// gauge x[nz-1] = 0 (Thomas only) instead of from the FP32 transform.
+// given, the (kx,ky) = (0,0) system is solved from them in FP64 instead of
+// from the FP32 transform, with its free constant fixed: x[nz-1] = 0 under
+// Thomas, y3 = 0 at the singular interface of a two-partition PDD.
 // Mixed step: the pressure update applied to the FP32 solution dp of the
 // increment solve, fused into the inverse x transform where the layout
 // allows (one kernel otherwise): p_new = (incremental ? q : 0) + dp stored
@@ -95,6 +107,30 @@ int ppe_solve_fp32(Ppe *s, float *d_var, const double *mode0, cudaStream_t st, c
 // the same solve when d_var already holds the forward x transform
 int ppe_solve_fp32_from_x(Ppe *s, float *d_var, const double *mode0, cudaStream_t st,
                           const PressureUpdate *pu = nullptr);
+
+// the plan of z slab `rank` of `nranks` (nz_global planes distributed as
+// decomp_2d.c:261-283 distributes them; PDD across the slabs)
+int ppe_create_slab(Ppe *s, int nx, int ny, int nz_global, double dx, double dy, const double *dzf_global,
+                    int nranks, int rank, int prec);
+// Slab solve, in three parts around the two PDD plane exchanges
+// (psolve_trid, mod_poisson_solver.c:361-466):
+//   ppe_slab_forward_from_x: y transform of d_var (which holds the x
+//     transform), the FP64 copy into the sweep buffer, the local sweep
+//     (mode0, mixed path: this slab's plane sums of the right-hand side,
+//     the (0,0) column's FP64 right-hand side);
+//   [the caller sends the sweep buffer's first plane (d_scratch) to the lower
+//    neighbour and receives the upper neighbour's into d_tvar]
+//   ppe_slab_iface: y2, y3 of the interface with the upper neighbour
+//     (gauge00: the mixed path over two slabs, whose (0,0) interface system
+//     is singular: y3 = 0 there);
+//   [the caller sends d_y3 to the upper neighbour, receives d_y1 from the lower]
+//   ppe_slab_backward: x = xs - v y1 - w y2 into d_var, inverse y and x
+//     transforms (with the mixed path's pressure update when pu is given).
+template <typename T> int ppe_slab_forward_from_x(Ppe *s, T *d_var, cudaStream_t st, const double *mode0);
+// the same from the right-hand side itself (x transform first)
+template <typename T> int ppe_slab_forward(Ppe *s, T *d_var, cudaStream_t st, const double *mode0);
+int ppe_slab_iface(Ppe *s, cudaStream_t st, int gauge00);
+template <typename T> int ppe_slab_backward(Ppe *s, T *d_var, cudaStream_t st, const PressureUpdate *pu);
 
 
 // Solve reading from / writing to a strided device array (the reference's

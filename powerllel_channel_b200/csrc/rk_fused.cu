@@ -131,11 +131,11 @@ __global__ void __launch_bounds__(FX *FY, 3) k_rk_fused(const double *__restrict
     // the rings hold the fields as loaded: a plane is copied asynchronously
     // (cp.async), in flight while stage 2 runs
     auto load_u_plane_async = [&](int kq, int s) {
-        const size_t gk = sk * kq;
+        const long long gk = (long long)sk * kq; // kq >= -1 (a slab's lower halo)
 #pragma unroll
         for (int sl = 0; sl < 2; sl++) {
             if (sl == 0 || lval1) {
-                const size_t g = gk + loff[sl];
+                const long long g = gk + loff[sl];
                 const int q = s * UPS + lxy[sl];
                 cp_async_8(ur + 0 * FS + q, u + g);
                 cp_async_8(ur + 1 * FS + q, v + g);
@@ -170,7 +170,7 @@ __global__ void __launch_bounds__(FX *FY, 3) k_rk_fused(const double *__restrict
             // u1 = u + dt*(visc - conv); w1(nz) = 0, the wall
             qr[oc] = ur[oc] + dt * (ru + (R)p.fb[0]);
             qr[FS + oc] = ur[FS + oc] + dt * (rv + (R)p.fb[1]);
-            qr[2 * FS + oc] = (mq == p.nz) ? (R)0 : ur[2 * FS + oc] + dt * (rw + (R)p.fb[2]);
+            qr[2 * FS + oc] = (p.whi && mq == p.nz) ? (R)0 : ur[2 * FS + oc] + dt * (rw + (R)p.fb[2]);
         }
     };
 
@@ -209,8 +209,8 @@ __global__ void __launch_bounds__(FX *FY, 3) k_rk_fused(const double *__restrict
         const double nw = ((double)qr[2 * FS + n.c] + p.dt * ((double)rw + p.fb[2]) + wc) * 0.5;
         uo[g] = nu;
         vo[g] = nv;
-        if (kq != p.nz) wo[g] = nw;
-        wall_fill<double>(uo, vo, wo, g, kq, sk, p.nz, 0.0 - p.u_crf, nu, nv);
+        if (kq != p.nz || !p.whi) wo[g] = nw;
+        wall_fill<double>(uo, vo, wo, g, kq, sk, p.nz, 0.0 - p.u_crf, nu, nv, p.wlo, p.whi);
         su += nu * __ldg(m.dzflzi + kq);
     };
 
@@ -223,10 +223,13 @@ __global__ void __launch_bounds__(FX *FY, 3) k_rk_fused(const double *__restrict
     // The mesh constants of plane mq (cur) and mq-1 (prev) roll in
     // registers: moving up one plane loads three values, dzf(mq+2),
     // dzc_inv(mq+1) and dzf_inv(mq+2), instead of all eleven per evaluation.
-    const int mstart = max(kbeg - 1, 1), mend = min(kend + 1, p.nz);
+    // stage 1 runs one plane beyond the chunk, but not on a wall plane
+    // (whose u1 is the wall fill); at a slab interface it runs on the halo
+    const int mstart = max(kbeg - 1, p.wlo ? 1 : 0), mend = min(kend + 1, p.whi ? p.nz : p.nz + 1);
     RhsConst<R> cur = rhs_const<R>(p, m, mstart), prev = cur; // prev is unused until mq = mstart + 1
     // ring slots of the planes mq-1, mq, mq+1, rotated once per plane
-    int sa = (mstart - 1) % NS, sb = mstart % NS, sc = (mstart + 1) % NS;
+    // ring slot of plane k: (k + NS) % NS (k >= -1 at a slab interface)
+    int sa = (mstart - 1 + NS) % NS, sb = mstart % NS, sc = (mstart + 1) % NS;
     load_u_plane_async(mstart - 1, sa);
     load_u_plane_async(mstart, sb);
     load_u_plane_async(mstart + 1, sc);
@@ -239,13 +242,13 @@ __global__ void __launch_bounds__(FX *FY, 3) k_rk_fused(const double *__restrict
         // the copy of u plane mq+2 into the slot of plane mq-1 (which
         // nothing reads after produce(mq)) overlaps stage 2
         if (next) load_u_plane_async(mq + 2, sa);
-        if (mq == 1) {
+        if (p.wlo && mq == 1) {
             wall(0, 1);
             __syncthreads();
         }
         // plane mq-2 sits in slot sc
         if (mq - 1 >= kbeg && mq - 1 <= kend) stage2(mq - 1, sc, sa, sb, prev);
-        if (mq == p.nz) {
+        if (p.whi && mq == p.nz) {
             // the top wall plane reuses the ring slot of u1(nz-2), which
             // stage2(nz-1) above has just consumed
             __syncthreads();

@@ -360,8 +360,8 @@ __global__ void __launch_bounds__(MT, 2) k_rk_mixed(const double *__restrict__ u
     // uniform
     auto issue = [&](int kq, int last) {
         if (kq <= last) {
-            const size_t off = sk * kq;
-            double *d = stg + (kq % NSTG) * SST;
+            const long long off = (long long)sk * kq; // kq >= -1 (a slab's lower halo)
+            double *d = stg + ((kq + NSTG) % NSTG) * SST;
 #pragma unroll
             for (int sl = 0; sl < 5; sl++)
                 if (sl < 4 || pv4) cp_async_16(d + pk[sl], src[sl] + off);
@@ -372,7 +372,7 @@ __global__ void __launch_bounds__(MT, 2) k_rk_mixed(const double *__restrict__ u
     // staged plane kq (every thread's copies landed and a barrier passed) ->
     // FP32 ring slot s
     auto convert = [&](int kq, int s) {
-        const double *d = stg + (kq % NSTG) * SST;
+        const double *d = stg + ((kq + NSTG) % NSTG) * SST;
         float *o = ur + s * SST;
 #pragma unroll
         for (int sl = 0; sl < 5; sl++) {
@@ -403,11 +403,14 @@ __global__ void __launch_bounds__(MT, 2) k_rk_mixed(const double *__restrict__ u
     const int gxp = (gi == p.nx - 1) ? 0 : gi + 1, gjB2 = (gjA + 2 >= p.ny) ? gjA + 2 - p.ny : gjA + 2;
     const size_t gA = (size_t)gi + (size_t)p.nx * gjA;
 
-    const int mstart = max(kbeg - 1, 1), mend = min(kend + 1, p.nz);
+    // stage 1 runs one plane beyond the chunk, but not on a wall plane
+    // (whose u1 is the wall fill); at a slab interface it runs on the halo
+    const int mstart = max(kbeg - 1, p.wlo ? 1 : 0), mend = min(kend + 1, p.whi ? p.nz : p.nz + 1);
     const int last = mend + 1; // the last u plane the march reads
-    int sa = (mstart - 1) % MNS, sb = mstart % MNS, sc = (mstart + 1) % MNS;
+    // ring slot of plane k: (k + 3) % 3 (k >= -1 at a slab interface)
+    int sa = (mstart - 1 + MNS) % MNS, sb = mstart % MNS, sc = (mstart + 1) % MNS;
     {
-        const int k0 = max(kbeg - 2, 0), np = min(kbeg + kchunk + 1, p.nz + 1) - k0 + 1;
+        const int k0 = max(kbeg - 2, p.wlo ? 0 : -1), np = min(kbeg + kchunk + 1, p.nz + (p.whi ? 1 : 2)) - k0 + 1;
         for (int q = tid; q < 3 * np; q += MT) ptab[q] = __ldg(tab + 3 * k0 + q);
         for (int q = tid; q < np; q += MT) pzl[q] = __ldg(m.dzflzi + k0 + q);
         ptab -= 3 * k0; // indexable by the global plane
@@ -511,8 +514,8 @@ __global__ void __launch_bounds__(MT, 2) k_rk_mixed(const double *__restrict__ u
             const double nu = cv.u[q] + (double)iu[q], nv = cv.v[q] + (double)iv[q], nw = cv.w[q] + (double)iw[q];
             uo[gq] = nu;
             vo[gq] = nv;
-            if (kq != p.nz) wo[gq] = nw;
-            wall_fill<double>(uo, vo, wo, gq, kq, sk, p.nz, 0.0 - p.u_crf, nu, nv);
+            if (kq != p.nz || !p.whi) wo[gq] = nw;
+            wall_fill<double>(uo, vo, wo, gq, kq, sk, p.nz, 0.0 - p.u_crf, nu, nv, p.wlo, p.whi);
             su += nu * zl;
         }
     };
@@ -545,7 +548,7 @@ __global__ void __launch_bounds__(MT, 2) k_rk_mixed(const double *__restrict__ u
         if (do2) cv = centre(mq - 1); // in flight during stage 1
         {
             const MxPlane P = mx_plane(ptab, mq);
-            const bool top = (mq == p.nz), bottom = (mq == 1);
+            const bool top = p.whi && mq == p.nz, bottom = p.wlo && mq == 1;
             mx_rhs2<CRF>(ur, sa * SST + hxy0, sb * SST + hxy0, sc * SST + hxy0, P, K, cA, cB, d1[0], d1[1], d1[2],
                          d1[3], d1[4], d1[5]);
             if (top) d1[2] = d1[5] = 0.f; // w1(nz) = 0, the wall
@@ -561,7 +564,7 @@ __global__ void __launch_bounds__(MT, 2) k_rk_mixed(const double *__restrict__ u
         __syncthreads();
         // plane mq-2 sits in slot sc
         if (do2) stage2(mq - 1, sc, sa, sb, e1, cv);
-        if (mq == p.nz) {
+        if (p.whi && mq == p.nz) {
             // the top wall plane of u1 takes the slot of plane nz-2, which
             // stage 2 at nz-1 has just consumed
             __syncthreads();
@@ -602,14 +605,20 @@ static int mx_chunks(const StepParams &p, long resident)
 }
 
 std::vector<float> rk_mixed_table(const StepParams &p, const std::vector<double> &dzf,
-                                  const std::vector<double> &dzf_inv, const std::vector<double> &dzc_inv)
+                                  const std::vector<double> &dzf_inv, const std::vector<double> &dzc_inv, int kg0,
+                                  size_t np)
 {
-    const int nz = p.nz;
-    std::vector<float> t((size_t)(nz + 2) * 12, 0.f);
+    // dzf, dzf_inv, dzc_inv: the global mesh, planes 0 .. nzg+1; entry q of
+    // the table is global plane kg0 + q (entries beyond the global range,
+    // only outside a wall, stay zero: nothing reads them)
+    const int nzg = (int)dzf.size() - 2;
+    std::vector<float> t(np * 12, 0.f);
     const double dt = p.dt, re = p.re_inv;
     const double cxx = dt * re * p.dx_inv * p.dx_inv, cyy = dt * re * p.dy_inv * p.dy_inv;
-    for (int k = 0; k <= nz; k++) {
-        float *r = t.data() + (size_t)12 * k;
+    for (size_t q = 0; q < np; q++) {
+        const int k = kg0 + (int)q;
+        if (k < 0 || k > nzg) continue;
+        float *r = t.data() + (size_t)12 * q;
         r[0] = (float)(dzf[k + 1] * dzc_inv[k]); // a
         r[1] = (float)(dzf[k] * dzc_inv[k]);     // b
         if (k == 0) continue;

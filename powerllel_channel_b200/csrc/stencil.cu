@@ -139,6 +139,7 @@ __global__ void k_finish_means(const double *partial, int nb, double dnx, double
     if (threadIdx.x == 0) {
         const double mean = sh[0] / dnx / dny; // Mean_h/nx_global/ny_global (mod_utils.f90:128)
         scalar[comp] = mean;
+        if (comp == 0) scalar[6] = sh[0]; // the sum itself (z slabs add theirs across ranks)
         const double f = comp == 0 ? f0 : (comp == 1 ? f1 : f2);
         scalar[3 + comp] = f - mean;
     }
@@ -283,8 +284,10 @@ __global__ void __launch_bounds__(256) k_init_fill(double *u, double *v, double 
 {
     PL_POINT_INDEX();
     const size_t c = (size_t)i + (size_t)p.nx * j + sk * k;
-    const uint64_t nint = (uint64_t)p.nx * p.ny * p.nz;
-    const uint64_t lin = (uint64_t)i + (uint64_t)p.nx * ((uint64_t)j + (uint64_t)p.ny * (uint64_t)(k - 1));
+    // the counter is the point's global index, so a z slab draws the same
+    // numbers as the whole domain
+    const uint64_t nint = (uint64_t)p.nx * p.ny * (p.nzg > 0 ? p.nzg : p.nz);
+    const uint64_t lin = (uint64_t)i + (uint64_t)p.nx * ((uint64_t)j + (uint64_t)p.ny * (uint64_t)(p.kofs + k - 1));
     // var + 2*(rn - 0.5)*norm (mod_initFlow.f90:372), rounded op by op like the
     // reference (no fused multiply-add)
     u[c] = __dadd_rn(__ldg(prof + k), __dmul_rn(__dmul_rn(2.0, splitmix_uniform(seed, lin) - 0.5), noise));
@@ -322,7 +325,7 @@ __global__ void __launch_bounds__(256) k_init_finish(double *u, double *v, doubl
     if (meanold != 0.0) nu = nu / meanold * u_ref;
     nu = nu - p.u_crf;
     u[c] = nu;
-    wall_fill<double>(u, v, w, c, k, sk, p.nz, 0.0 - p.u_crf, nu, v[c]);
+    wall_fill<double>(u, v, w, c, k, sk, p.nz, 0.0 - p.u_crf, nu, v[c], p.wlo, p.whi);
 }
 
 __global__ void __launch_bounds__(256) k_fill_bc(double *u, double *v, double *w, StepParams p)
@@ -520,7 +523,7 @@ __global__ void __launch_bounds__(RHS_BX *RHS_BY) k_correct_force(const TP *__re
     const double pxpb = (double)__ldg(pp + (size_t)p.nx * j + sk * (k - 1) + ip2); // (i+2, j)
     const P2 py = __ldg(reinterpret_cast<const P2 *>(pp + (size_t)p.nx * jp + sk * (k - 1) + i));
     double pza = p0a, pzb = p0b;
-    if (k < p.nz) {
+    if (k < p.nz || !p.whi) { // at a slab interface plane nz + 1 is the neighbour's first (a halo)
         const P2 pz = __ldg(reinterpret_cast<const P2 *>(pp + pc + sk));
         pza = (double)pz.x;
         pzb = (double)pz.y;
@@ -540,11 +543,11 @@ __global__ void __launch_bounds__(RHS_BX *RHS_BY) k_correct_force(const TP *__re
     *reinterpret_cast<double2 *>(v + c) = make_double2(nva, nvb);
     *reinterpret_cast<double2 *>(w + c) = make_double2(nwa, nwb);
     const double bcu = 0.0 - p.u_crf;
-    if (k == 1) {
+    if (p.wlo && k == 1) {
         *reinterpret_cast<double2 *>(u + c - sk) = make_double2(2.0 * bcu - nua, 2.0 * bcu - nub);
         *reinterpret_cast<double2 *>(v + c - sk) = make_double2(-nva, -nvb);
     }
-    if (k == p.nz) {
+    if (p.whi && k == p.nz) {
         *reinterpret_cast<double2 *>(u + c + sk) = make_double2(2.0 * bcu - nua, 2.0 * bcu - nub);
         *reinterpret_cast<double2 *>(v + c + sk) = make_double2(-nva, -nvb);
     }
@@ -670,6 +673,42 @@ int launch_init_finish(double *u, double *v, double *w, const StepParams &p, dou
                        cudaStream_t st)
 {
     k_finish_means<<<3, 1024, 0, st>>>(rb.partial, nblocks(p), (double)p.nx, (double)p.ny, 0.0, 0.0, 0.0, rb.scalar);
+    PL_CHECK_LAUNCH();
+    k_init_finish<<<point_grid(p), point_block(), 0, st>>>(u, v, w, p, u_ref, rb.scalar);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
+// Mean_h from the sum of u dzf/lz over all z slabs (scalar[6], summed across
+// the ranks by the caller): scalar[0] = Mean_h, scalar[3] = vel_force - Mean_h
+__global__ void k_mean_from_sum(double *scalar, double dnx, double dny, double vel_force)
+{
+    const double mean = scalar[6] / dnx / dny;
+    scalar[0] = mean;
+    scalar[3] = vel_force - mean;
+}
+
+int launch_mean_from_sum(double *scalar, const StepParams &p, double vel_force, cudaStream_t st)
+{
+    k_mean_from_sum<<<1, 1, 0, st>>>(scalar, (double)p.nx, (double)p.ny, vel_force);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
+// the block partials of launch_mean_sum (component 0) reduced: scalar[0] =
+// this grid's Mean_h, scalar[6] = its sum
+int launch_mean_partials(const StepParams &p, ReduceBuf &rb, cudaStream_t st)
+{
+    k_finish_means<<<1, 1024, 0, st>>>(rb.partial, nblocks(p), (double)p.nx, (double)p.ny, 0.0, 0.0, 0.0, rb.scalar);
+    PL_CHECK_LAUNCH();
+    return 0;
+}
+
+// initial-field normalisation u / Mean_h(u) u_ref from the summed scalar[6]
+int launch_init_finish_sum(double *u, double *v, double *w, const StepParams &p, double u_ref, ReduceBuf &rb,
+                           cudaStream_t st)
+{
+    k_mean_from_sum<<<1, 1, 0, st>>>(rb.scalar, (double)p.nx, (double)p.ny, 0.0);
     PL_CHECK_LAUNCH();
     k_init_finish<<<point_grid(p), point_block(), 0, st>>>(u, v, w, p, u_ref, rb.scalar);
     PL_CHECK_LAUNCH();

@@ -17,6 +17,11 @@ struct StepParams {
     int nx, ny, nz;
     double dx_inv, dy_inv, re_inv, dt, u_crf;
     double fb[3]; // uniform body force added to both RK stages (FP64 path; zero in the reference's step)
+    // z slab of a multi-GPU run: wlo / whi = 1 where the slab's bottom / top
+    // is a wall (imposeNoSlipBC), 0 at an interface with a neighbouring slab,
+    // whose velocity planes -1, 0 (nz+1, nz+2) are halos filled by exchange
+    int wlo = 1, whi = 1;
+    int kofs = 0, nzg = 0; // the slab's first plane in the global grid, the global nz (0: nz)
 };
 
 // Reduction scratch: per-block partial results and the final scalars.
@@ -73,8 +78,10 @@ struct MxConst {
 };
 bool rk_mixed_supported(const StepParams &p);
 int rk_mixed_blocks(const StepParams &p);
+// the table's np planes from global plane kg0 on (the mesh vectors are global)
 std::vector<float> rk_mixed_table(const StepParams &p, const std::vector<double> &dzf,
-                                  const std::vector<double> &dzf_inv, const std::vector<double> &dzc_inv);
+                                  const std::vector<double> &dzf_inv, const std::vector<double> &dzc_inv, int kg0,
+                                  size_t np);
 int launch_rk_mixed(const double *u, const double *v, const double *w, double *uo, double *vo, double *wo,
                     const StepParams &p, const MeshDev &m, const float *tab, MeanState &ms, const float *pq, int pinc,
                     cudaStream_t st);
@@ -114,5 +121,11 @@ int launch_mean_sum(const double *var, const StepParams &p, const MeshDev &m, Re
 int launch_init_finish(double *u, double *v, double *w, const StepParams &p, double u_ref, ReduceBuf &rb,
                        cudaStream_t st);
 int launch_fill_bc_vel(double *u, double *v, double *w, const StepParams &p, cudaStream_t st);
+// z slabs: Mean_h and the forceVel shift from the cross-rank sum in
+// scalar[6]; the initial-field normalisation likewise
+int launch_mean_from_sum(double *scalar, const StepParams &p, double vel_force, cudaStream_t st);
+int launch_mean_partials(const StepParams &p, ReduceBuf &rb, cudaStream_t st);
+int launch_init_finish_sum(double *u, double *v, double *w, const StepParams &p, double u_ref, ReduceBuf &rb,
+                           cudaStream_t st);
 
 } // namespace pl

@@ -179,17 +179,18 @@ __device__ __forceinline__ void momentum_rhs(const AU &u, const AV &v, const AW 
 }
 
 
-// wall fills of imposeNoSlipBC for the plane just written (k == 1 or nz)
+// wall fills of imposeNoSlipBC for the plane just written (k == 1 or nz),
+// where that side is a wall (wlo, whi: see StepParams)
 template <typename T>
 __device__ __forceinline__ void wall_fill(T *u, T *v, T *w, size_t c, int k, size_t sk, int nz, T bcu, T uval,
-                                          T vval)
+                                          T vval, int wlo = 1, int whi = 1)
 {
-    if (k == 1) {
+    if (wlo && k == 1) {
         u[c - sk] = (T)2.0 * bcu - uval;
         v[c - sk] = -vval;
         w[c - sk] = (T)0;
     }
-    if (k == nz) {
+    if (whi && k == nz) {
         u[c + sk] = (T)2.0 * bcu - uval;
         v[c + sk] = -vval;
         w[c] = (T)0;
@@ -270,6 +271,7 @@ __device__ __forceinline__ void mean_reduce(double su, const MeanRed &r)
         const double mean = s / r.dnx / r.dny;
         r.scalar[0] = mean;
         r.scalar[3] = r.vel_force - mean;
+        r.scalar[6] = s; // the plane-weighted sum itself (z slabs add theirs across ranks)
         *r.counter = 0u;
     }
 }
