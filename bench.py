@@ -11,8 +11,15 @@ no L2 flush is needed between steps.
 
 Arms: --impl b200 (default) times this library; --impl reference times the
 reference's own C PPE (src/src_c built unmodified in oracle/_ref) inside the C
-restatement of the Fortran stencils on the host cores.  N > 1: independent
-replicas, one per GPU (the 1-GPU path does not shard), max time over ranks.
+restatement of the Fortran stencils on the host cores.
+
+N > 1 (torchrun, one rank per GPU, NCCL): weak scaling over z slabs, as the
+reference decomposes with p_row = 1.  Every GPU holds a 512x384x256 slab of
+the 512x384x(256 N) channel, the wall-normal systems are solved by PDD with N
+partitions (one per GPU) and the planes move between the slabs' phases over
+NCCL on each slab's stream (powerllel_channel_b200.slab).  The value is N
+slab-steps per step time: steps/s in units of the 512x384x256 workload; the
+step time is the slowest rank's.
 """
 from __future__ import annotations
 
@@ -218,30 +225,142 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def _timed(ch, K, W, body, world):
+    """device time of K calls of body after W untimed ones: CUDA events on
+    the channel's stream, barrier and synchronisation on both sides, the
+    slowest rank's"""
+    import torch
+    for _ in range(W):
+        body()
+    ch.synchronize()
+    torch.cuda.synchronize()
+    st = torch.cuda.ExternalStream(ch.stream_handle)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0.record(st)
+    for _ in range(K):
+        body()
+    e1.record(st)
+    ch.synchronize()
+    torch.cuda.synchronize()
+    barrier(world)
+    return max_over_ranks(e0.elapsed_time(e1), world)
+
+
+def run_slabs(args, world, rank, local):
+    """N GPUs, one z slab each (weak scaling): see the module docstring"""
+    import torch
+    import powerllel_channel_b200 as plb
+    from powerllel_channel_b200 import slab as S
+    nzg = NZ * world
+    nzs = S.slab_sizes(nzg, world)[1]
+    peak, peak_kind = peaks()
+    npts = NX * NY * nzs[rank]
+    workload = (f"channel {NX}x{NY}x{nzg} as {world} z slabs of {NX}x{NY}x{NZ} (one per GPU), Re_tau {RE_TAU:g}, "
+                f"tanh stretch {STRETCH:g}, PDD over {world} partitions, dt {DT:g}, seed {SEED}, noise {NOISE:g}")
+
+    def measure(prec):
+        cfg = plb.ChannelConfig(nx=NX, ny=NY, nz=nzg, stretch_ratio=STRETCH, re_tau=RE_TAU, dt=DT, precision=prec,
+                                trid_parts=world)
+        sl = S.Slab(cfg, rank, world)
+        tr = S.DistTransport(sl)
+        S.init_flow([sl], tr, nzs, SEED, NOISE)
+        clocks = ClockSampler(local)
+        clocks.start()
+        ms = _timed(sl, args.steps, args.warmup, lambda: S.step([sl], tr, nzs), world)
+        clk = clocks.stop()
+        # per-phase device times over 3 steps (events on the slab's stream)
+        st = torch.cuda.ExternalStream(sl.stream_handle)
+        names, evs = [], []
+
+        def mark(name):
+            e = torch.cuda.Event(enable_timing=True)
+            e.record(st)
+            names.append(name)
+            evs.append(e)
+        mark("start")
+        for _ in range(3):
+            S.step([sl], tr, nzs, mark)
+        sl.synchronize()
+        nper = (len(evs) - 1) // 3
+        prof = []
+        for q in range(nper):
+            t = sum(evs[s * nper + q].elapsed_time(evs[s * nper + q + 1]) for s in range(3)) / 3
+            prof.append((names[q + 1], t))
+        return sl, tr, ms, clk, prof
+
+    sl, tr, ms64, clk64, prof64 = measure(plb.PL_FP64)
+    sl.close()
+    sl, tr, msm, clkm, profm = measure(plb.PL_MIXED)
+    sps64 = world * args.steps / (ms64 / 1000.0)
+    spsm = world * args.steps / (msm / 1000.0)
+    top = max((kv for kv in profm if not kv[0].startswith("x_")), key=lambda kv: kv[1])
+    alg = ALG_BYTES["mixed"].get(top[0], 0) * npts
+    achieved = alg / (top[1] / 1000.0) / 1e9
+    traffic = traffic_from_profiles(top[0])
+
+    # end to end: every step uploads this rank's u, v, w slab from pinned
+    # host memory, steps, downloads them
+    host = torch.empty(3 * sl.compact_elems, dtype=torch.float64).pin_memory()
+    sl.download_compact(host.data_ptr())
+    sl.synchronize()
+    nbytes = 3 * sl.compact_elems * 8
+    ke = max(3, min(args.steps, 10))
+
+    def e2e_body():
+        sl.upload_compact(host.data_ptr())
+        S.step([sl], tr, nzs)
+        sl.download_compact(host.data_ptr())
+
+    ms_e2e = _timed(sl, ke, 1, e2e_body, world)
+    e2e_sps = world * ke / (ms_e2e / 1000.0)
+    launches = S.launches_per_step(sl)
+    sl.close()
+    del host
+
+    if rank == 0:
+        def table(prof):
+            tot = sum(t for _, t in prof)
+            return {n: {"ms": round(t, 4), "share": round(t / tot, 4)} for n, t in prof}
+        line = {
+            "metric": METRIC, "value": spsm, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": msm / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "mixed: f32 stencils/FFT, f64 u,v,w,p and tridiagonal",
+            "data": "synthetic",
+            "config": {"workload": workload, "precision": "mixed", "grid": [NX, NY, nzg], "slab": [NX, NY, NZ],
+                       "l2": "inputs larger than L2 (403 MB per FP64 field per GPU), no flush",
+                       "parallelism": f"{world} z slabs, PDD across GPUs, NCCL plane exchanges",
+                       "value": "slab-steps/s (512x384x256 steps/s)"},
+            "fp64_steps_per_s": sps64, "fp64_ms_per_step": ms64 / args.steps,
+            "mixed_over_fp64": spsm / sps64,
+            "clocks": clkm, "clocks_fp64": clk64,
+            "e2e": {"value": e2e_sps, "unit": "steps/s", "h2d_bytes_per_step": nbytes,
+                    "d2h_bytes_per_step": nbytes, "per": "rank"},
+            "gpu_launches": launches * args.steps,
+            "roofline": {"bound": "hbm", "kernel": top[0], "achieved": round(achieved, 1), "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "traffic": traffic, "alg_bytes": alg},
+            "phases_mixed_rank0": table(profm), "phases_fp64_rank0": table(prof64),
+            "cpu_baseline": None,
+        }
+        print(json.dumps(line), flush=True)
+    import torch.distributed as dist
+    dist.destroy_process_group()
+
+
 def run_b200(args):
     world, rank, local = dist_setup(args.gpus)
     import numpy as np
     import torch
     torch.cuda.set_device(local)
+    if world > 1:
+        run_slabs(args, world, rank, local)
+        return
     import powerllel_channel_b200 as plb
 
     def timed(ch, K, W, body):
-        for _ in range(W):
-            body()
-        ch.synchronize()
-        torch.cuda.synchronize()
-        st = torch.cuda.ExternalStream(ch.stream_handle)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        barrier(world)
-        torch.cuda.synchronize()
-        e0.record(st)
-        for _ in range(K):
-            body()
-        e1.record(st)
-        ch.synchronize()
-        torch.cuda.synchronize()
-        barrier(world)
-        return max_over_ranks(e0.elapsed_time(e1), world)
+        return _timed(ch, K, W, body, world)
 
     peak, peak_kind = peaks()
     npts = NX * NY * NZ
@@ -346,7 +465,7 @@ def run_b200(args):
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "precision": "mixed", "grid": [NX, NY, NZ],
                        "l2": "inputs larger than L2 (403 MB per FP64 field), no flush",
-                       "parallelism": "1 GPU" if world == 1 else f"{world} independent replicas"},
+                       "parallelism": "1 GPU"},
             "fp64_steps_per_s": sps64, "fp64_ms_per_step": ms64 / args.steps,
             "mixed_over_fp64": spsm / sps64,
             "accuracy_after_100_steps": acc,

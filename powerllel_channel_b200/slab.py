@@ -135,6 +135,20 @@ class Slab:
     def stream_handle(self) -> int:
         return lib().pl_channel_stream(self._h) or 0
 
+    @property
+    def compact_elems(self) -> int:
+        """doubles per field of upload_compact / download_compact: the slab's
+        planes 0 .. nz+1, nx x ny each"""
+        return self.cfg.nx * self.cfg.ny * (self.nz + 2)
+
+    def upload_compact(self, host_ptr: int) -> None:
+        """u, v, w (planes 0 .. nz+1 each, back to back) from host memory,
+        asynchronously on the slab's stream"""
+        _check(lib().pl_channel_upload_compact(self._h, C.c_void_p(host_ptr)), "pl_channel_upload_compact")
+
+    def download_compact(self, host_ptr: int) -> None:
+        _check(lib().pl_channel_download_compact(self._h, C.c_void_p(host_ptr)), "pl_channel_download_compact")
+
     def synchronize(self):
         _check(lib().pl_channel_synchronize(self._h), "pl_channel_synchronize")
 
@@ -266,33 +280,59 @@ def velocity_halo_pairs(nzs):
     return pairs
 
 
-def pdd_solve(slabs, transport, nzs):
+def _noop(name):
+    pass
+
+
+def pdd_solve(slabs, transport, nzs, mark=_noop):
     """the PDD part of the solve: local sweeps, the first swept plane down,
     the interface solves, y3 up, the corrections and inverse transforms"""
     for s in slabs:
         s.rhs_sweep()
+    mark("rhs_sweep")
     transport.exchange(_pairs_down(nzs, F_SWEEP, lambda n: 0, F_TVAR, lambda n: 0))
+    mark("x_tvar")
     for s in slabs:
         s.pdd_iface()
+    mark("pdd_iface")
     transport.exchange(_pairs_up(nzs, F_Y3, lambda n: 0, F_Y1, lambda n: 0))
+    mark("x_y3")
     for s in slabs:
         s.finish()
+    mark("pdd_finish")
 
 
-def step(slabs, transport, nzs):
+def step(slabs, transport, nzs, mark=_noop):
     """one RK2 projection step (main.f90:137-208) over the slabs of this
-    process; nzs: every rank's plane count"""
+    process; nzs: every rank's plane count.  mark(name) is called after
+    each phase and exchange is issued (a profiler records an event there)."""
     for s in slabs:
         s.rk()
+    mark("rk_fused")
     transport.allreduce_sum(F_MEAN)
+    mark("x_mean")
     for s in slabs:
         s.mean_finish()
+    mark("mean_finish")
     transport.exchange(_pairs_up(nzs, F_W, lambda n: n, F_W, lambda n: 0))
-    pdd_solve(slabs, transport, nzs)
+    mark("x_w")
+    pdd_solve(slabs, transport, nzs, mark)
     transport.exchange(_pairs_down(nzs, F_P, lambda n: 0, F_P, lambda n: n))
+    mark("x_p")
     for s in slabs:
         s.correct()
+    mark("correct_force")
     transport.exchange(velocity_halo_pairs(nzs))
+    mark("x_vel")
+
+
+def launches_per_step(slab) -> int:
+    """this library's kernel launches in one step of ``slab``: RK 1, the
+    Mean_h finish 1, the fused divergence + x transform, y transform and
+    sweep 3 (mixed: + the plane sums and the FP64 widening), the interface
+    solve 1 (not on the top slab), correction + inverse y and x transforms 3,
+    velocity correction 1"""
+    return 1 + 1 + (5 if slab.mixed else 3) + (1 if slab.rank < slab.ranks - 1 else 0) + 3 + 1
 
 
 def init_flow(slabs, transport, nzs, seed, noise):

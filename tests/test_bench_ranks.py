@@ -1,8 +1,8 @@
 """The multi-GPU bench logic on CPU: two gloo ranks.
 
-With N GPUs the bench runs N independent replicas (the step does not shard
-here) and reports the job time as the slowest rank's, so every rank must
-agree on the max of the per-rank times; the reference arm prints one line
+With N GPUs the bench runs N z slabs of one channel (their exchanges are
+covered by the slab schedule test) and reports the job time as the slowest
+rank's, so every rank must agree on the max of the per-rank times; the reference arm prints one line
 from rank 0 and the other ranks exit without work.  Both are checked with
 torch.distributed over gloo, world size 2, no GPU."""
 import os
