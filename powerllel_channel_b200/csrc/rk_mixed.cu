@@ -10,9 +10,15 @@
 // written once and the FP32 pressure prediction read once.  The FP64 planes
 // arrive through a three-slot staging ring filled by 16-byte cp.async copies
 // two planes ahead of their conversion to FP32, so no load latency and no
-// extra barrier sits on the march's critical path; the stage-2 centre values
-// of the next plane are loaded into registers before stage 1, so their
-// latency hides behind it.
+// extra barrier sits on the march's critical path.
+//
+// The kernel is bound by instruction issue, not by HBM, so its layout
+// serves the instruction count: the march is unrolled by three, so every
+// ring slot is a compile-time constant and every ring access one base
+// register plus an immediate; a thread's two points are evaluated in packed
+// FP32 pairs (one two-lane instruction for both points, each lane rounded as
+// the scalar operation); every thread copies the same two (row, column)
+// pairs of the three fields, so the copy map costs four registers.
 //
 // The arithmetic is the reference's stencil rearranged into fluxes, which
 // the FP64 path (the parity path) does not do:
@@ -26,9 +32,9 @@
 //   * (q_c + q_xp)^2 - (q_xm + q_c)^2 = (q_xp - q_xm)(q_xp + q_xm + 2 q_c), and
 //     the viscous terms are one five-point combination per direction with
 //     dt, 0.25, 1/Re and the mesh factors folded into per-plane coefficients;
-//   * each thread evaluates its two points together: 41 shared-memory loads
-//     instead of 50, and the upper point's south fluxes are the lower
-//     point's north fluxes;
+//   * each thread evaluates its two points together, point B's terms being
+//     point A's one row up: the pair's south fluxes are (A's south, A's
+//     north), so no value crosses between the lanes of a pair;
 //   * the stage-1 increment d1 = dt RHS(u) of the tile's own points stays in
 //     the thread's registers from stage 1 of plane k to stage 2 of plane k
 //     (the thread that forms it consumes it), so only u1 goes through
@@ -40,6 +46,7 @@
 // FP32 and the sum in FP64: u, v, w stay FP64, and the projection residual of
 // the increment solve is the FP64 divergence of the stored u_hat, whatever
 // rounding the bracket carries.
+#include <type_traits>
 #include <vector>
 
 #include "fft.cuh" // cp.async helpers
@@ -173,135 +180,98 @@ __device__ __forceinline__ MxPlane mx_plane(const float4 *tab, int k)
 }
 
 
+// Packed FP32 pairs (Blackwell's two-lane FP32 instructions, each lane
+// rounded as the scalar operation): .x belongs to point A, .y to point B.
+typedef float2 f2;
+__device__ __forceinline__ f2 add2(f2 a, f2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ f2 sub2(f2 a, f2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ f2 mul2(f2 a, f2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ f2 bc2(float s) { return make_float2(s, s); }
+// values at offsets o (point A) and o + MW (point B) of a ring field
+__device__ __forceinline__ f2 ld2(const float *q, int o) { return make_float2(q[o], q[o + MW]); }
+
+// the carried top fluxes of the pair
+struct Carry2 {
+    f2 euw, evw, cw;
+};
+
 // dt * (momentum right-hand side) at the points A (oc) and B = A + y (oc + MW)
-// of a ring, sharing their loads and the edge products of their common face:
-// A's north fluxes are B's south fluxes.  cA, cB: the carried bottom fluxes
-// of A and B (top fluxes on return).
+// of a ring in packed pairs.  Every term of B is its term of A one row up,
+// so each pair is two loads one row apart: B's south fluxes (A's north
+// ones) come out of the pair (south of A, north of A), with no exchange
+// between the lanes.  cy: the pair's carried bottom fluxes (top fluxes on
+// return); du, dv, dw: the pair's increments.
 template <bool CRF>
 __device__ __forceinline__ void mx_rhs2(const float *R, int om, int oc, int op, const MxPlane &P, const MxConst &K,
-                                        Carry &cA, Carry &cB, float &duA, float &dvA, float &dwA, float &duB,
-                                        float &dvB, float &dwB)
+                                        Carry2 &cy, f2 &du, f2 &dv, f2 &dw)
 {
     const float *u = R, *v = R + FST, *w = R + 2 * FST;
-    // u: the centre column y-1 .. y+2, the +x and -x columns, the planes above and below
-    const float uym = u[oc - MW], uA = u[oc], uB = u[oc + MW], uyp2 = u[oc + 2 * MW];
-    const float uxpA = u[oc + 1], uxpB = u[oc + 1 + MW];
-    const float uxmA = u[oc - 1], uxmB = u[oc - 1 + MW], uxm2 = u[oc - 1 + 2 * MW];
-    const float uzpA = u[op], uzpB = u[op + MW], uzmA = u[om], uzmB = u[om + MW];
-    const float uxmzpA = u[op - 1], uxmzpB = u[op - 1 + MW];
-    const float vym = v[oc - MW], vA = v[oc], vB = v[oc + MW], vyp2 = v[oc + 2 * MW];
-    const float vxpym = v[oc + 1 - MW], vxpA = v[oc + 1], vxpB = v[oc + 1 + MW];
-    const float vxmA = v[oc - 1], vxmB = v[oc - 1 + MW];
-    const float vzpA = v[op], vzpB = v[op + MW], vzmA = v[om], vzmB = v[om + MW];
-    const float vymzp = v[op - MW];
-    const float wym = w[oc - MW], wA = w[oc], wB = w[oc + MW], wyp2 = w[oc + 2 * MW];
-    const float wxpA = w[oc + 1], wxpB = w[oc + 1 + MW], wxmA = w[oc - 1], wxmB = w[oc - 1 + MW];
-    const float wzpA = w[op], wzpB = w[op + MW], wzmA = w[om], wzmB = w[om + MW];
+    const f2 uC = ld2(u, oc), uYP = ld2(u, oc + MW), uYM = ld2(u, oc - MW);
+    const f2 uXP = ld2(u, oc + 1), uXM = ld2(u, oc - 1), uXMYP = ld2(u, oc - 1 + MW);
+    const f2 uZP = ld2(u, op), uZM = ld2(u, om), uXMZP = ld2(u, op - 1);
+    const f2 vC = ld2(v, oc), vYP = ld2(v, oc + MW), vYM = ld2(v, oc - MW);
+    const f2 vXP = ld2(v, oc + 1), vXM = ld2(v, oc - 1), vXPYM = ld2(v, oc + 1 - MW);
+    const f2 vZP = ld2(v, op), vZM = ld2(v, om), vYMZP = ld2(v, op - MW);
+    const f2 wC = ld2(w, oc), wYP = ld2(w, oc + MW), wYM = ld2(w, oc - MW);
+    const f2 wXP = ld2(w, oc + 1), wXM = ld2(w, oc - 1), wZP = ld2(w, op), wZM = ld2(w, om);
+    const f2 a = bc2(P.a), b = bc2(P.b);
 
-    // edge fluxes
-    const float euv_nA = (uA + uB) * (vA + vxpA); // = south flux of B
-    const float euv_nB = (uB + uyp2) * (vB + vxpB);
-    const float euv_sA = (uym + uA) * (vym + vxpym);
-    const float euv_wA = (uxmA + uxmB) * (vxmA + vA);
-    const float euv_wB = (uxmB + uxm2) * (vxmB + vB);
-    const float euw_tA = (uA * P.a + uzpA * P.b) * (wA + wxpA);
-    const float euw_tB = (uB * P.a + uzpB * P.b) * (wB + wxpB);
-    const float euw_wA = (uxmA * P.a + uxmzpA * P.b) * (wxmA + wA);
-    const float euw_wB = (uxmB * P.a + uxmzpB * P.b) * (wxmB + wB);
-    const float evw_tA = (vA * P.a + vzpA * P.b) * (wA + wB); // = south flux of B
-    const float evw_tB = (vB * P.a + vzpB * P.b) * (wB + wyp2);
-    const float evw_sA = (vym * P.a + vymzp * P.b) * (wym + wA);
-    const float wtA = wA + wzpA, wtB = wB + wzpB;
-    const float cw_tA = wtA * wtA, cw_tB = wtB * wtB;
+    // edge fluxes: (A, B) of the north, south, west, top faces
+    const f2 euv_n = mul2(add2(uC, uYP), add2(vC, vXP));
+    const f2 euv_s = mul2(add2(uYM, uC), add2(vYM, vXPYM)); // (south of A, north of A)
+    const f2 euv_w = mul2(add2(uXM, uXMYP), add2(vXM, vC));
+    const f2 euw_t = mul2(fma2(uC, a, mul2(uZP, b)), add2(wC, wXP));
+    const f2 euw_w = mul2(fma2(uXM, a, mul2(uXMZP, b)), add2(wXM, wC));
+    const f2 evw_t = mul2(fma2(vC, a, mul2(vZP, b)), add2(wC, wYP));
+    const f2 evw_s = mul2(fma2(vYM, a, mul2(vYMZP, b)), add2(wYM, wC)); // (south of A, top of A)
+    const f2 wt = add2(wC, wZP);
+    const f2 cw_t = mul2(wt, wt);
 
-    float r;
-    // u at A and B
+    const f2 cxx = bc2(K.cxx), cyy = bc2(K.cyy), nhx = bc2(-K.hx), nhy = bc2(-K.hy);
+    f2 r;
     {
-        const float sx = uxpA + uxmA, sy = uB + uym, dx = uxpA - uxmA;
-        r = K.cxx * sx;
-        r = fmaf(K.cyy, sy, r);
-        r = fmaf(P.azp, uzpA, r);
-        r = fmaf(P.azm, uzmA, r);
-        r = fmaf(-P.ccuv, uA, r);
-        r = fmaf(-K.hx, dx * fmaf(2.f, uA, sx), r);
-        r = fmaf(-K.hy, euv_nA - euv_sA, r);
-        r = fmaf(-P.hzuv, euw_tA - cA.euw, r);
-        if (CRF) r = fmaf(-K.ucx, dx, r);
-        duA = r;
+        const f2 sx = add2(uXP, uXM), sy = add2(uYP, uYM), dx = sub2(uXP, uXM);
+        r = mul2(cxx, sx);
+        r = fma2(cyy, sy, r);
+        r = fma2(bc2(P.azp), uZP, r);
+        r = fma2(bc2(P.azm), uZM, r);
+        r = fma2(bc2(-P.ccuv), uC, r);
+        r = fma2(nhx, mul2(dx, fma2(bc2(2.f), uC, sx)), r);
+        r = fma2(nhy, sub2(euv_n, euv_s), r);
+        r = fma2(bc2(-P.hzuv), sub2(euw_t, cy.euw), r);
+        if (CRF) r = fma2(bc2(-K.ucx), dx, r);
+        du = r;
     }
     {
-        const float sx = uxpB + uxmB, sy = uyp2 + uA, dx = uxpB - uxmB;
-        r = K.cxx * sx;
-        r = fmaf(K.cyy, sy, r);
-        r = fmaf(P.azp, uzpB, r);
-        r = fmaf(P.azm, uzmB, r);
-        r = fmaf(-P.ccuv, uB, r);
-        r = fmaf(-K.hx, dx * fmaf(2.f, uB, sx), r);
-        r = fmaf(-K.hy, euv_nB - euv_nA, r);
-        r = fmaf(-P.hzuv, euw_tB - cB.euw, r);
-        if (CRF) r = fmaf(-K.ucx, dx, r);
-        duB = r;
-    }
-    // v at A and B
-    {
-        const float sx = vxpA + vxmA, sy = vB + vym, dy = vB - vym;
-        r = K.cxx * sx;
-        r = fmaf(K.cyy, sy, r);
-        r = fmaf(P.azp, vzpA, r);
-        r = fmaf(P.azm, vzmA, r);
-        r = fmaf(-P.ccuv, vA, r);
-        r = fmaf(-K.hx, euv_nA - euv_wA, r);
-        r = fmaf(-K.hy, dy * fmaf(2.f, vA, sy), r);
-        r = fmaf(-P.hzuv, evw_tA - cA.evw, r);
-        if (CRF) r = fmaf(-K.ucx, vxpA - vxmA, r);
-        dvA = r;
+        const f2 sx = add2(vXP, vXM), sy = add2(vYP, vYM), dy = sub2(vYP, vYM);
+        r = mul2(cxx, sx);
+        r = fma2(cyy, sy, r);
+        r = fma2(bc2(P.azp), vZP, r);
+        r = fma2(bc2(P.azm), vZM, r);
+        r = fma2(bc2(-P.ccuv), vC, r);
+        r = fma2(nhx, sub2(euv_n, euv_w), r);
+        r = fma2(nhy, mul2(dy, fma2(bc2(2.f), vC, sy)), r);
+        r = fma2(bc2(-P.hzuv), sub2(evw_t, cy.evw), r);
+        if (CRF) r = fma2(bc2(-K.ucx), sub2(vXP, vXM), r);
+        dv = r;
     }
     {
-        const float sx = vxpB + vxmB, sy = vyp2 + vA, dy = vyp2 - vA;
-        r = K.cxx * sx;
-        r = fmaf(K.cyy, sy, r);
-        r = fmaf(P.azp, vzpB, r);
-        r = fmaf(P.azm, vzmB, r);
-        r = fmaf(-P.ccuv, vB, r);
-        r = fmaf(-K.hx, euv_nB - euv_wB, r);
-        r = fmaf(-K.hy, dy * fmaf(2.f, vB, sy), r);
-        r = fmaf(-P.hzuv, evw_tB - cB.evw, r);
-        if (CRF) r = fmaf(-K.ucx, vxpB - vxmB, r);
-        dvB = r;
+        const f2 sx = add2(wXP, wXM), sy = add2(wYP, wYM);
+        r = mul2(cxx, sx);
+        r = fma2(cyy, sy, r);
+        r = fma2(bc2(P.bzp), wZP, r);
+        r = fma2(bc2(P.bzm), wZM, r);
+        r = fma2(bc2(-P.ccw), wC, r);
+        r = fma2(nhx, sub2(euw_t, euw_w), r);
+        r = fma2(nhy, sub2(evw_t, evw_s), r);
+        r = fma2(bc2(-P.hzw), sub2(cw_t, cy.cw), r);
+        if (CRF) r = fma2(bc2(-K.ucx), sub2(wXP, wXM), r);
+        dw = r;
     }
-    // w at A and B
-    {
-        const float sx = wxpA + wxmA, sy = wB + wym;
-        r = K.cxx * sx;
-        r = fmaf(K.cyy, sy, r);
-        r = fmaf(P.bzp, wzpA, r);
-        r = fmaf(P.bzm, wzmA, r);
-        r = fmaf(-P.ccw, wA, r);
-        r = fmaf(-K.hx, euw_tA - euw_wA, r);
-        r = fmaf(-K.hy, evw_tA - evw_sA, r);
-        r = fmaf(-P.hzw, cw_tA - cA.cw, r);
-        if (CRF) r = fmaf(-K.ucx, wxpA - wxmA, r);
-        dwA = r;
-    }
-    {
-        const float sx = wxpB + wxmB, sy = wyp2 + wA;
-        r = K.cxx * sx;
-        r = fmaf(K.cyy, sy, r);
-        r = fmaf(P.bzp, wzpB, r);
-        r = fmaf(P.bzm, wzmB, r);
-        r = fmaf(-P.ccw, wB, r);
-        r = fmaf(-K.hx, euw_tB - euw_wB, r);
-        r = fmaf(-K.hy, evw_tB - evw_tA, r);
-        r = fmaf(-P.hzw, cw_tB - cB.cw, r);
-        if (CRF) r = fmaf(-K.ucx, wxpB - wxmB, r);
-        dwB = r;
-    }
-    cA.euw = euw_tA;
-    cA.evw = evw_tA;
-    cA.cw = cw_tA;
-    cB.euw = euw_tB;
-    cB.evw = evw_tB;
-    cB.cw = cw_tB;
+    cy.euw = euw_t;
+    cy.evw = evw_t;
+    cy.cw = cw_t;
 }
 } // namespace
 
@@ -328,57 +298,70 @@ __global__ void __launch_bounds__(MT, 2) k_rk_mixed(const double *__restrict__ u
     const size_t sk = (size_t)p.nx * p.ny;
     const int tid = lane + MX * wid;
 
-    // Ring-plane loads (36 x 20 of u, v, w): 1080 aligned pairs of doubles
-    // per plane, pair q = t + 256 s of thread t (s < 5; the fifth only for
-    // t < 56), pair q = field f, row r, x pair c (q = 360 f + 18 r + c).  Each
-    // pair is one 16-byte copy (cp.async.cg: L2 only, no L1 pollution) into
-    // the FP64 staging slot, and one 16-byte shared load, two conversions and
-    // an 8-byte store into the FP32 ring, at the same offset within the slot.
-    // The pair's global source (periodic in x and y; a pair never straddles
-    // the wrap, nx being even) and offset are fixed for the whole march.
+    // Ring-plane loads (36 x 20 of u, v, w): 360 aligned pairs of doubles
+    // per field and plane, pair q = row r, x pair c (q = 18 r + c); thread t
+    // copies pair t of every field and, for t >= 152, pair t + 104 (warps
+    // 0-3 carry the halo stencil instead).  Each pair is one 16-byte copy
+    // (cp.async.cg: L2 only, no L1 pollution) into the FP64 staging slot, and
+    // one 16-byte shared load, two conversions and an 8-byte store into the
+    // FP32 ring, at the same offset within the slot.  The pair's position in
+    // the plane (periodic in x and y; a pair never straddles the wrap, nx
+    // being even) and in the slot are the same for the three fields and fixed
+    // for the whole march.
     static_assert(MX == 32 && MY == 16 && MW == 36 && MH == 20, "pair maps of the 32 x 16 tile");
-    constexpr int NPAIR = 3 * MH * (MW / 2); // 1080
-    const double *src[5];
-    int pk[5]; // offset of the pair in a staging slot and in a ring slot
+    constexpr int FPAIR = MH * (MW / 2), PAIR2 = MT - (FPAIR - MT); // 360 pairs per field; 152
+    int soff[2], pk[2]; // the pair's element offset in a plane and its offset in a ring field
 #pragma unroll
-    for (int sl = 0; sl < 5; sl++) {
-        int q = tid + MT * sl;
-        if (q >= NPAIR) q = 0; // unused slot (sl = 4, tid >= 56)
-        const int fld = q / 360, r = (q % 360) / 18, c = q % 18;
+    for (int h = 0; h < 2; h++) {
+        const int q = h == 0 ? tid : (tid >= PAIR2 ? tid + (FPAIR - MT) : 0);
+        const int r = q / 18, c = q % 18;
         int gx = i0 - 2 + 2 * c, gy = j0 - 2 + r;
         gx += (gx < 0) ? p.nx : 0;
         gx -= (gx >= p.nx) ? p.nx : 0;
         gy += (gy < 0) ? p.ny : 0;
         gy -= (gy >= p.ny) ? p.ny : 0;
-        src[sl] = (fld == 0 ? u : (fld == 1 ? v : w)) + (size_t)gy * p.nx + gx;
-        pk[sl] = fld * MPS + r * MW + 2 * c;
+        soff[h] = gy * p.nx + gx;
+        pk[h] = r * MW + 2 * c;
     }
-    const bool pv4 = tid + MT * 4 < NPAIR;
+    const bool pv2 = tid >= PAIR2;
 
-    // copy u, v, w plane kq (in [0, nz+1]; none past last) into its staging
-    // slot; one commit group per call, empty or not, so the wait counts stay
-    // uniform
-    auto issue = [&](int kq, int last) {
+    // Slots: plane k of the march sits in slot (k - mstart + 1) % 3 of the
+    // staging ring and of both FP32 rings, so that with the march unrolled by
+    // three every slot is a compile-time constant and every ring access one
+    // per-thread base address plus an immediate offset.
+    // copy u, v, w plane kq (in [-1, nz+2]; none past last) into staging
+    // slot `slot`; one commit group per call, empty or not, so the wait counts
+    // stay uniform
+    auto issue = [&](int kq, int last, int slot) {
         if (kq <= last) {
             const long long off = (long long)sk * kq; // kq >= -1 (a slab's lower halo)
-            double *d = stg + ((kq + NSTG) % NSTG) * SST;
+            double *d = stg + slot * SST;
 #pragma unroll
-            for (int sl = 0; sl < 5; sl++)
-                if (sl < 4 || pv4) cp_async_16(d + pk[sl], src[sl] + off);
+            for (int h = 0; h < 2; h++) {
+                if (h == 0 || pv2) {
+                    const long long o = off + soff[h];
+                    cp_async_16(d + pk[h], u + o);
+                    cp_async_16(d + FST + pk[h], v + o);
+                    cp_async_16(d + 2 * FST + pk[h], w + o);
+                }
+            }
         }
         cp_async_commit();
     };
 
-    // staged plane kq (every thread's copies landed and a barrier passed) ->
+    // staging slot s (every thread's copies landed and a barrier passed) ->
     // FP32 ring slot s
-    auto convert = [&](int kq, int s) {
-        const double *d = stg + ((kq + NSTG) % NSTG) * SST;
+    auto convert = [&](int s) {
+        const double *d = stg + s * SST;
         float *o = ur + s * SST;
 #pragma unroll
-        for (int sl = 0; sl < 5; sl++) {
-            if (sl < 4 || pv4) {
-                const double2 x = *reinterpret_cast<const double2 *>(d + pk[sl]);
-                *reinterpret_cast<float2 *>(o + pk[sl]) = make_float2((float)x.x, (float)x.y);
+        for (int h = 0; h < 2; h++) {
+            if (h == 0 || pv2) {
+#pragma unroll
+                for (int f = 0; f < 3; f++) {
+                    const double2 x = *reinterpret_cast<const double2 *>(d + f * FST + pk[h]);
+                    *reinterpret_cast<float2 *>(o + f * FST + pk[h]) = make_float2((float)x.x, (float)x.y);
+                }
             }
         }
     };
@@ -403,12 +386,12 @@ __global__ void __launch_bounds__(MT, 2) k_rk_mixed(const double *__restrict__ u
     const int gxp = (gi == p.nx - 1) ? 0 : gi + 1, gjB2 = (gjA + 2 >= p.ny) ? gjA + 2 - p.ny : gjA + 2;
     const size_t gA = (size_t)gi + (size_t)p.nx * gjA;
 
-    // stage 1 runs one plane beyond the chunk, but not on a wall plane
-    // (whose u1 is the wall fill); at a slab interface it runs on the halo
-    const int mstart = max(kbeg - 1, p.wlo ? 1 : 0), mend = min(kend + 1, p.whi ? p.nz : p.nz + 1);
-    const int last = mend + 1; // the last u plane the march reads
-    // ring slot of plane k: (k + 3) % 3 (k >= -1 at a slab interface)
-    int sa = (mstart - 1 + MNS) % MNS, sb = mstart % MNS, sc = (mstart + 1) % MNS;
+    // stage 1 runs one plane beyond the chunk, but not on a wall plane:
+    // under the top wall the march's step at nz+1 forms the wall plane of u1
+    // instead; at a slab interface stage 1 runs on the halo
+    const int mstart = max(kbeg - 1, p.wlo ? 1 : 0), mend = min(kend + 1, p.nz + 1);
+    const bool wall_step = p.whi && mend == p.nz + 1;
+    const int last = wall_step ? p.nz + 1 : mend + 1; // the last u plane the march reads
     {
         const int k0 = max(kbeg - 2, p.wlo ? 0 : -1), np = min(kbeg + kchunk + 1, p.nz + (p.whi ? 1 : 2)) - k0 + 1;
         for (int q = tid; q < 3 * np; q += MT) ptab[q] = __ldg(tab + 3 * k0 + q);
@@ -418,31 +401,35 @@ __global__ void __launch_bounds__(MT, 2) k_rk_mixed(const double *__restrict__ u
     }
     // a plane is issued two iterations before its conversion at the end of
     // an iteration
-    issue(mstart - 1, last);
-    issue(mstart, last);
-    issue(mstart + 1, last);
+    issue(mstart - 1, last, 0);
+    issue(mstart, last, 1);
+    issue(mstart + 1, last, 2);
     cp_async_wait<0>();
     __syncthreads();
-    convert(mstart - 1, sa);
-    convert(mstart, sb);
-    convert(mstart + 1, sc);
+    convert(0);
+    convert(1);
+    convert(2);
     __syncthreads();
-    issue(mstart + 2, last); // into the staging slots of mstart - 1 and mstart, converted above
-    issue(mstart + 3, last);
+    issue(mstart + 2, last, 0); // into the staging slots of mstart - 1 and mstart, converted above
+    issue(mstart + 3, last, 1);
     cp_async_wait<1>(); // plane mstart + 2 landed; the barrier below publishes it
     __syncthreads();
 
     // bottom fluxes of the first stage-1 plane (the top fluxes of mstart - 1)
     const Carry zero = {0.f, 0.f, 0.f};
-    Carry cA, cB, cH, c2A = zero, c2B = zero;
+    auto pair = [](const Carry &x, const Carry &y) {
+        return Carry2{make_float2(x.euw, y.euw), make_float2(x.evw, y.evw), make_float2(x.cw, y.cw)};
+    };
+    Carry cH;
+    Carry2 c1, c2 = pair(zero, zero);
     {
         const MxPlane Pm = mx_plane(ptab, mstart - 1);
-        cA = mx_top(ur, sa * SST + hxy0, sb * SST + hxy0, Pm.a, Pm.b);
-        cB = mx_top(ur, sa * SST + hxy0 + MW, sb * SST + hxy0 + MW, Pm.a, Pm.b);
-        cH = hval1 ? mx_top(ur, sa * SST + hxy1, sb * SST + hxy1, Pm.a, Pm.b) : zero;
+        c1 = pair(mx_top(ur, hxy0, SST + hxy0, Pm.a, Pm.b), mx_top(ur, hxy0 + MW, SST + hxy0 + MW, Pm.a, Pm.b));
+        cH = hval1 ? mx_top(ur, hxy1, SST + hxy1, Pm.a, Pm.b) : zero;
     }
-    // d1 of the own pair at plane mq (this iteration) and at mq - 1
-    float d1[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, e1[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    // d1 of the own pair (u, v, w; .x point A, .y point B) at plane mq (this
+    // iteration) and at mq - 1
+    f2 d1[3] = {bc2(0.f), bc2(0.f), bc2(0.f)}, e1[3] = {bc2(0.f), bc2(0.f), bc2(0.f)};
     bool first2 = true;
     double su = 0.0;
     const float bcu2 = (float)(2.0 * (0.0 - p.u_crf));
@@ -478,40 +465,52 @@ __global__ void __launch_bounds__(MT, 2) k_rk_mixed(const double *__restrict__ u
         return c;
     };
 
+    // the pressure-prediction lines of centre(kq) into L1 ahead of their
+    // loads, which follow the barrier (a prefetch holds no registers)
+    auto pf = [](const void *a) { asm volatile("prefetch.global.L1 [%0];" ::"l"(a)); };
+    auto prefetch = [&](int kq) {
+        if (pinc) {
+            const size_t pl = sk * (kq - 1);
+            const size_t rowA = (size_t)p.nx * gjA + pl, rowB = rowA + p.nx, rowB2 = (size_t)p.nx * gjB2 + pl;
+            pf(pq + rowA + gi);
+            pf(pq + rowB + gi);
+            pf(pq + rowA + gxp);
+            pf(pq + rowB + gxp);
+            pf(pq + rowB2 + gi);
+            if (kq < p.nz) {
+                pf(pq + rowA + sk + gi);
+                pf(pq + rowB + sk + gi);
+            }
+        }
+    };
+
     // stage 2 at interior plane kq from the stage-1 planes kq-1 (sm), kq (s0),
-    // kq+1 (sp); e: the pair's d1 at kq (uA, vA, wA, uB, vB, wB)
-    auto stage2 = [&](int kq, int sm, int s0, int sp, const float *e, const Centre &cv) {
+    // kq+1 (sp); e: the pair's d1 at kq
+    auto stage2 = [&](int kq, int sm, int s0, int sp, const f2 *e, const Centre &cv) {
         const MxPlane P = mx_plane(ptab, kq);
         if (first2) { // bottom fluxes of u1 at kq: the top fluxes of plane kq - 1
             const MxPlane Pm = mx_plane(ptab, kq - 1);
-            c2A = mx_top(sr, sm * SST + hxy0, s0 * SST + hxy0, Pm.a, Pm.b);
-            c2B = mx_top(sr, sm * SST + hxy0 + MW, s0 * SST + hxy0 + MW, Pm.a, Pm.b);
+            c2 = pair(mx_top(sr, sm * SST + hxy0, s0 * SST + hxy0, Pm.a, Pm.b),
+                      mx_top(sr, sm * SST + hxy0 + MW, s0 * SST + hxy0 + MW, Pm.a, Pm.b));
             first2 = false;
         }
-        float d[6];
-        mx_rhs2<CRF>(sr, sm * SST + hxy0, s0 * SST + hxy0, sp * SST + hxy0, P, K, c2A, c2B, d[0], d[1], d[2], d[3],
-                     d[4], d[5]);
-        float iu[2], iv[2], iw[2];
-#pragma unroll
-        for (int q = 0; q < 2; q++) {
-            iu[q] = 0.5f * (e[3 * q] + d[3 * q]);
-            iv[q] = 0.5f * (e[3 * q + 1] + d[3 * q + 1]);
-            iw[q] = 0.5f * (e[3 * q + 2] + d[3 * q + 2]);
-        }
+        f2 d[3];
+        mx_rhs2<CRF>(sr, sm * SST + hxy0, s0 * SST + hxy0, sp * SST + hxy0, P, K, c2, d[0], d[1], d[2]);
+        const f2 half = bc2(0.5f);
+        f2 iu = mul2(half, add2(e[0], d[0])), iv = mul2(half, add2(e[1], d[1])), iw = mul2(half, add2(e[2], d[2]));
         if (pinc) {
-            iu[0] = fmaf(-K.gx, cv.qxA - cv.qA, iu[0]);
-            iu[1] = fmaf(-K.gx, cv.qxB - cv.qB, iu[1]);
-            iv[0] = fmaf(-K.gy, cv.qB - cv.qA, iv[0]);
-            iv[1] = fmaf(-K.gy, cv.qyB - cv.qB, iv[1]);
-            iw[0] = fmaf(-P.gz, cv.qzA - cv.qA, iw[0]);
-            iw[1] = fmaf(-P.gz, cv.qzB - cv.qB, iw[1]);
+            const f2 q = make_float2(cv.qA, cv.qB);
+            iu = fma2(bc2(-K.gx), sub2(make_float2(cv.qxA, cv.qxB), q), iu);
+            iv = fma2(bc2(-K.gy), sub2(make_float2(cv.qB, cv.qyB), q), iv);
+            iw = fma2(bc2(-P.gz), sub2(make_float2(cv.qzA, cv.qzB), q), iw);
         }
         const size_t g = gA + sk * kq;
         const double zl = pzl[kq];
 #pragma unroll
         for (int q = 0; q < 2; q++) {
             const size_t gq = g + (size_t)q * p.nx;
-            const double nu = cv.u[q] + (double)iu[q], nv = cv.v[q] + (double)iv[q], nw = cv.w[q] + (double)iw[q];
+            const double nu = cv.u[q] + (double)(q ? iu.y : iu.x), nv = cv.v[q] + (double)(q ? iv.y : iv.x),
+                         nw = cv.w[q] + (double)(q ? iw.y : iw.x);
             uo[gq] = nu;
             vo[gq] = nv;
             if (kq != p.nz || !p.whi) wo[gq] = nw;
@@ -540,20 +539,26 @@ __global__ void __launch_bounds__(MT, 2) k_rk_mixed(const double *__restrict__ u
     };
 
     // Two barriers per plane: stage 1 at plane mq reads u planes mq-1..mq+1
-    // and writes u1 plane mq; then stage 2 at mq-1 reads u1 planes mq-2..mq,
+    // and writes u1 plane mq (under the top wall, at mq = nz+1, the wall
+    // plane of u1 instead); then stage 2 at mq-1 reads u1 planes mq-2..mq,
     // and the staged u plane mq+2 is converted into the slot of plane mq-1.
-    for (int mq = mstart; mq <= mend; mq++) {
+    // PH = (mq - mstart) % 3: planes mq-1, mq, mq+1 in slots sa, sb, sc.
+    auto march = [&](auto PH, int mq) {
+        constexpr int sa = decltype(PH)::value, sb = (sa + 1) % MNS, sc = (sa + 2) % MNS;
         const bool do2 = (mq - 1 >= kbeg && mq - 1 <= kend);
-        Centre cv;
-        if (do2) cv = centre(mq - 1); // in flight during stage 1
-        {
+        if (do2) prefetch(mq - 1);
+        if (wall_step && mq == p.nz + 1) {
+            // imposeNoSlipBC on u1 at the top wall, from u1 plane nz (slot sa)
+            top1(sb, sa, hxy0);
+            top1(sb, sa, hxy0 + MW);
+            if (hval1) top1(sb, sa, hxy1);
+        } else {
             const MxPlane P = mx_plane(ptab, mq);
             const bool top = p.whi && mq == p.nz, bottom = p.wlo && mq == 1;
-            mx_rhs2<CRF>(ur, sa * SST + hxy0, sb * SST + hxy0, sc * SST + hxy0, P, K, cA, cB, d1[0], d1[1], d1[2],
-                         d1[3], d1[4], d1[5]);
-            if (top) d1[2] = d1[5] = 0.f; // w1(nz) = 0, the wall
-            put1(sb, sa, hxy0, d1[0], d1[1], d1[2], bottom);
-            put1(sb, sa, hxy0 + MW, d1[3], d1[4], d1[5], bottom);
+            mx_rhs2<CRF>(ur, sa * SST + hxy0, sb * SST + hxy0, sc * SST + hxy0, P, K, c1, d1[0], d1[1], d1[2]);
+            if (top) d1[2] = bc2(0.f); // w1(nz) = 0, the wall
+            put1(sb, sa, hxy0, d1[0].x, d1[1].x, d1[2].x, bottom);
+            put1(sb, sa, hxy0 + MW, d1[0].y, d1[1].y, d1[2].y, bottom);
             if (hval1) {
                 float du, dv, dw;
                 mx_rhs<CRF>(ur, sa * SST + hxy1, sb * SST + hxy1, sc * SST + hxy1, P, K, cH, du, dv, dw);
@@ -563,30 +568,24 @@ __global__ void __launch_bounds__(MT, 2) k_rk_mixed(const double *__restrict__ u
         }
         __syncthreads();
         // plane mq-2 sits in slot sc
-        if (do2) stage2(mq - 1, sc, sa, sb, e1, cv);
-        if (p.whi && mq == p.nz) {
-            // the top wall plane of u1 takes the slot of plane nz-2, which
-            // stage 2 at nz-1 has just consumed
-            __syncthreads();
-            top1(sc, sb, hxy0);
-            top1(sc, sb, hxy0 + MW);
-            if (hval1) top1(sc, sb, hxy1);
-            __syncthreads();
-            if (p.nz >= kbeg && p.nz <= kend) stage2(p.nz, sa, sb, sc, d1, centre(p.nz));
-        }
+        if (do2) stage2(mq - 1, sc, sa, sb, e1, centre(mq - 1));
         // staged plane mq+2 (landed and published by the last iteration's
-        // wait and barrier) into the FP32 slot of plane mq-1
-        // ((mq + 2) % 3 == (mq - 1) % 3), which stage 1 above has finished with
-        if (mq + 2 <= last) convert(mq + 2, sa);
-        issue(mq + 4, last); // into the staging slot of plane mq + 1, converted last iteration
-        cp_async_wait<1>();  // plane mq + 3 landed (mq + 4 may be in flight)
+        // wait and barrier; its staging slot is sa) into the FP32 slot of
+        // plane mq-1, which stage 1 above has finished with
+        if (mq + 2 <= last) convert(sa);
+        issue(mq + 4, last, sc); // into the staging slot of plane mq + 1, converted last iteration
+        cp_async_wait<1>();      // plane mq + 3 landed (mq + 4 may be in flight)
 #pragma unroll
-        for (int q = 0; q < 6; q++) e1[q] = d1[q];
-        const int st = sa;
-        sa = sb;
-        sb = sc;
-        sc = st;
+        for (int q = 0; q < 3; q++) e1[q] = d1[q];
         __syncthreads();
+    };
+    for (int mq = mstart;;) {
+        march(std::integral_constant<int, 0>{}, mq);
+        if (++mq > mend) break;
+        march(std::integral_constant<int, 1>{}, mq);
+        if (++mq > mend) break;
+        march(std::integral_constant<int, 2>{}, mq);
+        if (++mq > mend) break;
     }
     cp_async_wait<0>();
     mean_reduce(su, red);

@@ -27,7 +27,7 @@ struct StepParams {
 // Reduction scratch: per-block partial results and the final scalars.
 struct ReduceBuf {
     double *partial = nullptr; // >= max blocks * 3
-    double *scalar = nullptr;  // [0..2] component means, [3..5] forcing shift
+    double *scalar = nullptr;  // [0..2] component means, [3..5] forcing shift, [6] u's plane-weighted sum
     int max_blocks = 0;
 };
 
@@ -51,7 +51,7 @@ int launch_force_fp64(double *u, double *v, double *w, const StepParams &p, cons
 struct MeanState {
     double *partial = nullptr;       // >= max_blocks
     unsigned int *counter = nullptr; // zero-initialised once
-    double *scalar = nullptr;        // >= 4
+    double *scalar = nullptr;        // >= 7 (as ReduceBuf::scalar)
     int max_blocks = 0;
     double vel_force = 0.0;
 };
