@@ -208,6 +208,15 @@ __device__ __forceinline__ void pressure_update(const PressureUpdate &pu, size_t
     pu.p[o] = pn;
 }
 
+// the same from the staged prediction q and old pressure pold of point o
+__device__ __forceinline__ void pressure_update_staged(const PressureUpdate &pu, size_t o, float dp, float q,
+                                                       float pold)
+{
+    const float pn = (pu.incremental ? q : 0.f) + dp;
+    pu.qnext[o] = pu.qmode ? 2.f * pn - pold : pn;
+    pu.p[o] = pn;
+}
+
 __global__ void __launch_bounds__(256) k_pressure_update(const float *__restrict__ dp, PressureUpdate pu, size_t n)
 {
     for (size_t o = (size_t)blockIdx.x * 256 + threadIdx.x; o < n; o += (size_t)gridDim.x * 256)
@@ -244,17 +253,28 @@ template <typename T, int N> __host__ __device__ constexpr int pf_x_smem_elems()
     using V = typename cplx_of<T>::type;
     return (fpad_elems<V>(pf_x_lines<T, N>() * N) + 1) / 2 * 2 + pf_x_lines<T, N>() * N + N;
 }
+// ... and with the mixed pressure update fused (FP32 inverse): the group's
+// rows of the prediction q and of the old pressure, staged (bytes)
+template <typename T, int N> __host__ __device__ constexpr int pf_x_pu_bytes()
+{
+    return 2 * 2 * pf_x_lines<T, N>() * N * 4;
+}
 template <typename T, int N> __host__ __device__ constexpr int pf_y_smem_elems()
 {
     using V = typename cplx_of<T>::type;
     return (fpad_elems<V>(pf_y_cols<V, N>() * N) + 1) / 2 * 2 + pf_y_cols<V, N>() * N + N;
 }
 
-template <typename T, int N, bool FWD>
+// PU (FP32 inverse only): the pressure update of the mixed path is fused
+// into the last stage; the group's rows of q and of the old pressure are
+// copied into shared memory when the group starts, so their latency hides
+// behind its butterflies instead of sitting in the epilogue.
+template <typename T, int N, bool FWD, bool PU = false>
 __global__ void __launch_bounds__(pf_x_threads<T>()) k_xfft_pf(const T *__restrict__ in, T *__restrict__ out,
                                                                const typename cplx_of<T>::type *__restrict__ twg,
                                                                int ny, int total, T scale, PressureUpdate pu)
 {
+    static_assert(!PU || (sizeof(T) == 4 && !FWD), "the fused pressure update is the FP32 inverse's");
     using V = typename cplx_of<T>::type;
     constexpr int NT = pf_x_threads<T>();
     constexpr int NB = pf_x_lines<T, N>(), BUF = (fpad_elems<V>(NB * N) + 1) / 2 * 2;
@@ -263,9 +283,20 @@ __global__ void __launch_bounds__(pf_x_threads<T>()) k_xfft_pf(const T *__restri
     V *buf = reinterpret_cast<V *>(smem_raw);
     T *stage = reinterpret_cast<T *>(buf + BUF); // 2 NB rows of N values, 16-byte aligned
     V *tw = reinterpret_cast<V *>(stage + 2 * NB * N);
+    float *pst = reinterpret_cast<float *>(tw + N); // PU: [2][2 NB N], q then the old pressure
     const int tid = threadIdx.x;
     const int gpk = (ny / 2 + NB - 1) / NB; // groups per k-plane
     ct_build_twiddles<V, N, NT>(twg, tw, tid);
+    // PU: the group's rows of q and p (the run the group writes), one commit group
+    auto fetch_pu = [&](int g) {
+        const int k = g / gpk, p0 = (g % gpk) * NB, cnt = min(NB, ny / 2 - p0) * 2 * N;
+        const size_t o = (size_t)k * N * ny + (size_t)2 * p0 * N;
+        for (int e = tid * 4; e < cnt; e += NT * 4) {
+            if (pu.incremental) cp_async_16(pst + e, pu.q + o + e);
+            cp_async_16(pst + 2 * NB * N + e, pu.p + o + e);
+        }
+        cp_async_commit();
+    };
     // rows 2 p0 .. 2 p0 + 2 nb - 1 of plane k are one contiguous run
     auto fetch = [&](int g) {
         const int k = g / gpk, p0 = (g % gpk) * NB, cnt = min(NB, ny / 2 - p0) * 2 * N;
@@ -278,7 +309,8 @@ __global__ void __launch_bounds__(pf_x_threads<T>()) k_xfft_pf(const T *__restri
         const int tid = opaque_tid();
         const int k = g / gpk, p0 = (g % gpk) * NB, nb = min(NB, ny / 2 - p0);
         cp_async_wait<0>(); // this thread's copies of group g have landed
-        __syncthreads();    // ... and everyone's; the previous group is done with buf
+        __syncthreads();    // ... and everyone's; the previous group is done with buf (and pst)
+        if (PU) fetch_pu(g);
         // first stage straight from the staged rows: line b pairs rows 2b, 2b+1
         auto in = [&](int b, int m) {
             const T *r0 = stage + 2 * b * N, *r1 = r0 + N;
@@ -299,7 +331,10 @@ __global__ void __launch_bounds__(pf_x_threads<T>()) k_xfft_pf(const T *__restri
         };
         ct_first_stage<V, FWD, false, N, NB, 1, N, NT>(buf, nb, in, tid);
         __syncthreads();
-        if (g + (int)gridDim.x < total) fetch(g + gridDim.x);
+        if (g + (int)gridDim.x < total)
+            fetch(g + gridDim.x);
+        else if (PU)
+            cp_async_commit(); // one group after fetch_pu(g), as in the other rounds
         T *dst = out + (size_t)k * N * ny + (size_t)2 * p0 * N;
         if constexpr (FWD) {
             ct_batch_ip<V, FWD, false, N, NB, 1, N, NT, 1, ct_nstages(N) - 1>(buf, nb, tw, tid);
@@ -312,15 +347,20 @@ __global__ void __launch_bounds__(pf_x_threads<T>()) k_xfft_pf(const T *__restri
             ct_last_stage_pairs<V, FWD, false, N, NB, 1, N, NT>(buf, nb, tw, tid, put);
         } else {
             ct_batch_ip<V, FWD, false, N, NB, 1, N, NT, 1, ct_nstages(N) - 1>(buf, nb, tw, tid);
+            if (PU) {
+                cp_async_wait<1>(); // fetch_pu(g) landed (the next group's fetch may be in flight)
+                __syncthreads();
+            }
             // the last stage writes the two real rows of line b from registers
             auto put = [&](int b, int m, V z) {
                 const T d0 = z.x * scale, d1 = z.y * scale;
                 dst[(size_t)2 * b * N + m] = d0; // mixed: the increment itself, for the correction
                 dst[(size_t)(2 * b + 1) * N + m] = d1;
-                if (sizeof(T) == 4 && pu.p) {
-                    const size_t o = (size_t)k * N * ny + (size_t)2 * p0 * N + (size_t)2 * b * N + m;
-                    pressure_update(pu, o, (float)d0);
-                    pressure_update(pu, o + N, (float)d1);
+                if (PU) {
+                    const int r = 2 * b * N + m;
+                    const size_t o = (size_t)k * N * ny + (size_t)2 * p0 * N + r;
+                    pressure_update_staged(pu, o, (float)d0, pst[r], pst[2 * NB * N + r]);
+                    pressure_update_staged(pu, o + N, (float)d1, pst[r + N], pst[2 * NB * N + r + N]);
                 }
             };
             ct_last_stage<V, FWD, false, N, NB, 1, N, NT>(buf, nb, tw, tid, put);
@@ -330,7 +370,11 @@ __global__ void __launch_bounds__(pf_x_threads<T>()) k_xfft_pf(const T *__restri
 }
 
 template <typename T, int N, bool FWD>
-__global__ void __launch_bounds__(pf_y_threads<T>()) k_yfft_pf(T *__restrict__ data, const typename cplx_of<T>::type *__restrict__ twg,
+// CTAs per SM the register budget is cut for: up to 80 registers for FP32
+// lines up to 512 (three CTAs), 128 for FP64 ones (two); longer lines keep
+// more registers rather than spill
+__global__ void __launch_bounds__(pf_y_threads<T>(), sizeof(T) == 4 ? (N <= 512 ? 3 : 2) : (N <= 512 ? 2 : 1))
+    k_yfft_pf(T *__restrict__ data, const typename cplx_of<T>::type *__restrict__ twg,
                                                  int nx, int total)
 {
     using V = typename cplx_of<T>::type;
@@ -347,13 +391,25 @@ __global__ void __launch_bounds__(pf_y_threads<T>()) k_yfft_pf(T *__restrict__ d
     auto fetch = [&](int g) {
         const int k = g / gpk, c0 = (g % gpk) * W, nb = min(W, ncol - c0);
         const V *plane = reinterpret_cast<const V *>(data) + (size_t)k * N * ncol;
-        for (int e = tid; e < RAW; e += NT) {
-            const int c = e % W, m = e / W;
-            if (c < nb) {
-                if (sizeof(V) == 16)
+        if (sizeof(V) == 8 && W % 2 == 0 && ncol % 2 == 0) {
+            // FP32: two columns per 16-byte copy (c0 and c even, rows of even
+            // length: 16-byte aligned); a lone last column takes an 8-byte one
+            for (int e = 2 * tid; e < RAW; e += 2 * NT) {
+                const int c = e % W, m = e / W;
+                if (c + 1 < nb)
                     cp_async_16(stage + e, plane + (size_t)m * ncol + c0 + c);
-                else
+                else if (c < nb)
                     cp_async_8(stage + e, plane + (size_t)m * ncol + c0 + c);
+            }
+        } else {
+            for (int e = tid; e < RAW; e += NT) {
+                const int c = e % W, m = e / W;
+                if (c < nb) {
+                    if (sizeof(V) == 16)
+                        cp_async_16(stage + e, plane + (size_t)m * ncol + c0 + c);
+                    else
+                        cp_async_8(stage + e, plane + (size_t)m * ncol + c0 + c);
+                }
             }
         }
         cp_async_commit();
@@ -1221,15 +1277,27 @@ static int launch_x_ct(const Ppe *s, const T *in, size_t in_off, size_t in_sj, s
     if (aligned && in_off == 0 && out_off == 0 && in_sj == (size_t)N && out_sj == (size_t)N && in_sk == sk &&
         out_sk == sk) {
         constexpr int NT = pf_x_threads<T>(), NBP = pf_x_lines<T, N>();
+        const int total = ((s->ny / 2 + NBP - 1) / NBP) * s->nz;
+        if constexpr (sizeof(T) == 4 && !FWD) {
+            if (pu != nullptr) {
+                const size_t shmp = sizeof(V) * (size_t)pf_x_smem_elems<T, N>() + pf_x_pu_bytes<T, N>();
+                auto kern = k_xfft_pf<T, N, false, true>;
+                if (shmp > 48 * 1024)
+                    PL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmp));
+                kern<<<persistent_grid(kern, shmp, total, NT), NT, shmp, st>>>(in, out, tw, s->ny, total, scale, *pu);
+                PL_CHECK_LAUNCH();
+                *fused = true;
+                return 0;
+            }
+        }
         const size_t shmp = sizeof(V) * (size_t)pf_x_smem_elems<T, N>();
         if (shmp > 48 * 1024)
             PL_CUDA_TRY(
                 cudaFuncSetAttribute(k_xfft_pf<T, N, FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmp));
-        const int total = ((s->ny / 2 + NBP - 1) / NBP) * s->nz;
         k_xfft_pf<T, N, FWD><<<persistent_grid(k_xfft_pf<T, N, FWD>, shmp, total, NT), NT, shmp, st>>>(
-            in, out, tw, s->ny, total, scale, (pu && !FWD) ? *pu : PressureUpdate{});
+            in, out, tw, s->ny, total, scale, PressureUpdate{});
         PL_CHECK_LAUNCH();
-        *fused = (pu != nullptr) && !FWD;
+        *fused = false;
         return 0;
     }
     if (shm > 48 * 1024)
