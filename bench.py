@@ -37,9 +37,27 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 NX, NY, NZ = 512, 384, 256
-RE_TAU, STRETCH, SEED, NOISE, DT = 1000.0, 2.0, 11, 0.1, 1e-4
+RE_TAU, STRETCH, SEED, NOISE, DT, PARTS = 1000.0, 2.0, 11, 0.1, 1e-4, 0
 METRIC = "RK2 steps/s @512x384x256: mixed vs FP64 on same GPU at rel err<=1e-5"
 WORKLOAD = "channel 512x384x256, Re_tau 1000, tanh stretch 2.0, Thomas, dt 1e-4, seed 11, noise 0.1"
+
+# the benchmark configurations (grid, Re_tau, tanh stretch, PDD partitions
+# (0 = Thomas), seed, perturbation); C3 is the workload of the headline line
+CONFIGS = {
+    "C1": ((64, 64, 64), 180.0, 1.5, 0, 42, 0.1),
+    "C2": ((256, 192, 128), 550.0, 1.8, 4, 7, 0.05),
+    "C3": ((512, 384, 256), 1000.0, 2.0, 0, 11, 0.1),
+    "C4": ((1024, 768, 512), 2000.0, 2.0, 8, 11, 0.1),
+}
+
+
+def set_config(name):
+    global NX, NY, NZ, RE_TAU, STRETCH, PARTS, SEED, NOISE, METRIC, WORKLOAD
+    (NX, NY, NZ), RE_TAU, STRETCH, PARTS, SEED, NOISE = CONFIGS[name]
+    grid = f"{NX}x{NY}x{NZ}"
+    METRIC = METRIC.replace("512x384x256", grid)
+    WORKLOAD = (f"channel {grid}, Re_tau {RE_TAU:g}, tanh stretch {STRETCH:g}, "
+                f"{'PDD over %d partitions' % PARTS if PARTS else 'Thomas'}, dt {DT:g}, seed {SEED}, noise {NOISE:g}")
 
 # algorithmic bytes per grid point per launch slot, by kernel and path: the
 # compulsory field passes (reads + writes of whole fields at their storage
@@ -59,7 +77,9 @@ ALG_BYTES = {
 # u_hat (FP64): 24 + 4 + 24; ppe_xfft_bwd reads the FP32 half-complex line and
 # writes the FP32 increment, plus the FP32 pressure update (reads the
 # prediction and p_n, writes p_n+1 and the next prediction): 4 + 4 + 16
-# kernel launches per step (this library's kernels only)
+# kernel launches per step (this library's kernels only), Thomas; PDD adds
+# the mixed path's widening of the FP32 right-hand side into the FP64 sweep
+# buffer (the FP64 path copies it with cudaMemcpyAsync)
 LAUNCHES = {"fp64": 7, "mixed": 8}
 
 
@@ -157,12 +177,13 @@ def cpu_reference_steps(nsteps_max, warmup, budget_s=150.0):
     g = O.Grid(NX, NY, NZ, stretch=STRETCH, re_tau=RE_TAU, dt=DT)
     u, v, w, p = g.init_flow(SEED, NOISE)
     u1, v1, w1 = g.zeros(), g.zeros(), g.zeros()
-    if O.ref_available():
+    if O.ref_available() and PARTS == 0:
         ppe = O.RefPPE(NX, NY, NZ, g.g.dx, g.g.dy, g.dzf_global)
         what = "reference C PPE (src/src_c built unmodified) + C restatement of the Fortran stencils"
     else:
-        ppe = O.PPE(NX, NY, NZ, g.g.dx, g.g.dy, g.dzf_global)
-        what = "C restatement of the PPE and of the Fortran stencils"
+        ppe = O.PPE(NX, NY, NZ, g.g.dx, g.g.dy, g.dzf_global, nparts=PARTS)
+        what = "C restatement of the PPE" + (f" (PDD, {PARTS} partitions)" if PARTS else "") + \
+               " and of the Fortran stencils"
     t0 = time.perf_counter()
     for _ in range(max(1, warmup)):
         g.step(ppe, u, v, w, u1, v1, w1, p)
@@ -326,7 +347,7 @@ def run_slabs(args, world, rank, local):
         line = {
             "metric": METRIC, "value": spsm, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": msm / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "mixed: f32 stencils/FFT, f64 u,v,w,p and tridiagonal",
+            "vs_baseline": None, "dtype": "mixed: f32 stencils/FFT/pressure state, f64 u,v,w and tridiagonal",
             "data": "synthetic",
             "config": {"workload": workload, "precision": "mixed", "grid": [NX, NY, nzg], "slab": [NX, NY, NZ],
                        "l2": "inputs larger than L2 (403 MB per FP64 field per GPU), no flush",
@@ -366,7 +387,8 @@ def run_b200(args):
     npts = NX * NY * NZ
 
     def measure(prec_name, prec):
-        cfg = plb.ChannelConfig(nx=NX, ny=NY, nz=NZ, stretch_ratio=STRETCH, re_tau=RE_TAU, dt=DT, precision=prec)
+        cfg = plb.ChannelConfig(nx=NX, ny=NY, nz=NZ, stretch_ratio=STRETCH, re_tau=RE_TAU, dt=DT, precision=prec,
+                                trid_parts=PARTS)
         ch = plb.Channel(cfg)
         ch.init_flow(SEED, NOISE)
         clocks = ClockSampler(local)
@@ -416,7 +438,7 @@ def run_b200(args):
     # in a subprocess on all host threads).  That oracle run is also the CPU
     # baseline: its steps after the first are the timed sample.
     acc, cpu = None, None
-    if rank == 0 and world == 1 and not args.no_accuracy:
+    if rank == 0 and world == 1 and not args.no_accuracy and (NX, NY, NZ, PARTS) == (512, 384, 256, 0):
         import tempfile
         from oracle import run_channel as R  # the checker and the CPU-baseline leg
         gpu_fields, gpu_div = {}, {}
@@ -458,20 +480,23 @@ def run_b200(args):
                    "sample": f"unavailable: {e}"}
 
     if rank == 0:
+        fbytes = NX * NY * (NZ + 2) * 8
         line = {
             "metric": METRIC, "value": spsm, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": msm / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "mixed: f32 stencils/FFT, f64 u,v,w,p and tridiagonal",
+            "vs_baseline": None, "dtype": "mixed: f32 stencils/FFT/pressure state, f64 u,v,w and tridiagonal",
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "precision": "mixed", "grid": [NX, NY, NZ],
-                       "l2": "inputs larger than L2 (403 MB per FP64 field), no flush",
-                       "parallelism": "1 GPU"},
+                       "l2": (f"inputs larger than L2 ({fbytes / 1e6:.0f} MB per FP64 field), no flush"
+                              if fbytes > 126e6 else
+                              f"{fbytes / 1e6:.1f} MB per FP64 field: the working set stays in L2 (no flush)"),
+                       "trid_parts": PARTS, "parallelism": "1 GPU"},
             "fp64_steps_per_s": sps64, "fp64_ms_per_step": ms64 / args.steps,
             "mixed_over_fp64": spsm / sps64,
             "accuracy_after_100_steps": acc,
             "clocks": clkm, "clocks_fp64": clk64,
             "e2e": {"value": e2e_sps, "unit": "steps/s", "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
-            "gpu_launches": LAUNCHES["mixed"] * args.steps,
+            "gpu_launches": (LAUNCHES["mixed"] + (1 if PARTS else 0)) * args.steps,
             "roofline": {"bound": "hbm", "kernel": top[0], "achieved": round(achieved, 1), "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                          "traffic": traffic, "alg_bytes": alg},
@@ -494,7 +519,7 @@ def run_capture(args):
     import powerllel_channel_b200 as plb
     prec = plb.PL_MIXED if args.capture == "mixed" else plb.PL_FP64
     cfg = plb.ChannelConfig(nx=NX, ny=NY, nz=NZ, stretch_ratio=STRETCH, re_tau=RE_TAU, dt=DT, precision=prec,
-                            trid_parts=args.trid_parts)
+                            trid_parts=args.trid_parts or PARTS)
     ch = plb.Channel(cfg)
     ch.init_flow(SEED, NOISE)
     ch.step(args.warmup + args.steps)
@@ -518,7 +543,12 @@ def main():
     ap.add_argument("--capture", choices=["fp64", "mixed"], default=None,
                     help="run one precision path untimed (the command an ncu capture wraps)")
     ap.add_argument("--trid-parts", type=int, default=0, help="--capture only: PDD partitions (0 = Thomas)")
+    ap.add_argument("--config", choices=sorted(CONFIGS), default=None,
+                    help="one of the benchmark configurations (default: C3, the headline workload); the 100-step "
+                         "accuracy comparison runs for C3 only")
     args = ap.parse_args()
+    if args.config:
+        set_config(args.config)
     if args.warmup < 3:
         args.warmup = 3
     if args.grid:

@@ -244,20 +244,46 @@ __global__ void __launch_bounds__(256) k_diag(const double *__restrict__ u, cons
     }
 }
 
-__global__ void k_diag_finish(const double *part, const long long *ipart, int nb, StepParams p, double *out,
-                              int *loc)
+// the block partials reduced by one CTA: max |div| and max CFL with the
+// first location among equal values (better() is associative and
+// commutative, so the tree gives the scan's result), the NaN count summed
+// (whole numbers, exact in any order)
+constexpr int DIAG_FIN_THREADS = 1024;
+__global__ void __launch_bounds__(DIAG_FIN_THREADS) k_diag_finish(const double *part, const long long *ipart, int nb,
+                                                                  StepParams p, double *out, int *loc)
 {
-    if (threadIdx.x != 0) return;
+    __shared__ double sdv[DIAG_FIN_THREADS], scv[DIAG_FIN_THREADS], snan[DIAG_FIN_THREADS];
+    __shared__ long long sdi[DIAG_FIN_THREADS], sci[DIAG_FIN_THREADS];
+    const int t = threadIdx.x;
     double dv = -1.0, cv = -1.0, nan = 0.0;
     long long di = 0x7fffffffffffffffLL, ci = 0x7fffffffffffffffLL;
-    for (int b = 0; b < nb; b++) {
+    for (int b = t; b < nb; b += DIAG_FIN_THREADS) {
         better(dv, di, part[b], ipart[b]);
         better(cv, ci, part[nb + b], ipart[nb + b]);
         nan += part[2 * nb + b];
     }
+    sdv[t] = dv;
+    sdi[t] = di;
+    scv[t] = cv;
+    sci[t] = ci;
+    snan[t] = nan;
+    __syncthreads();
+    for (int o = DIAG_FIN_THREADS / 2; o > 0; o >>= 1) {
+        if (t < o) {
+            better(sdv[t], sdi[t], sdv[t + o], sdi[t + o]);
+            better(scv[t], sci[t], scv[t + o], sci[t + o]);
+            snan[t] += snan[t + o];
+        }
+        __syncthreads();
+    }
+    if (t != 0) return;
+    dv = sdv[0];
+    di = sdi[0];
+    cv = scv[0];
+    ci = sci[0];
     out[0] = dv;
     out[1] = cv * p.dt;
-    out[2] = nan;
+    out[2] = snan[0];
     const long long nxy = (long long)p.nx * p.ny;
     loc[0] = (int)(di % p.nx) + 1;
     loc[1] = (int)((di / p.nx) % p.ny) + 1;
@@ -644,7 +670,7 @@ int launch_diagnostics_fp64(const double *u, const double *v, const double *w, c
     }
     k_diag<<<point_grid(p), point_block(), 0, st>>>(u, v, w, p, m, d_part, d_ipart);
     PL_CHECK_LAUNCH();
-    k_diag_finish<<<1, 32, 0, st>>>(d_part, d_ipart, nblocks(p), p, d_out, d_loc);
+    k_diag_finish<<<1, DIAG_FIN_THREADS, 0, st>>>(d_part, d_ipart, nblocks(p), p, d_out, d_loc);
     PL_CHECK_LAUNCH();
     return 0;
 }
