@@ -370,10 +370,13 @@ __global__ void __launch_bounds__(pf_x_threads<T>()) k_xfft_pf(const T *__restri
 }
 
 template <typename T, int N, bool FWD>
-// CTAs per SM the register budget is cut for: up to 80 registers for FP32
-// lines up to 512 (three CTAs), 128 for FP64 ones (two); longer lines keep
-// more registers rather than spill
-__global__ void __launch_bounds__(pf_y_threads<T>(), sizeof(T) == 4 ? (N <= 512 ? 3 : 2) : (N <= 512 ? 2 : 1))
+// CTAs per SM the register budget is cut for, as measured fastest at
+// N = 384: up to 80 registers (three CTAs) for FP32 lines up to 512 and for
+// the FP64 inverse (a spill of 4-16 bytes, served from L1, costs less than
+// the third CTA gains), 128 (two) for the FP64 forward, which would spill
+// 80 bytes at 80; longer lines keep more registers rather than spill
+__global__ void __launch_bounds__(pf_y_threads<T>(),
+                                  sizeof(T) == 4 ? (N <= 512 ? 3 : 2) : (N <= 512 ? (FWD ? 2 : 3) : 1))
     k_yfft_pf(T *__restrict__ data, const typename cplx_of<T>::type *__restrict__ twg,
                                                  int nx, int total)
 {
@@ -866,6 +869,232 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
     }
 }
 
+// Two-ended Thomas in tensor memory (mixed path; 16 <= nz <= 256, nz % 16
+// == 0).  The one-ended sweep above is one dependent FP64 chain of 2 nz
+// steps per column at one warp per scheduler.  Here each column is swept
+// from both walls at once: rows below p = nz/2 by the LU elimination (the
+// same multipliers and pivots), rows p .. nz-1 by the elimination from the
+// top wall (TridTables::tmult / trb), the 2x2 system of rows p-1 and p joins
+// the halves, and the back substitution runs outwards from them: two
+// independent chains of nz steps per thread.  The forward-swept values of
+// both halves share the thread's tensor-memory lane (row k at cell 2k); each
+// ring slot carries 8 rows of each half.  The (0,0) class's junction rows
+// hold the gauge x_p = 0.
+constexpr int TTW_G = 8, TTW_NS = 4;
+
+template <typename T> __host__ __device__ constexpr size_t ttw_smem_bytes()
+{
+    // ring [NS][2G][NT] of table values (double) and of right-hand sides (T),
+    // (0,0)-mode ring [NS][2G], c_k and a_k [256], TMEM address slot; at
+    // least 116 KB so that two CTAs never share an SM
+    const size_t b = (size_t)TTW_NS * 2 * TTW_G * TTM_THREADS * (8 + sizeof(T)) + TTW_NS * 2 * TTW_G * 8 +
+                     2 * TTM_TM_ROWS * 8 + 16;
+    return b < 116 * 1024 ? 116 * 1024 : b;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(TTM_THREADS, 1)
+    k_thomas_tw(const T *xin, T *xout, const double *tm, const double *tr, const double *ak, const double *ck,
+                int nx, int ny, int nz, int ncx, int ncy, const double *mode0, int rounds, uint32_t tcols)
+{
+    constexpr int G = TTW_G, NS = TTW_NS, NT = TTM_THREADS, R = 2 * G;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *cring = reinterpret_cast<double *>(smem_raw);          // [NS][2G][NT] tables
+    T *xring = reinterpret_cast<T *>(cring + NS * R * NT);           // [NS][2G][NT] right-hand side
+    double *zring = reinterpret_cast<double *>(xring + NS * R * NT); // [NS][2G] (0,0) mode
+    double *csh = zring + NS * R;                                    // c_k
+    double *ash = csh + TTM_TM_ROWS;                                 // a_k
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(ash + TTM_TM_ROWS);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int p = nz / 2, ngh = p / G, per_round = 2 * ngh;
+    const size_t stride = (size_t)nx * ny, cstride = (size_t)ncx * ncy;
+    const int ncol = nx * ny;
+    TridDev td{nx, ny, nz, ncx, ncy, nullptr, nullptr, nullptr};
+
+    for (int k = tid; k < nz; k += NT) {
+        csh[k] = __ldg(ck + k);
+        ash[k] = __ldg(ak + k);
+    }
+    if (warp == 0) tmem_alloc(tslot, tcols);
+    tmem_fence_before_sync();
+    __syncthreads();
+    tmem_fence_after_sync();
+    const uint32_t tbase = *tslot + ((uint32_t)(warp * 32) << 16);
+
+    auto column = [&](int r) {
+        TtmColumn c{false, 0, 0};
+        const int q = (r * (int)gridDim.x + (int)blockIdx.x) * NT + tid;
+        if (q < ncol) {
+            const int b = q / nx, px = q - b * nx, py = trid_pair_row(b, ny);
+            c = TtmColumn{true, (size_t)px + (size_t)nx * py, trid_class(px, py, td)};
+        }
+        return c;
+    };
+    const bool zcta = (mode0 != nullptr) && blockIdx.x == 0;
+
+    // copy stream: forward group g brings rows g G + u (lower) and
+    // nz-1 - g G - u (upper) of the right-hand side and of tm; backward group
+    // h rows p-1 - h G - u and p + h G + u of tr
+    int ir = 0, ig = 0, islot = 0;
+    TtmColumn ic = column(0);
+    const T *xl = xin + ic.col, *xu = xin + ic.col + (size_t)(nz - 1) * stride;
+    const double *ml = tm + ic.cls, *mu = tm + ic.cls + (size_t)(nz - 1) * cstride;
+    const double *rl = tr + ic.cls + (size_t)(p - 1) * cstride, *ru = tr + ic.cls + (size_t)p * cstride;
+    auto issue_next = [&]() {
+        if (ir < rounds) {
+            double *cdst = cring + islot * R * NT + tid;
+            if (ig < ngh) {
+                T *xdst = xring + islot * R * NT + tid;
+                const bool z = zcta && ir == 0 && tid == 0;
+                if (ic.valid) {
+#pragma unroll
+                    for (int u = 0; u < G; u++) {
+                        cp_async_8(cdst + u * NT, ml);
+                        cp_async_8(cdst + (G + u) * NT, mu);
+                        if (z) {
+                            cp_async_8(zring + islot * R + u, mode0 + ig * G + u);
+                            cp_async_8(zring + islot * R + G + u, mode0 + (nz - 1 - ig * G - u));
+                        } else if (sizeof(T) == 8) {
+                            cp_async_8(xdst + u * NT, xl);
+                            cp_async_8(xdst + (G + u) * NT, xu);
+                        } else {
+                            cp_async_4(xdst + u * NT, xl);
+                            cp_async_4(xdst + (G + u) * NT, xu);
+                        }
+                        ml += cstride;
+                        mu -= cstride;
+                        xl += stride;
+                        xu -= stride;
+                    }
+                }
+            } else if (ic.valid) {
+#pragma unroll
+                for (int u = 0; u < G; u++) {
+                    cp_async_8(cdst + u * NT, rl);
+                    cp_async_8(cdst + (G + u) * NT, ru);
+                    rl -= cstride;
+                    ru += cstride;
+                }
+            }
+            if (++ig == per_round) {
+                ig = 0;
+                if (++ir < rounds) {
+                    ic = column(ir);
+                    xl = xin + ic.col;
+                    xu = xin + ic.col + (size_t)(nz - 1) * stride;
+                    ml = tm + ic.cls;
+                    mu = tm + ic.cls + (size_t)(nz - 1) * cstride;
+                    rl = tr + ic.cls + (size_t)(p - 1) * cstride;
+                    ru = tr + ic.cls + (size_t)p * cstride;
+                }
+            }
+        }
+        cp_async_commit(); // one group per step, empty or not
+        islot = (islot + 1 == NS) ? 0 : islot + 1;
+    };
+
+    for (int q = 0; q < NS - 1; q++) issue_next();
+    int slot = 0;
+    for (int r = 0; r < rounds; r++) {
+        const TtmColumn cc = column(r);
+        const bool zr = zcta && r == 0; // warp-uniform
+        // the junction's 2x2 coefficients, needed after the forward sweep
+        const double jE = __ldg(tm + cc.cls + (size_t)nz * cstride), jC = __ldg(tm + cc.cls + (size_t)(nz + 1) * cstride);
+        const double jD = __ldg(tr + cc.cls + (size_t)nz * cstride), jA = __ldg(tr + cc.cls + (size_t)(nz + 1) * cstride);
+        // forward: xs_k = r_k - m_k xs_{k-1} (lower, k = 0 .. p-1) and
+        // ys_k = r_k - m_k ys_{k+1} (upper, k = nz-1 .. p)
+        double sl = 0.0, su = 0.0;
+        for (int g = 0; g < ngh; g++) {
+            cp_async_wait<NS - 2>(); // this step's group has landed
+            const double *cs = cring + slot * R * NT + tid;
+            const T *xs = xring + slot * R * NT + tid;
+            double xvl[G], mvl[G], xvu[G], mvu[G];
+#pragma unroll
+            for (int u = 0; u < G; u++) {
+                xvl[u] = (double)xs[u * NT];
+                xvu[u] = (double)xs[(G + u) * NT];
+                mvl[u] = cs[u * NT];
+                mvu[u] = cs[(G + u) * NT];
+            }
+            if (zr && tid == 0) {
+#pragma unroll
+                for (int u = 0; u < G; u++) {
+                    xvl[u] = zring[slot * R + u];
+                    xvu[u] = zring[slot * R + G + u];
+                }
+            }
+            issue_next(); // refills the slot consumed one step ago
+            uint32_t vl[2 * G], vu[2 * G];
+#pragma unroll
+            for (int u = 0; u < G; u++) {
+                sl = xvl[u] - mvl[u] * sl;
+                su = xvu[u] - mvu[u] * su;
+                vl[2 * u] = (uint32_t)__double2loint(sl);
+                vl[2 * u + 1] = (uint32_t)__double2hiint(sl);
+                const int i = G - 1 - u; // upper row nz-1 - g G - u is cell pair i of its block
+                vu[2 * i] = (uint32_t)__double2loint(su);
+                vu[2 * i + 1] = (uint32_t)__double2hiint(su);
+            }
+            __syncwarp();
+            tmem_st16(tbase + 2 * (g * G), vl);
+            tmem_st16(tbase + 2 * (nz - G - g * G), vu);
+            slot = (slot + 1 == NS) ? 0 : slot + 1;
+        }
+        tmem_wait_st();
+        // rows p-1 and p from the joining 2x2 system
+        const double xa = sl * jE - su * jC, xb = su * jD - sl * jA;
+        // backward: x_k = (xs_k - c_k x_{k+1}) / d_k below, x_k = (ys_k - a_k x_{k-1}) / e_k above
+        double wl = 0.0, wu = 0.0;
+        T *dl = xout + cc.col + (size_t)(p - 1) * stride, *du = xout + cc.col + (size_t)p * stride;
+        for (int h = 0; h < ngh; h++) {
+            uint32_t vl[2 * G], vu[2 * G];
+            __syncwarp();
+            tmem_ld16_start(tbase + 2 * (p - G - h * G), vl); // rows p-G-hG .. p-1-hG
+            tmem_ld16_start(tbase + 2 * (p + h * G), vu);     // rows p+hG .. p+hG+G-1
+            cp_async_wait<NS - 2>();
+            const double *cs = cring + slot * R * NT + tid;
+            double rvl[G], rvu[G], cvl[G], avu[G];
+#pragma unroll
+            for (int u = 0; u < G; u++) {
+                rvl[u] = cs[u * NT];
+                rvu[u] = cs[(G + u) * NT];
+                cvl[u] = csh[p - 1 - h * G - u];
+                avu[u] = ash[p + h * G + u];
+            }
+            issue_next();
+            tmem_wait_ld(vl);
+            tmem_wait_ld(vu);
+#pragma unroll
+            for (int u = 0; u < G; u++) {
+                const int i = G - 1 - u;
+                const double xsl = __hiloint2double((int)vl[2 * i + 1], (int)vl[2 * i]);
+                const double xsu = __hiloint2double((int)vu[2 * u + 1], (int)vu[2 * u]);
+                if (u == 0 && h == 0) {
+                    wl = xa;
+                    wu = xb;
+                } else {
+                    wl = (xsl - cvl[u] * wl) * rvl[u];
+                    wu = (xsu - avu[u] * wu) * rvu[u];
+                }
+                if (cc.valid) {
+                    *dl = (T)wl;
+                    *du = (T)wu;
+                }
+                dl -= stride;
+                du += stride;
+            }
+            slot = (slot + 1 == NS) ? 0 : slot + 1;
+        }
+    }
+    cp_async_wait<0>();
+    tmem_fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tmem_fence_after_sync();
+        tmem_free(*tslot, tcols);
+    }
+}
+
 constexpr int PDD_MAX_PARTS = 64;
 
 struct PddDev {
@@ -1105,7 +1334,18 @@ int ppe_create(Ppe *s, int nx, int ny, int nz, double dx, double dy, const doubl
 
     // tridiagonal coefficients, pivots and PDD spikes per eigenvalue class
     TridTables tt;
-    trid_build(tt, nx, ny, nz, dx, dy, dzf_global, nparts);
+    const bool twisted = prec == PREC_MIXED && nparts == 0 && nz % (2 * TTW_G) == 0 && nz >= 2 * TTW_G &&
+                         nz <= TTM_TM_ROWS;
+    trid_build(tt, nx, ny, nz, dx, dy, dzf_global, nparts, twisted);
+    if (prec == PREC_MIXED && nparts == 0) {
+        // The (0,0) class has lambda = 0: its Neumann system is singular and
+        // its last pivot is round-off, so the reference's division at row
+        // nz-1 gives x a constant of order 1e7 |x| that an FP32 result cannot
+        // carry.  The mixed plan takes the gauge x[nz-1] = 0 there instead,
+        // as the sweeps' plane-sum branch does; the FP64 plan keeps the
+        // reference's pivots.
+        tt.rb[(size_t)(nz - 1) * ((size_t)s->ncx * s->ncy)] = 0.0;
+    }
     s->kst = tt.kst;
     s->ksz = tt.ksz;
     const size_t ncls = (size_t)s->ncx * s->ncy;
@@ -1127,6 +1367,12 @@ int ppe_create(Ppe *s, int nx, int ny, int nz, double dx, double dy, const doubl
         PL_CUDA_TRY(cudaMemcpy(s->d_v, v.data(), sizeof(double) * ncls * nz, cudaMemcpyHostToDevice));
         PL_CUDA_TRY(cudaMemcpy(s->d_w, w.data(), sizeof(double) * ncls * nz, cudaMemcpyHostToDevice));
         PL_CUDA_TRY(cudaMemcpy(s->d_tmpv, tmpv.data(), sizeof(double) * ncls * P, cudaMemcpyHostToDevice));
+    }
+    if (twisted) {
+        PL_CUDA_TRY(cudaMalloc(&s->d_tmult, sizeof(double) * ncls * (nz + 2)));
+        PL_CUDA_TRY(cudaMalloc(&s->d_trb, sizeof(double) * ncls * (nz + 2)));
+        PL_CUDA_TRY(cudaMemcpy(s->d_tmult, tt.tmult.data(), sizeof(double) * ncls * (nz + 2), cudaMemcpyHostToDevice));
+        PL_CUDA_TRY(cudaMemcpy(s->d_trb, tt.trb.data(), sizeof(double) * ncls * (nz + 2), cudaMemcpyHostToDevice));
     }
     if (prec == PREC_MIXED || nparts >= 1) {
         s->scratch_elems = (size_t)nx * ny * nz;
@@ -1172,7 +1418,8 @@ int ppe_create_slab(Ppe *s, int nx, int ny, int nz_global, double dx, double dy,
     s->slab = 1;
     s->has_down = rank > 0;
     s->has_up = rank < nranks - 1;
-    s->d_mult = s->d_rb = s->d_c = s->d_a = s->d_bt = s->d_v = s->d_w = s->d_tmpv = s->d_scratch = nullptr;
+    s->d_tmult = s->d_trb = s->d_mult = s->d_rb = s->d_c = s->d_a = s->d_bt = s->d_v = s->d_w = s->d_tmpv =
+        s->d_scratch = nullptr;
     const size_t ncls = (size_t)s->ncx * s->ncy, nxy = (size_t)nx * ny;
     auto slice = [&](const double *src, size_t per_plane, int k_from, int nk, double **dst) -> int {
         PL_CUDA_TRY(cudaMalloc(dst, sizeof(double) * per_plane * nk));
@@ -1214,6 +1461,8 @@ void ppe_destroy(Ppe *s)
     cudaFree(s->d_twy32);
     cudaFree(s->d_mult);
     cudaFree(s->d_rb);
+    cudaFree(s->d_tmult);
+    cudaFree(s->d_trb);
     cudaFree(s->d_c);
     cudaFree(s->d_a);
     cudaFree(s->d_bt);
@@ -1410,6 +1659,20 @@ template <typename T> static int launch_trid(Ppe *s, T *x, cudaStream_t st, cons
 {
     TridDev t{s->nx, s->ny, s->nz, s->ncx, s->ncy, s->d_mult, s->d_rb, s->d_c};
     dim3 grid((s->nx + 127) / 128, s->ny);
+    if (sizeof(T) == 4 && s->nparts == 0 && s->d_tmult != nullptr) {
+        // the two-ended sweep (mixed path): two chains per column
+        const size_t shm = ttw_smem_bytes<T>();
+        const int ncol = s->nx * s->ny;
+        const int ctas = std::max(1, std::min(sm_count(), (ncol + TTM_THREADS - 1) / TTM_THREADS));
+        const int rounds = (ncol + ctas * TTM_THREADS - 1) / (ctas * TTM_THREADS);
+        uint32_t tcols = 32;
+        while (tcols < 2u * (uint32_t)s->nz) tcols *= 2;
+        PL_CUDA_TRY(cudaFuncSetAttribute(k_thomas_tw<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        k_thomas_tw<T><<<ctas, TTM_THREADS, shm, st>>>(x, x, s->d_tmult, s->d_trb, s->d_a, s->d_c, s->nx, s->ny, s->nz,
+                                                         s->ncx, s->ncy, mode0, rounds, tcols);
+        PL_CHECK_LAUNCH();
+        return 0;
+    }
     double *xs = (sizeof(T) == 8 && s->nparts == 0) ? reinterpret_cast<double *>(x) : s->d_scratch;
     if (s->nparts == 0 && s->nz % TTM_G == 0 && s->nz <= TTM_MAX_NZ &&
         (s->nz <= TTM_TM_ROWS || sizeof(T) == 8 || s->d_scratch != nullptr)) {

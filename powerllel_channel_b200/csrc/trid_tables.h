@@ -24,6 +24,16 @@ struct TridTables {
     std::vector<double> mult;      // a[k]/b[k-1]; 0 at a partition's first row
     std::vector<double> rb;        // 1/b[k], 0 where b == 0 (the guard of :337-342)
     std::vector<double> v, w, tmpv; // PDD only
+    // Two-ended (twisted) sweep of a Thomas column, nz even: rows below
+    // p = nz/2 keep the LU multipliers and reciprocal pivots above; rows
+    // p .. nz-1 hold the elimination from the top wall, tmult[k] =
+    // c[k]/e[k+1] (0 at nz-1) and trb[k] = 1/e[k], e[nz-1] = b[nz-1],
+    // e[k] = b[k] - tmult[k] a[k+1].  Rows nz and nz+1 hold the 2x2 system
+    // that joins the halves, d x_{p-1} + c[p-1] x_p = xs_{p-1} and
+    // a[p] x_{p-1} + e[p] x_p = ys_p: x_{p-1} = xs tmult[nz] - ys tmult[nz+1],
+    // x_p = ys trb[nz] - xs trb[nz+1].  Where that system is singular (the
+    // (0,0) class: zero row sums) the rows give the gauge x_p = 0.
+    std::vector<double> tmult, trb;
 };
 
 // decomp_2d.c:261-283, 0-based starts
@@ -56,7 +66,7 @@ inline void trid_distribute(int num, int nprocs, std::vector<int> &st0, std::vec
 
 // nparts 0: Thomas over the whole column; nparts >= 1: PDD partitions
 inline void trid_build(TridTables &t, int nx, int ny, int nz, double dx, double dy, const double *dzf_global,
-                       int nparts)
+                       int nparts, bool twisted = false)
 {
     t = TridTables();
     t.nx = nx;
@@ -83,6 +93,12 @@ inline void trid_build(TridTables &t, int nx, int ny, int nz, double dx, double 
     std::vector<double> &a = t.a, &bt = t.bt;
     t.mult.assign(ncls * nz, 0.0);
     t.rb.assign(ncls * nz, 0.0);
+    twisted = twisted && nparts == 0 && nz % 2 == 0 && nz >= 4;
+    if (twisted) {
+        t.tmult.assign(ncls * (nz + 2), 0.0);
+        t.trb.assign(ncls * (nz + 2), 0.0);
+    }
+    std::vector<double> e(twisted ? nz : 0);
     if (nparts >= 1) {
         t.v.assign(ncls * nz, 0.0);
         t.w.assign(ncls * nz, 0.0);
@@ -150,6 +166,37 @@ inline void trid_build(TridTables &t, int nx, int ny, int nz, double dx, double 
             }
             if (nparts >= 1)
                 for (int m = 0; m + 1 < P; m++) t.tmpv[cl + ncls * m] = t.v[cl + ncls * t.kst[m + 1]];
+            if (twisted) {
+                const int p = nz / 2;
+                for (int k = 0; k < p; k++) {
+                    t.tmult[cl + ncls * k] = t.mult[cl + ncls * k];
+                    t.trb[cl + ncls * k] = t.rb[cl + ncls * k];
+                }
+                e[nz - 1] = bt[nz - 1] + lam;
+                for (int k = nz - 2; k >= p; k--) {
+                    const double mu = c[k] / e[k + 1];
+                    e[k] = (bt[k] + lam) - mu * a[k + 1];
+                    t.tmult[cl + ncls * k] = mu;
+                }
+                for (int k = p; k < nz; k++) t.trb[cl + ncls * k] = (e[k] != 0.0) ? 1.0 / e[k] : 0.0;
+                // b[p-1] is the LU pivot d_{p-1} (eliminated in place above)
+                const double d = b[p - 1], ep = e[p], det = d * ep - c[p - 1] * a[p];
+                double E, C, D, A;
+                if (!(fabs(det) > 1e-13 * fabs(d * ep))) { // singular: gauge x_p = 0
+                    E = (d != 0.0) ? 1.0 / d : 0.0;
+                    C = D = A = 0.0;
+                } else {
+                    const double idet = 1.0 / det;
+                    E = ep * idet;
+                    C = c[p - 1] * idet;
+                    D = d * idet;
+                    A = a[p] * idet;
+                }
+                t.tmult[cl + ncls * nz] = E;
+                t.tmult[cl + ncls * (nz + 1)] = C;
+                t.trb[cl + ncls * nz] = D;
+                t.trb[cl + ncls * (nz + 1)] = A;
+            }
         }
 }
 

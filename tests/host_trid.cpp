@@ -62,3 +62,33 @@ extern "C" int host_trid_solve(int nx, int ny, int nz, double dx, double dy, con
         }
     return 0;
 }
+
+// the two-ended sweep of k_thomas_tw (mixed path): the LU elimination on rows
+// below p = nz/2, the elimination from the top wall on rows p .. nz-1, the
+// 2x2 system of rows p-1 and p, back substitution outwards (nz even)
+extern "C" int host_trid_solve_twisted(int nx, int ny, int nz, double dx, double dy, const double *dzf, double *x)
+{
+    TridTables t;
+    trid_build(t, nx, ny, nz, dx, dy, dzf, 0, true);
+    if (t.tmult.empty()) return -1;
+    const size_t stride = (size_t)nx * ny, cs = (size_t)t.ncx * t.ncy;
+    const int p = nz / 2;
+    std::vector<double> xs(nz);
+    for (int py = 0; py < ny; py++)
+        for (int px = 0; px < nx; px++) {
+            const size_t col = (size_t)px + (size_t)nx * py;
+            const int ix = px < nx - px ? px : nx - px, jy = py < ny - py ? py : ny - py;
+            const size_t cls = (size_t)ix + (size_t)t.ncx * jy;
+            auto M = [&](int k) { return t.tmult[cls + (size_t)k * cs]; };
+            auto R = [&](int k) { return t.trb[cls + (size_t)k * cs]; };
+            double sl = 0.0, su = 0.0;
+            for (int k = 0; k < p; k++) xs[k] = sl = x[col + (size_t)k * stride] - M(k) * sl;
+            for (int k = nz - 1; k >= p; k--) xs[k] = su = x[col + (size_t)k * stride] - M(k) * su;
+            double wl = sl * M(nz) - su * M(nz + 1), wu = su * R(nz) - sl * R(nz + 1);
+            x[col + (size_t)(p - 1) * stride] = wl;
+            x[col + (size_t)p * stride] = wu;
+            for (int k = p - 2; k >= 0; k--) x[col + (size_t)k * stride] = wl = (xs[k] - t.c[k] * wl) * R(k);
+            for (int k = p + 1; k < nz; k++) x[col + (size_t)k * stride] = wu = (xs[k] - t.a[k] * wu) * R(k);
+        }
+    return 0;
+}

@@ -26,6 +26,8 @@ def host_lib():
         _lib = C.CDLL(so)
         _lib.host_trid_solve.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                          C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double)]
+        _lib.host_trid_solve_twisted.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                                 C.POINTER(C.c_double), C.POINTER(C.c_double)]
     return _lib
 
 
@@ -71,6 +73,30 @@ def test_trid_tables_reproduce_reference(path):
     dzf = np.ascontiguousarray(d["dzf"])
     host_lib().host_trid_solve(nx, ny, nz, float(d["dx"]), float(d["dy"]), dzf.ctypes.data_as(C.POINTER(C.c_double)),
                                nparts, x.ctypes.data_as(C.POINTER(C.c_double)))
+    p = hc2r(hc2r(x, 1), 2) / (nx * ny)
+    ref = d["p"]
+    err = np.abs((p - p.mean()) - (ref - ref.mean())).max() / np.abs(ref - ref.mean()).max()
+    assert err < 1e-12, err
+
+
+GOLDEN_THOMAS = [p for p in GOLDEN_PPE if not int(np.load(p)["pdd"]) and int(np.load(p)["nz"]) % 2 == 0]
+
+
+@pytest.mark.parametrize("path", GOLDEN_THOMAS, ids=[os.path.basename(p)[:-4] for p in GOLDEN_THOMAS])
+def test_twisted_sweep_matches_reference_thomas(path):
+    """The mixed path's two-ended sweep (k_thomas_tw's column algorithm, its
+    tables from the same builder) against the reference's own Thomas solve:
+    the same solution up to rounding, modulo the Neumann null mode's constant
+    (its gauge is x_p = 0 at the middle row instead of the reference's
+    round-off division)."""
+    d = np.load(path)
+    nx, ny, nz = int(d["nx"]), int(d["ny"]), int(d["nz"])
+    x = np.ascontiguousarray(r2hc(r2hc(d["rhs"], 2), 1))
+    dzf = np.ascontiguousarray(d["dzf"])
+    rc = host_lib().host_trid_solve_twisted(nx, ny, nz, float(d["dx"]), float(d["dy"]),
+                                            dzf.ctypes.data_as(C.POINTER(C.c_double)),
+                                            x.ctypes.data_as(C.POINTER(C.c_double)))
+    assert rc == 0
     p = hc2r(hc2r(x, 1), 2) / (nx * ny)
     ref = d["p"]
     err = np.abs((p - p.mean()) - (ref - ref.mean())).max() / np.abs(ref - ref.mean()).max()
