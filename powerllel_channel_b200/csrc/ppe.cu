@@ -232,10 +232,12 @@ __global__ void __launch_bounds__(256) k_pressure_update(const float *__restrict
 // lines into complex values (and, for the inverse, merges the half-complex
 // spectra).  The y kernel moves whole 32-byte sectors: W column pairs of V
 // per row (W * sizeof(V) = 64 bytes when N allows).
-template <typename V, int N> __host__ __device__ constexpr int pf_y_cols()
+// (FP64: the forward transform measured faster with 8 columns at N = 384,
+// 0.173 -> 0.160 ms at 512x384x256, the inverse with 4, 0.177 against 0.182)
+template <typename V, int N, bool FWD> __host__ __device__ constexpr int pf_y_cols()
 {
     return sizeof(V) == 8 ? ((3072 / N) >= 8 ? 8 : ((3072 / N) >= 4 ? 4 : 2))
-                          : ((1536 / N) >= 4 ? 4 : ((1536 / N) >= 2 ? 2 : 1));
+                          : (FWD && (3072 / N) >= 8 ? 8 : ((1536 / N) >= 4 ? 4 : ((1536 / N) >= 2 ? 2 : 1)));
 }
 
 // threads per CTA of the persistent x kernel, and line pairs per group: one
@@ -259,10 +261,10 @@ template <typename T, int N> __host__ __device__ constexpr int pf_x_pu_bytes()
 {
     return 2 * 2 * pf_x_lines<T, N>() * N * 4;
 }
-template <typename T, int N> __host__ __device__ constexpr int pf_y_smem_elems()
+template <typename T, int N, bool FWD> __host__ __device__ constexpr int pf_y_smem_elems()
 {
     using V = typename cplx_of<T>::type;
-    return (fpad_elems<V>(pf_y_cols<V, N>() * N) + 1) / 2 * 2 + pf_y_cols<V, N>() * N + N;
+    return (fpad_elems<V>(pf_y_cols<V, N, FWD>() * N) + 1) / 2 * 2 + pf_y_cols<V, N, FWD>() * N + N;
 }
 
 // PU (FP32 inverse only): the pressure update of the mixed path is fused
@@ -382,7 +384,7 @@ __global__ void __launch_bounds__(pf_y_threads<T>(),
 {
     using V = typename cplx_of<T>::type;
     constexpr int NT = pf_y_threads<T>();
-    constexpr int W = pf_y_cols<V, N>(), BUF = (fpad_elems<V>(W * N) + 1) / 2 * 2, RAW = W * N;
+    constexpr int W = pf_y_cols<V, N, FWD>(), BUF = (fpad_elems<V>(W * N) + 1) / 2 * 2, RAW = W * N;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int ncol = nx / 2;
     V *buf = reinterpret_cast<V *>(smem_raw);
@@ -869,47 +871,56 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
     }
 }
 
-// Two-ended Thomas in tensor memory (mixed path; 16 <= nz <= 256, nz % 16
-// == 0).  The one-ended sweep above is one dependent FP64 chain of 2 nz
-// steps per column at one warp per scheduler.  Here each column is swept
-// from both walls at once: rows below p = nz/2 by the LU elimination (the
-// same multipliers and pivots), rows p .. nz-1 by the elimination from the
-// top wall (TridTables::tmult / trb), the 2x2 system of rows p-1 and p joins
-// the halves, and the back substitution runs outwards from them: two
-// independent chains of nz steps per thread.  The forward-swept values of
-// both halves share the thread's tensor-memory lane (row k at cell 2k); each
-// ring slot carries 8 rows of each half.  The (0,0) class's junction rows
-// hold the gauge x_p = 0.
-constexpr int TTW_G = 8, TTW_NS = 4;
+// rows per ring group of the two-ended sweep below
+constexpr int TTW_G = 8;
 
-template <typename T> __host__ __device__ constexpr size_t ttw_smem_bytes()
+// Two-ended Thomas with one thread per half column (mixed path; 16 <= nz <=
+// 256, nz % 16 == 0), the tables TridTables::tmult and trb.  A 256-thread CTA solves 128
+// columns per round: threads 0-127 sweep the lower halves (rows 0 .. p-1, the
+// LU elimination), threads 128-255 the upper halves (rows nz-1 .. p, the
+// elimination from the top wall), each thread one chain of nz steps.  Both
+// threads of a column share a tensor-memory lane (warps w and w+4 reach the
+// same lanes): the lower half's swept rows at cells 2k, the upper half's at
+// cells nz + 2(k - p).  They meet at the 2x2 system of rows p-1 and p through
+// shared memory, one barrier per round.  (One thread per column with both
+// chains interleaved ran at 0.179 ms against 0.186 for the one-ended sweep;
+// this kernel, two warps per scheduler, at 0.177 ms, at 512x384x256: the
+// per-row instruction latency binds, not the FP64 recurrence alone.)
+constexpr int TTH_NS = 4;
+
+template <typename T> __host__ __device__ constexpr size_t tth_smem_bytes()
 {
-    // ring [NS][2G][NT] of table values (double) and of right-hand sides (T),
-    // (0,0)-mode ring [NS][2G], c_k and a_k [256], TMEM address slot; at
-    // least 116 KB so that two CTAs never share an SM
-    const size_t b = (size_t)TTW_NS * 2 * TTW_G * TTM_THREADS * (8 + sizeof(T)) + TTW_NS * 2 * TTW_G * 8 +
-                     2 * TTM_TM_ROWS * 8 + 16;
+    // ring [NS][G][256] of table values (double) and right-hand sides (T),
+    // (0,0)-mode ring [NS][2][G], c_k and a_k [256], junction values [2][2][128],
+    // TMEM address slot; at least 116 KB so that two CTAs never share an SM
+    const size_t b = (size_t)TTH_NS * TTW_G * 2 * TTM_THREADS * (8 + sizeof(T)) + TTH_NS * 2 * TTW_G * 8 +
+                     2 * TTM_TM_ROWS * 8 + 4 * TTM_THREADS * 8 + 16;
     return b < 116 * 1024 ? 116 * 1024 : b;
 }
 
 template <typename T>
-__global__ void __launch_bounds__(TTM_THREADS, 1)
-    k_thomas_tw(const T *xin, T *xout, const double *tm, const double *tr, const double *ak, const double *ck,
+__global__ void __launch_bounds__(2 * TTM_THREADS, 1)
+    k_thomas_th(const T *xin, T *xout, const double *tm, const double *tr, const double *ak, const double *ck,
                 int nx, int ny, int nz, int ncx, int ncy, const double *mode0, int rounds, uint32_t tcols)
 {
-    constexpr int G = TTW_G, NS = TTW_NS, NT = TTM_THREADS, R = 2 * G;
+    constexpr int G = TTW_G, NS = TTH_NS, NC = TTM_THREADS, NT = 2 * NC;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *cring = reinterpret_cast<double *>(smem_raw);          // [NS][2G][NT] tables
-    T *xring = reinterpret_cast<T *>(cring + NS * R * NT);           // [NS][2G][NT] right-hand side
-    double *zring = reinterpret_cast<double *>(xring + NS * R * NT); // [NS][2G] (0,0) mode
-    double *csh = zring + NS * R;                                    // c_k
+    double *cring = reinterpret_cast<double *>(smem_raw);          // [NS][G][NT] tables
+    T *xring = reinterpret_cast<T *>(cring + NS * G * NT);           // [NS][G][NT] right-hand side
+    double *zring = reinterpret_cast<double *>(xring + NS * G * NT); // [NS][2][G] (0,0) mode
+    double *csh = zring + NS * 2 * G;                                // c_k
     double *ash = csh + TTM_TM_ROWS;                                 // a_k
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(ash + TTM_TM_ROWS);
-    const int tid = threadIdx.x, warp = tid >> 5;
+    double *jv = ash + TTM_TM_ROWS;                                  // [2 parities][2 halves][NC]
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(jv + 4 * NC);
+    const int tid = threadIdx.x, warp = tid >> 5, half = tid >= NC ? 1 : 0, lt = tid - half * NC;
     const int p = nz / 2, ngh = p / G, per_round = 2 * ngh;
-    const size_t stride = (size_t)nx * ny, cstride = (size_t)ncx * ncy;
+    const long long stride = (long long)nx * ny, cstride = (long long)ncx * ncy;
     const int ncol = nx * ny;
     TridDev td{nx, ny, nz, ncx, ncy, nullptr, nullptr, nullptr};
+    // this half's walk: forward from its wall towards the middle, backward
+    // from the middle towards its wall
+    const long long fx = half ? -stride : stride, fm = half ? -cstride : cstride, br = half ? cstride : -cstride;
+    const int kx0 = half ? nz - 1 : 0, kr0 = half ? p : p - 1;
 
     for (int k = tid; k < nz; k += NT) {
         csh[k] = __ldg(ck + k);
@@ -919,11 +930,11 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
     tmem_fence_before_sync();
     __syncthreads();
     tmem_fence_after_sync();
-    const uint32_t tbase = *tslot + ((uint32_t)(warp * 32) << 16);
+    const uint32_t tbase = *tslot + ((uint32_t)((warp & 3) * 32) << 16) + (half ? (uint32_t)nz : 0u);
 
     auto column = [&](int r) {
         TtmColumn c{false, 0, 0};
-        const int q = (r * (int)gridDim.x + (int)blockIdx.x) * NT + tid;
+        const int q = (r * (int)gridDim.x + (int)blockIdx.x) * NC + lt;
         if (q < ncol) {
             const int b = q / nx, px = q - b * nx, py = trid_pair_row(b, ny);
             c = TtmColumn{true, (size_t)px + (size_t)nx * py, trid_class(px, py, td)};
@@ -932,60 +943,48 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
     };
     const bool zcta = (mode0 != nullptr) && blockIdx.x == 0;
 
-    // copy stream: forward group g brings rows g G + u (lower) and
-    // nz-1 - g G - u (upper) of the right-hand side and of tm; backward group
-    // h rows p-1 - h G - u and p + h G + u of tr
+    // copy stream: forward group g brings this half's rows kx0 +- (g G + u)
+    // of the right-hand side and of tm, backward group h its rows
+    // kr0 -+ (h G + u) of tr
     int ir = 0, ig = 0, islot = 0;
     TtmColumn ic = column(0);
-    const T *xl = xin + ic.col, *xu = xin + ic.col + (size_t)(nz - 1) * stride;
-    const double *ml = tm + ic.cls, *mu = tm + ic.cls + (size_t)(nz - 1) * cstride;
-    const double *rl = tr + ic.cls + (size_t)(p - 1) * cstride, *ru = tr + ic.cls + (size_t)p * cstride;
+    const T *xp_ = xin + ic.col + kx0 * stride;
+    const double *mp_ = tm + ic.cls + kx0 * cstride, *rp_ = tr + ic.cls + kr0 * cstride;
     auto issue_next = [&]() {
         if (ir < rounds) {
-            double *cdst = cring + islot * R * NT + tid;
+            double *cdst = cring + islot * G * NT + tid;
             if (ig < ngh) {
-                T *xdst = xring + islot * R * NT + tid;
-                const bool z = zcta && ir == 0 && tid == 0;
+                T *xdst = xring + islot * G * NT + tid;
+                const bool z = zcta && ir == 0 && lt == 0;
                 if (ic.valid) {
 #pragma unroll
                     for (int u = 0; u < G; u++) {
-                        cp_async_8(cdst + u * NT, ml);
-                        cp_async_8(cdst + (G + u) * NT, mu);
-                        if (z) {
-                            cp_async_8(zring + islot * R + u, mode0 + ig * G + u);
-                            cp_async_8(zring + islot * R + G + u, mode0 + (nz - 1 - ig * G - u));
-                        } else if (sizeof(T) == 8) {
-                            cp_async_8(xdst + u * NT, xl);
-                            cp_async_8(xdst + (G + u) * NT, xu);
-                        } else {
-                            cp_async_4(xdst + u * NT, xl);
-                            cp_async_4(xdst + (G + u) * NT, xu);
-                        }
-                        ml += cstride;
-                        mu -= cstride;
-                        xl += stride;
-                        xu -= stride;
+                        cp_async_8(cdst + u * NT, mp_);
+                        if (z)
+                            cp_async_8(zring + (islot * 2 + half) * G + u,
+                                       mode0 + (half ? nz - 1 - ig * G - u : ig * G + u));
+                        else if (sizeof(T) == 8)
+                            cp_async_8(xdst + u * NT, xp_);
+                        else
+                            cp_async_4(xdst + u * NT, xp_);
+                        mp_ += fm;
+                        xp_ += fx;
                     }
                 }
             } else if (ic.valid) {
 #pragma unroll
                 for (int u = 0; u < G; u++) {
-                    cp_async_8(cdst + u * NT, rl);
-                    cp_async_8(cdst + (G + u) * NT, ru);
-                    rl -= cstride;
-                    ru += cstride;
+                    cp_async_8(cdst + u * NT, rp_);
+                    rp_ += br;
                 }
             }
             if (++ig == per_round) {
                 ig = 0;
                 if (++ir < rounds) {
                     ic = column(ir);
-                    xl = xin + ic.col;
-                    xu = xin + ic.col + (size_t)(nz - 1) * stride;
-                    ml = tm + ic.cls;
-                    mu = tm + ic.cls + (size_t)(nz - 1) * cstride;
-                    rl = tr + ic.cls + (size_t)(p - 1) * cstride;
-                    ru = tr + ic.cls + (size_t)p * cstride;
+                    xp_ = xin + ic.col + kx0 * stride;
+                    mp_ = tm + ic.cls + kx0 * cstride;
+                    rp_ = tr + ic.cls + kr0 * cstride;
                 }
             }
         }
@@ -997,91 +996,90 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
     int slot = 0;
     for (int r = 0; r < rounds; r++) {
         const TtmColumn cc = column(r);
-        const bool zr = zcta && r == 0; // warp-uniform
+        const bool zr = zcta && r == 0 && lt == 0;
         // the junction's 2x2 coefficients, needed after the forward sweep
         const double jE = __ldg(tm + cc.cls + (size_t)nz * cstride), jC = __ldg(tm + cc.cls + (size_t)(nz + 1) * cstride);
         const double jD = __ldg(tr + cc.cls + (size_t)nz * cstride), jA = __ldg(tr + cc.cls + (size_t)(nz + 1) * cstride);
-        // forward: xs_k = r_k - m_k xs_{k-1} (lower, k = 0 .. p-1) and
-        // ys_k = r_k - m_k ys_{k+1} (upper, k = nz-1 .. p)
-        double sl = 0.0, su = 0.0;
+        // forward: s_k = r_k - m_k s_{k -+ 1} from this half's wall
+        double s = 0.0;
         for (int g = 0; g < ngh; g++) {
             cp_async_wait<NS - 2>(); // this step's group has landed
-            const double *cs = cring + slot * R * NT + tid;
-            const T *xs = xring + slot * R * NT + tid;
-            double xvl[G], mvl[G], xvu[G], mvu[G];
+            const double *cs = cring + slot * G * NT + tid;
+            const T *xs = xring + slot * G * NT + tid;
+            double xv[G], mv[G];
 #pragma unroll
             for (int u = 0; u < G; u++) {
-                xvl[u] = (double)xs[u * NT];
-                xvu[u] = (double)xs[(G + u) * NT];
-                mvl[u] = cs[u * NT];
-                mvu[u] = cs[(G + u) * NT];
+                xv[u] = (double)xs[u * NT];
+                mv[u] = cs[u * NT];
             }
-            if (zr && tid == 0) {
+            if (zr) {
 #pragma unroll
-                for (int u = 0; u < G; u++) {
-                    xvl[u] = zring[slot * R + u];
-                    xvu[u] = zring[slot * R + G + u];
-                }
+                for (int u = 0; u < G; u++) xv[u] = zring[(slot * 2 + half) * G + u];
             }
             issue_next(); // refills the slot consumed one step ago
-            uint32_t vl[2 * G], vu[2 * G];
+            double sv[G];
 #pragma unroll
-            for (int u = 0; u < G; u++) {
-                sl = xvl[u] - mvl[u] * sl;
-                su = xvu[u] - mvu[u] * su;
-                vl[2 * u] = (uint32_t)__double2loint(sl);
-                vl[2 * u + 1] = (uint32_t)__double2hiint(sl);
-                const int i = G - 1 - u; // upper row nz-1 - g G - u is cell pair i of its block
-                vu[2 * i] = (uint32_t)__double2loint(su);
-                vu[2 * i + 1] = (uint32_t)__double2hiint(su);
+            for (int u = 0; u < G; u++) sv[u] = s = xv[u] - mv[u] * s;
+            // cells of the 8-row block in ascending row order: the upper
+            // half walks its rows downwards (two branches, so that every
+            // index is a constant and the block stays in registers)
+            uint32_t v[2 * G];
+            if (half) {
+#pragma unroll
+                for (int u = 0; u < G; u++) {
+                    v[2 * (G - 1 - u)] = (uint32_t)__double2loint(sv[u]);
+                    v[2 * (G - 1 - u) + 1] = (uint32_t)__double2hiint(sv[u]);
+                }
+            } else {
+#pragma unroll
+                for (int u = 0; u < G; u++) {
+                    v[2 * u] = (uint32_t)__double2loint(sv[u]);
+                    v[2 * u + 1] = (uint32_t)__double2hiint(sv[u]);
+                }
             }
             __syncwarp();
-            tmem_st16(tbase + 2 * (g * G), vl);
-            tmem_st16(tbase + 2 * (nz - G - g * G), vu);
+            tmem_st16(tbase + 2 * (half ? p - G - g * G : g * G), v);
             slot = (slot + 1 == NS) ? 0 : slot + 1;
         }
         tmem_wait_st();
-        // rows p-1 and p from the joining 2x2 system
-        const double xa = sl * jE - su * jC, xb = su * jD - sl * jA;
-        // backward: x_k = (xs_k - c_k x_{k+1}) / d_k below, x_k = (ys_k - a_k x_{k-1}) / e_k above
-        double wl = 0.0, wu = 0.0;
-        T *dl = xout + cc.col + (size_t)(p - 1) * stride, *du = xout + cc.col + (size_t)p * stride;
+        // rows p-1 and p from the 2x2 system that joins the halves
+        double *jr = jv + (r & 1) * 2 * NC;
+        jr[half * NC + lt] = s;
+        __syncthreads();
+        const double xs_ = jr[lt], ys_ = jr[NC + lt];
+        const double xj = half ? ys_ * jD - xs_ * jA : xs_ * jE - ys_ * jC;
+        // backward from the middle: x_k = (s_k - c_k x_{k+1}) / d_k below,
+        // x_k = (s_k - a_k x_{k-1}) / e_k above
+        double w = 0.0;
+        T *dst = xout + cc.col + kr0 * stride;
         for (int h = 0; h < ngh; h++) {
-            uint32_t vl[2 * G], vu[2 * G];
+            uint32_t v[2 * G];
             __syncwarp();
-            tmem_ld16_start(tbase + 2 * (p - G - h * G), vl); // rows p-G-hG .. p-1-hG
-            tmem_ld16_start(tbase + 2 * (p + h * G), vu);     // rows p+hG .. p+hG+G-1
+            tmem_ld16_start(tbase + 2 * (half ? h * G : p - G - h * G), v);
             cp_async_wait<NS - 2>();
-            const double *cs = cring + slot * R * NT + tid;
-            double rvl[G], rvu[G], cvl[G], avu[G];
+            const double *cs = cring + slot * G * NT + tid;
+            double rv[G], cf[G];
 #pragma unroll
             for (int u = 0; u < G; u++) {
-                rvl[u] = cs[u * NT];
-                rvu[u] = cs[(G + u) * NT];
-                cvl[u] = csh[p - 1 - h * G - u];
-                avu[u] = ash[p + h * G + u];
+                rv[u] = cs[u * NT];
+                cf[u] = half ? ash[p + h * G + u] : csh[p - 1 - h * G - u];
             }
             issue_next();
-            tmem_wait_ld(vl);
-            tmem_wait_ld(vu);
+            tmem_wait_ld(v);
+            double sv[G];
+            if (half) {
+#pragma unroll
+                for (int u = 0; u < G; u++) sv[u] = __hiloint2double((int)v[2 * u + 1], (int)v[2 * u]);
+            } else {
+#pragma unroll
+                for (int u = 0; u < G; u++)
+                    sv[u] = __hiloint2double((int)v[2 * (G - 1 - u) + 1], (int)v[2 * (G - 1 - u)]);
+            }
 #pragma unroll
             for (int u = 0; u < G; u++) {
-                const int i = G - 1 - u;
-                const double xsl = __hiloint2double((int)vl[2 * i + 1], (int)vl[2 * i]);
-                const double xsu = __hiloint2double((int)vu[2 * u + 1], (int)vu[2 * u]);
-                if (u == 0 && h == 0) {
-                    wl = xa;
-                    wu = xb;
-                } else {
-                    wl = (xsl - cvl[u] * wl) * rvl[u];
-                    wu = (xsu - avu[u] * wu) * rvu[u];
-                }
-                if (cc.valid) {
-                    *dl = (T)wl;
-                    *du = (T)wu;
-                }
-                dl -= stride;
-                du += stride;
+                w = (u == 0 && h == 0) ? xj : (sv[u] - cf[u] * w) * rv[u];
+                if (cc.valid) *dst = (T)w;
+                dst -= fx;
             }
             slot = (slot + 1 == NS) ? 0 : slot + 1;
         }
@@ -1561,8 +1559,8 @@ static int launch_x_ct(const Ppe *s, const T *in, size_t in_off, size_t in_sj, s
 template <typename T, int N, bool FWD> static int launch_y_ct(const Ppe *s, T *data, cudaStream_t st)
 {
     using V = typename cplx_of<T>::type;
-    constexpr int W = pf_y_cols<V, N>();
-    const size_t shm = sizeof(V) * (size_t)pf_y_smem_elems<T, N>();
+    constexpr int W = pf_y_cols<V, N, FWD>();
+    const size_t shm = sizeof(V) * (size_t)pf_y_smem_elems<T, N, FWD>();
     if (shm > 48 * 1024)
         PL_CUDA_TRY(cudaFuncSetAttribute(k_yfft_pf<T, N, FWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
     const V *tw = reinterpret_cast<const V *>(sizeof(T) == 8 ? (const void *)s->d_twy64 : (const void *)s->d_twy32);
@@ -1661,15 +1659,16 @@ template <typename T> static int launch_trid(Ppe *s, T *x, cudaStream_t st, cons
     dim3 grid((s->nx + 127) / 128, s->ny);
     if (sizeof(T) == 4 && s->nparts == 0 && s->d_tmult != nullptr) {
         // the two-ended sweep (mixed path): two chains per column
-        const size_t shm = ttw_smem_bytes<T>();
+        // (one thread per half column: k_thomas_th)
+        const size_t shm = tth_smem_bytes<T>();
         const int ncol = s->nx * s->ny;
         const int ctas = std::max(1, std::min(sm_count(), (ncol + TTM_THREADS - 1) / TTM_THREADS));
         const int rounds = (ncol + ctas * TTM_THREADS - 1) / (ctas * TTM_THREADS);
         uint32_t tcols = 32;
         while (tcols < 2u * (uint32_t)s->nz) tcols *= 2;
-        PL_CUDA_TRY(cudaFuncSetAttribute(k_thomas_tw<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
-        k_thomas_tw<T><<<ctas, TTM_THREADS, shm, st>>>(x, x, s->d_tmult, s->d_trb, s->d_a, s->d_c, s->nx, s->ny, s->nz,
-                                                         s->ncx, s->ncy, mode0, rounds, tcols);
+        PL_CUDA_TRY(cudaFuncSetAttribute(k_thomas_th<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        k_thomas_th<T><<<ctas, 2 * TTM_THREADS, shm, st>>>(x, x, s->d_tmult, s->d_trb, s->d_a, s->d_c, s->nx, s->ny,
+                                                             s->nz, s->ncx, s->ncy, mode0, rounds, tcols);
         PL_CHECK_LAUNCH();
         return 0;
     }

@@ -63,7 +63,7 @@ extern "C" int host_trid_solve(int nx, int ny, int nz, double dx, double dy, con
     return 0;
 }
 
-// the two-ended sweep of k_thomas_tw (mixed path): the LU elimination on rows
+// the two-ended sweep of k_thomas_th (mixed path): the LU elimination on rows
 // below p = nz/2, the elimination from the top wall on rows p .. nz-1, the
 // 2x2 system of rows p-1 and p, back substitution outwards (nz even)
 extern "C" int host_trid_solve_twisted(int nx, int ny, int nz, double dx, double dy, const double *dzf, double *x)

@@ -84,7 +84,7 @@ GOLDEN_THOMAS = [p for p in GOLDEN_PPE if not int(np.load(p)["pdd"]) and int(np.
 
 @pytest.mark.parametrize("path", GOLDEN_THOMAS, ids=[os.path.basename(p)[:-4] for p in GOLDEN_THOMAS])
 def test_twisted_sweep_matches_reference_thomas(path):
-    """The mixed path's two-ended sweep (k_thomas_tw's column algorithm, its
+    """The mixed path's two-ended sweep (k_thomas_th's column algorithm, its
     tables from the same builder) against the reference's own Thomas solve:
     the same solution up to rounding, modulo the Neumann null mode's constant
     (its gauge is x_p = 0 at the middle row instead of the reference's
