@@ -7,7 +7,7 @@
  * (powerllel_channel_b200/) links or calls this code.
  *
  * The reference calls FFTW_R2HC / FFTW_HC2R through fftw_plan_guru_r2r
- * (src/src_c/mod_fft_fftw.inc:66-84,123-148) for the periodic ("PP")
+ * (src/src_c/mod_fft_fftw.inc:1-5, 56-63, 76-83) for the periodic ("PP")
  * directions.  Their published definitions (FFTW manual, "The Halfcomplex-format
  * DFT" and "Real even/odd DFTs"):
  *

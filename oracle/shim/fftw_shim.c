@@ -4,7 +4,7 @@
  * TEST INFRASTRUCTURE ONLY.
  *
  * Plan semantics follow the FFTW3 guru interface as the reference uses it
- * (src/src_c/mod_fft_fftw.inc:106-148): one transform dimension
+ * (src/src_c/mod_fft_fftw.inc:35-95): one transform dimension
  * {n, is, os} and one "howmany" loop dimension {n, is, os}; in-place
  * (in == out).  Execution may be called concurrently on different arrays
  * (the reference calls it inside OpenMP loops), so a plan holds no scratch.
