@@ -69,17 +69,17 @@ def set_config(name):
 # the transform written once)
 ALG_BYTES = {
     "fp64": {"rk_fused": 48, "rk1": 48, "rk2": 72, "calc_rhs": 32, "rhs_xfft": 32, "ppe_xfft_fwd": 16, "ppe_yfft_fwd": 16,
-             "ppe_thomas": 20, "ppe_pdd": 40, "ppe_yfft_bwd": 16, "ppe_xfft_bwd": 16, "correct_force": 56},
+             "ppe_thomas": 20, "ppe_pdd": 24, "ppe_yfft_bwd": 16, "ppe_xfft_bwd": 16, "correct_force": 56},
     "mixed": {"rk_fused": 52, "rk1": 36, "rk2": 64, "calc_rhs": 28, "rhs_xfft": 28, "ppe_xfft_fwd": 8, "ppe_yfft_fwd": 8,
-              "ppe_thomas": 12, "ppe_pdd": 32, "ppe_yfft_bwd": 8, "ppe_xfft_bwd": 24, "correct_force": 52},
+              "ppe_thomas": 12, "ppe_pdd": 16, "ppe_yfft_bwd": 8, "ppe_xfft_bwd": 24, "correct_force": 52},
 }
 # mixed: rk_fused reads u (FP64) and the FP32 pressure prediction and writes
 # u_hat (FP64): 24 + 4 + 24; ppe_xfft_bwd reads the FP32 half-complex line and
 # writes the FP32 increment, plus the FP32 pressure update (reads the
 # prediction and p_n, writes p_n+1 and the next prediction): 4 + 4 + 16
-# kernel launches per step (this library's kernels only), Thomas; PDD adds
-# the mixed path's widening of the FP32 right-hand side into the FP64 sweep
-# buffer (the FP64 path copies it with cudaMemcpyAsync)
+# kernel launches per step (this library's kernels only), Thomas, and PDD up
+# to 32 partitions (one kernel); PDD over more partitions adds the mixed
+# path's widening of the FP32 right-hand side into the FP64 sweep buffer
 LAUNCHES = {"fp64": 7, "mixed": 8}
 
 
@@ -496,7 +496,7 @@ def run_b200(args):
             "accuracy_after_100_steps": acc,
             "clocks": clkm, "clocks_fp64": clk64,
             "e2e": {"value": e2e_sps, "unit": "steps/s", "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
-            "gpu_launches": (LAUNCHES["mixed"] + (1 if PARTS else 0)) * args.steps,
+            "gpu_launches": (LAUNCHES["mixed"] + (1 if PARTS > 32 else 0)) * args.steps,
             "roofline": {"bound": "hbm", "kernel": top[0], "achieved": round(achieved, 1), "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                          "traffic": traffic, "alg_bytes": alg},

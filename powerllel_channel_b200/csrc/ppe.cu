@@ -553,9 +553,10 @@ template <typename T> __host__ __device__ constexpr int trid_unroll() { return s
 
 // Thomas on rows [k0, k0+ke) of one column.  Reads the right-hand side from
 // `xin` (type T), keeps the forward-swept values in `xs` (double; may alias
-// xin when T is double) and writes the solution to `xout` (type T).
-template <typename T>
-__device__ __forceinline__ void thomas_column(const T *xin, double *xs, T *xout, size_t col, size_t cls,
+// xin when T is double) and writes the solution to `xout` (type TO, T by
+// default; may alias xs).
+template <typename T, typename TO = T>
+__device__ __forceinline__ void thomas_column(const T *xin, double *xs, TO *xout, size_t col, size_t cls,
                                               size_t stride, size_t cstride, int k0, int ke, const TridDev &t)
 {
     constexpr int TRID_UNROLL = trid_unroll<T>();
@@ -583,7 +584,7 @@ __device__ __forceinline__ void thomas_column(const T *xin, double *xs, T *xout,
     // last row: x /= b, or 0 where b == 0 (:332-344); rb holds 1/b or 0
     const int kl = k0 + ke - 1;
     xp = xp * __ldg(t.rb + cls + (size_t)kl * cstride);
-    xout[col + (size_t)kl * stride] = (T)xp;
+    xout[col + (size_t)kl * stride] = (TO)xp;
     // back substitution: x_k = (x_k - c_k x_{k+1}) / b_k   (:346-356)
     for (int kb = ke - 2; kb >= 0; kb -= TRID_UNROLL) {
         double xv[TRID_UNROLL], rv[TRID_UNROLL];
@@ -600,7 +601,7 @@ __device__ __forceinline__ void thomas_column(const T *xin, double *xs, T *xout,
             const int k = k0 + kb - u;
             if (kb - u >= 0) {
                 xp = (xv[u] - __ldg(t.c + k) * xp) * rv[u];
-                xout[col + (size_t)k * stride] = (T)xp;
+                xout[col + (size_t)k * stride] = (TO)xp;
             }
         }
     }
@@ -1160,6 +1161,62 @@ __global__ void __launch_bounds__(128) k_pdd(double *xs, T *xout, TridDev t, Pdd
     }
 }
 
+// PDD with one thread per (column, partition), P <= 32: a 32 x P block
+// holds 32 adjacent columns (coalesced rows) and all their partitions.  Each
+// thread solves its partition's local system, reading the right-hand side
+// (FP32 or FP64) straight from the transform array; after the block's
+// barrier it forms the interface systems on both sides of its partition
+// from the neighbours' rows of the FP64 sweep buffer (y1 from the interface
+// below, y2 from the one above) and corrects its own rows.  The values are
+// k_pdd's, expression for expression; P threads per column instead of one
+// run the local sweeps side by side, and no widening or copy of the
+// right-hand side precedes them.
+template <typename T>
+__global__ void __launch_bounds__(1024) k_pdd_par(const T *xin, double *xs, T *xout, TridDev t, PddDev p,
+                                                  const double *mode0)
+{
+    const int m = threadIdx.y;
+    const int q = blockIdx.x * 32 + threadIdx.x, ncol = t.nx * t.ny;
+    const bool valid = q < ncol;
+    const int qq = valid ? q : 0, px = qq % t.nx, py = qq / t.nx;
+    const size_t col = (size_t)qq, stride = (size_t)t.nx * t.ny;
+    const size_t cls = trid_class(px, py, t), cstride = (size_t)t.ncx * t.ncy;
+    const int k0 = p.kst[m], ke = p.ksz[m];
+    if (valid) {
+        if (mode0 != nullptr && col == 0) { // mixed path: the (0,0) column from the FP64 plane sums
+            for (int k = k0; k < k0 + ke; k++) xs[(size_t)k * stride] = mode0[k];
+            thomas_column<double>(xs, xs, xs, col, cls, stride, cstride, k0, ke, t);
+        } else {
+            thomas_column<T, double>(xin, xs, xs, col, cls, stride, cstride, k0, ke, t);
+        }
+    }
+    __syncthreads();
+    if (!valid) return;
+    // the truncated 2x2 system at the top of partition mm (:423-438)
+    auto iface = [&](int mm, double &y2, double &y3) {
+        const int kt = p.kst[mm] + p.ksz[mm] - 1;
+        const double wt = __ldg(p.w + cls + (size_t)kt * cstride);
+        const double tv = __ldg(p.tmpv + cls + (size_t)mm * cstride);
+        const double xt = xs[col + (size_t)kt * stride];
+        const double tvar = xs[col + (size_t)p.kst[mm + 1] * stride];
+        const double det = wt * tv - 1.0;
+        y2 = (xt * tv - tvar) / det;
+        y3 = (tvar * wt - xt) / det;
+        if (pdd_gauge00(mode0, col, p.nparts)) {
+            y2 = tvar;
+            y3 = 0.0;
+        }
+    };
+    double y1 = 0.0, y2 = 0.0, unused;
+    if (m > 0) iface(m - 1, unused, y1); // y3 of the interface below is this partition's y1 (:444-446)
+    if (m + 1 < p.nparts) iface(m, y2, unused);
+    for (int k = k0; k < k0 + ke; k++) {
+        const size_t g = col + (size_t)k * stride;
+        const size_t gc = cls + (size_t)k * cstride;
+        xout[g] = (T)(xs[g] - __ldg(p.v + gc) * y1 - __ldg(p.w + gc) * y2);
+    }
+}
+
 // PDD of one z slab per GPU (psolve_trid, mod_poisson_solver.c:361-466, for
 // the rank that holds the partition): the local sweep, the interface solve
 // with the upper neighbour, and the correction, as three kernels around the
@@ -1696,6 +1753,19 @@ template <typename T> static int launch_trid(Ppe *s, T *x, cudaStream_t st, cons
         }
     } else if (s->nparts == 0) {
         k_thomas<T><<<grid, 128, 0, st>>>(x, xs, x, t, mode0);
+    } else if (s->nparts <= 32) {
+        PddDev p{};
+        p.nparts = s->nparts;
+        for (int m = 0; m < s->nparts; m++) {
+            p.kst[m] = s->kst[m];
+            p.ksz[m] = s->ksz[m];
+        }
+        p.v = s->d_v;
+        p.w = s->d_w;
+        p.tmpv = s->d_tmpv;
+        const int ncol = s->nx * s->ny;
+        k_pdd_par<T><<<(ncol + 31) / 32, dim3(32, s->nparts), 0, st>>>(x, s->d_scratch, x, t, p,
+                                                                      sizeof(T) == 4 ? mode0 : nullptr);
     } else {
         if (sizeof(T) == 4) {
             k_widen<<<1184, 256, 0, st>>>(reinterpret_cast<const float *>(x), xs, s->scratch_elems);
