@@ -1217,6 +1217,140 @@ __global__ void __launch_bounds__(1024) k_pdd_par(const T *xin, double *xs, T *x
     }
 }
 
+// PDD with one thread per (column, partition) and each partition's swept
+// values in tensor memory (P <= 8, every partition a multiple of 8 rows):
+// the local sweep writes its forward-swept rows to the thread's lane, the
+// back substitution reads them and writes the local solution over them, and
+// the correction reads that; HBM sees the right-hand side, the solution and
+// the class tables only.  Warp m holds partition m (lane quarter m % 4;
+// warps m and m+4 use the next 2 kmax cells).  The partitions' first and
+// last local values meet in shared memory for the interface systems.  The
+// values are k_pdd's, expression for expression.
+constexpr int PTM_G = 8;
+
+__host__ __device__ constexpr int pdd_tm_static_smem() { return 2 * 8 * 32 * 8 + 16; }
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_pdd_tm(const T *xin, T *xout, TridDev t, PddDev p, const double *mode0,
+                                                int kmax, uint32_t tcols)
+{
+    constexpr int G = PTM_G;
+    __shared__ double edge[2][8][32]; // [first / last local value][partition][column]
+    __shared__ uint32_t tslot;
+    const int cx = threadIdx.x, m = threadIdx.y;
+    const int q = blockIdx.x * 32 + cx, ncol = t.nx * t.ny;
+    const bool valid = q < ncol;
+    const int qq = valid ? q : 0, px = qq % t.nx, py = qq / t.nx;
+    const size_t col = (size_t)qq, stride = (size_t)t.nx * t.ny;
+    const size_t cls = trid_class(px, py, t), cstride = (size_t)t.ncx * t.ncy;
+    const int k0 = p.kst[m], ke = p.ksz[m], ng = ke / G;
+    const bool z = mode0 != nullptr && valid && col == 0; // mixed path: the (0,0) column from the plane sums
+
+    if (m == 0) tmem_alloc(&tslot, tcols);
+    tmem_fence_before_sync();
+    __syncthreads();
+    tmem_fence_after_sync();
+    const uint32_t tb = tslot + ((uint32_t)((m & 3) * 32) << 16) + (uint32_t)((m >> 2) * 2 * kmax);
+
+    // forward elimination of the partition (ssolve_trid :319-330; the
+    // multiplier is 0 at its first row)
+    double xp = 0.0;
+    for (int g = 0; g < ng; g++) {
+        double xv[G], mv[G];
+#pragma unroll
+        for (int u = 0; u < G; u++) {
+            const int k = k0 + g * G + u;
+            xv[u] = z ? mode0[k] : (double)xin[col + (size_t)k * stride];
+            mv[u] = __ldg(t.mult + cls + (size_t)k * cstride);
+        }
+        uint32_t v[2 * G];
+#pragma unroll
+        for (int u = 0; u < G; u++) {
+            xp = xv[u] - mv[u] * xp;
+            v[2 * u] = (uint32_t)__double2loint(xp);
+            v[2 * u + 1] = (uint32_t)__double2hiint(xp);
+        }
+        __syncwarp();
+        tmem_st16(tb + 2 * g * G, v);
+    }
+    tmem_wait_st();
+    // back substitution (:332-356): x = (x - c x_{k+1}) / b, with x_{k+1} = 0
+    // above the partition's last row; the local solution replaces the swept rows
+    double w = 0.0, first = 0.0, last = 0.0;
+    for (int g = ng - 1; g >= 0; g--) {
+        uint32_t v[2 * G];
+        __syncwarp();
+        tmem_ld16_start(tb + 2 * g * G, v);
+        double rv[G], cv[G];
+#pragma unroll
+        for (int u = 0; u < G; u++) {
+            const int k = k0 + g * G + u;
+            rv[u] = __ldg(t.rb + cls + (size_t)k * cstride);
+            cv[u] = __ldg(t.c + k);
+        }
+        tmem_wait_ld(v);
+#pragma unroll
+        for (int u = G - 1; u >= 0; u--) {
+            const double s = __hiloint2double((int)v[2 * u + 1], (int)v[2 * u]);
+            w = (s - cv[u] * w) * rv[u];
+            if (g == ng - 1 && u == G - 1) last = w;
+            v[2 * u] = (uint32_t)__double2loint(w);
+            v[2 * u + 1] = (uint32_t)__double2hiint(w);
+        }
+        __syncwarp();
+        tmem_st16(tb + 2 * g * G, v);
+    }
+    first = w;
+    tmem_wait_st();
+    edge[0][m][cx] = first;
+    edge[1][m][cx] = last;
+    __syncthreads();
+    // the truncated 2x2 systems at the partition's two interfaces (:423-438)
+    auto iface = [&](int mm, double &y2, double &y3) {
+        const int kt = p.kst[mm] + p.ksz[mm] - 1;
+        const double wt = __ldg(p.w + cls + (size_t)kt * cstride);
+        const double tv = __ldg(p.tmpv + cls + (size_t)mm * cstride);
+        const double xt = edge[1][mm][cx], tvar = edge[0][mm + 1][cx];
+        const double det = wt * tv - 1.0;
+        y2 = (xt * tv - tvar) / det;
+        y3 = (tvar * wt - xt) / det;
+        if (pdd_gauge00(mode0, col, p.nparts)) {
+            y2 = tvar;
+            y3 = 0.0;
+        }
+    };
+    double y1 = 0.0, y2 = 0.0, unused;
+    if (m > 0) iface(m - 1, unused, y1);
+    if (m + 1 < p.nparts) iface(m, y2, unused);
+    // correction x = x_local - v y1 - w y2 (:452-464)
+    for (int g = 0; g < ng; g++) {
+        uint32_t v[2 * G];
+        __syncwarp();
+        tmem_ld16_start(tb + 2 * g * G, v);
+        double vv[G], wv[G];
+#pragma unroll
+        for (int u = 0; u < G; u++) {
+            const size_t gc = cls + (size_t)(k0 + g * G + u) * cstride;
+            vv[u] = __ldg(p.v + gc);
+            wv[u] = __ldg(p.w + gc);
+        }
+        tmem_wait_ld(v);
+        if (valid) {
+#pragma unroll
+            for (int u = 0; u < G; u++) {
+                const double x = __hiloint2double((int)v[2 * u + 1], (int)v[2 * u]);
+                xout[col + (size_t)(k0 + g * G + u) * stride] = (T)(x - vv[u] * y1 - wv[u] * y2);
+            }
+        }
+    }
+    tmem_fence_before_sync();
+    __syncthreads();
+    if (m == 0) {
+        tmem_fence_after_sync();
+        tmem_free(tslot, tcols);
+    }
+}
+
 // PDD of one z slab per GPU (psolve_trid, mod_poisson_solver.c:361-466, for
 // the rank that holds the partition): the local sweep, the interface solve
 // with the upper neighbour, and the correction, as three kernels around the
@@ -1756,16 +1890,34 @@ template <typename T> static int launch_trid(Ppe *s, T *x, cudaStream_t st, cons
     } else if (s->nparts <= 32) {
         PddDev p{};
         p.nparts = s->nparts;
+        int kmax = 0;
+        bool groups = true;
         for (int m = 0; m < s->nparts; m++) {
             p.kst[m] = s->kst[m];
             p.ksz[m] = s->ksz[m];
+            kmax = std::max(kmax, s->ksz[m]);
+            groups = groups && s->ksz[m] >= PTM_G && s->ksz[m] % PTM_G == 0;
         }
         p.v = s->d_v;
         p.w = s->d_w;
         p.tmpv = s->d_tmpv;
         const int ncol = s->nx * s->ny;
-        k_pdd_par<T><<<(ncol + 31) / 32, dim3(32, s->nparts), 0, st>>>(x, s->d_scratch, x, t, p,
-                                                                      sizeof(T) == 4 ? mode0 : nullptr);
+        const int cells = ((s->nparts + 3) / 4) * 2 * kmax; // TMEM columns of one CTA
+        if (groups && s->nparts <= 8 && cells <= 512) {
+            // partitions in tensor memory; the dynamic shared memory (unused)
+            // caps the CTAs on an SM at what its 512 TMEM columns hold
+            uint32_t tcols = 32;
+            while (tcols < (uint32_t)cells) tcols *= 2;
+            const int per_sm = std::max(1, std::min(512 / (int)tcols, 2048 / (32 * s->nparts)));
+            const int dyn = std::max(0, 233472 / per_sm - 1024 - pdd_tm_static_smem() - 512);
+            if (dyn > 48 * 1024)
+                PL_CUDA_TRY(cudaFuncSetAttribute(k_pdd_tm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+            k_pdd_tm<T><<<(ncol + 31) / 32, dim3(32, s->nparts), dyn, st>>>(x, x, t, p, sizeof(T) == 4 ? mode0 : nullptr,
+                                                                             kmax, tcols);
+        } else {
+            k_pdd_par<T><<<(ncol + 31) / 32, dim3(32, s->nparts), 0, st>>>(x, s->d_scratch, x, t, p,
+                                                                          sizeof(T) == 4 ? mode0 : nullptr);
+        }
     } else {
         if (sizeof(T) == 4) {
             k_widen<<<1184, 256, 0, st>>>(reinterpret_cast<const float *>(x), xs, s->scratch_elems);
