@@ -95,11 +95,16 @@ def test_device_ppe_vs_golden(gpu, path):
 # for nz <= 256 (768x32x256: two rounds of columns per CTA; 16x8x8: one 8-row
 # group, exactly one CTA of 128 columns; 8x6x16: one CTA with 80 idle
 # threads), 256 of them for taller columns with the rest in HBM (32x24x264,
-# 32x24x512); in HBM alone for other nz
+# 32x24x512); in HBM alone for other nz.  PDD: each partition in tensor
+# memory for up to 8 partitions of multiples of 8 rows (256x192x32/4,
+# 64x48x32/2), one thread per (column, partition) with the swept values in
+# HBM otherwise up to 32 partitions (64x48x40/8, 96x72x30/4, 32x24x96/12,
+# 32x24x100/12), one thread per column beyond (32x24x96/40)
 @pytest.mark.parametrize("nx,ny,nz,nparts", [(64, 64, 64, 0), (128, 96, 48, 0), (256, 192, 32, 4),
                                             (64, 48, 40, 8), (96, 72, 30, 4), (64, 48, 32, 2),
                                             (64, 48, 30, 0), (32, 24, 264, 0), (768, 32, 256, 0),
-                                            (16, 8, 8, 0), (8, 6, 16, 0), (32, 24, 512, 0)])
+                                            (16, 8, 8, 0), (8, 6, 16, 0), (32, 24, 512, 0),
+                                            (32, 24, 96, 12), (32, 24, 100, 12), (32, 24, 96, 40)])
 def test_ppe_vs_oracle_live(gpu, oracle_mod, nx, ny, nz, nparts):
     """Sizes beyond the fixtures (radix-3 lengths, uneven PDD partitions)."""
     import torch
