@@ -691,9 +691,13 @@ struct TtmColumn {
 
 // TALL: nz > TTM_TM_ROWS (the HBM-scratch rows exist); a compile-time switch,
 // so that shorter columns run the tensor-memory path alone
-template <typename T, bool TALL>
+// TO: the solution's type (T by default; the slab sweep writes FP64).
+// GAUGE: the (0,0) column (mode0 given) takes x[nz-1] = 0, the free
+// constant of the singular whole-column system; a slab's partition system is
+// regular and solves that column from the plane sums without it.
+template <typename T, bool TALL, typename TO = T, bool GAUGE = true>
 __global__ void __launch_bounds__(TTM_THREADS, 1)
-    k_thomas_tmem(const T *xin, T *xout, double *xsc, TridDev t, const double *mode0, int rounds, uint32_t tcols)
+    k_thomas_tmem(const T *xin, TO *xout, double *xsc, TridDev t, const double *mode0, int rounds, uint32_t tcols)
 {
     constexpr int G = TTM_G, NS = TTM_NS, NT = TTM_THREADS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -831,7 +835,7 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
         // (:346-356); at k = nz-1, with x_{nz} = 0, it is x /= b (:332-344),
         // and the (0,0) mode takes the gauge x[nz-1] = 0 there
         xp = 0.0;
-        T *dst = xout + cc.col + (size_t)(nz - 1) * stride;
+        TO *dst = xout + cc.col + (size_t)(nz - 1) * stride;
         for (int h = 0; h < ngf; h++) {
             const int ktop = nz - 1 - h * G; // rows ktop, ktop-1, ..., ktop-G+1
             uint32_t v[2 * G];
@@ -848,7 +852,7 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
                 rv[u] = cs[u * NT];
                 cv[u] = csh[ktop - u];
             }
-            if (zr && tid == 0 && h == 0) rv[0] = 0.0;
+            if (GAUGE && zr && tid == 0 && h == 0) rv[0] = 0.0;
             issue_next();
             if (!hb) tmem_wait_ld(v);
             const double *ss = sring + slot * G * NT + tid;
@@ -857,7 +861,7 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
                 const int i = G - 1 - u;
                 const double x = hb ? ss[u * NT] : __hiloint2double((int)v[2 * i + 1], (int)v[2 * i]);
                 xp = (x - cv[u] * xp) * rv[u];
-                if (cc.valid) *dst = (T)xp;
+                if (cc.valid) *dst = (TO)xp;
                 dst -= stride;
             }
             slot = (slot + 1 == NS) ? 0 : slot + 1;
@@ -2037,6 +2041,23 @@ template <typename T> int ppe_slab_forward_from_x(Ppe *s, T *d_var, cudaStream_t
 {
     if (launch_y<T>(s, true, d_var, st)) return -1;
     mark(s, "ppe_yfft_fwd");
+    if (s->nz % TTM_G == 0 && s->nz <= TTM_TM_ROWS) {
+        // the partition's sweep in tensor memory, reading the right-hand side
+        // as stored and writing the local solution to the FP64 sweep buffer
+        TridDev t{s->nx, s->ny, s->nz, s->ncx, s->ncy, s->d_mult, s->d_rb, s->d_c};
+        const size_t shm = ttm_smem_bytes<T>(s->nz);
+        const int ncol = s->nx * s->ny;
+        const int ctas = std::max(1, std::min(sm_count(), (ncol + TTM_THREADS - 1) / TTM_THREADS));
+        const int rounds = (ncol + ctas * TTM_THREADS - 1) / (ctas * TTM_THREADS);
+        uint32_t tcols = 32;
+        while (tcols < 2u * (uint32_t)s->nz) tcols *= 2;
+        auto kern = k_thomas_tmem<T, false, double, false>;
+        PL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        kern<<<ctas, TTM_THREADS, shm, st>>>(d_var, s->d_scratch, s->d_scratch, t, mode0, rounds, tcols);
+        PL_CHECK_LAUNCH();
+        mark(s, "ppe_pdd_sweep");
+        return 0;
+    }
     if (sizeof(T) == 4) {
         k_widen<<<1184, 256, 0, st>>>(reinterpret_cast<const float *>(d_var), s->d_scratch, s->scratch_elems);
         PL_CHECK_LAUNCH();
