@@ -880,7 +880,8 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
 constexpr int TTW_G = 8;
 
 // Two-ended Thomas with one thread per half column (mixed path; 16 <= nz <=
-// 256, nz % 16 == 0), the tables TridTables::tmult and trb.  A 256-thread CTA solves 128
+// 256, nz % 16 == 0), the tables TridTables::tmult and trb (rows of tcs
+// values).  A 256-thread CTA solves 128
 // columns per round: threads 0-127 sweep the lower halves (rows 0 .. p-1, the
 // LU elimination), threads 128-255 the upper halves (rows nz-1 .. p, the
 // elimination from the top wall), each thread one chain of nz steps.  Both
@@ -906,7 +907,8 @@ template <typename T> __host__ __device__ constexpr size_t tth_smem_bytes()
 template <typename T>
 __global__ void __launch_bounds__(2 * TTM_THREADS, 1)
     k_thomas_th(const T *xin, T *xout, const double *tm, const double *tr, const double *ak, const double *ck,
-                int nx, int ny, int nz, int ncx, int ncy, const double *mode0, int rounds, uint32_t tcols)
+                int nx, int ny, int nz, int ncx, int ncy, long long tcs, const double *mode0, int rounds,
+                uint32_t tcols)
 {
     constexpr int G = TTW_G, NS = TTH_NS, NC = TTM_THREADS, NT = 2 * NC;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -919,7 +921,7 @@ __global__ void __launch_bounds__(2 * TTM_THREADS, 1)
     uint32_t *tslot = reinterpret_cast<uint32_t *>(jv + 4 * NC);
     const int tid = threadIdx.x, warp = tid >> 5, half = tid >= NC ? 1 : 0, lt = tid - half * NC;
     const int p = nz / 2, ngh = p / G, per_round = 2 * ngh;
-    const long long stride = (long long)nx * ny, cstride = (long long)ncx * ncy;
+    const long long stride = (long long)nx * ny, cstride = tcs;
     const int ncol = nx * ny;
     TridDev td{nx, ny, nz, ncx, ncy, nullptr, nullptr, nullptr};
     // this half's walk: forward from its wall towards the middle, backward
@@ -1084,6 +1086,249 @@ __global__ void __launch_bounds__(2 * TTM_THREADS, 1)
             for (int u = 0; u < G; u++) {
                 w = (u == 0 && h == 0) ? xj : (sv[u] - cf[u] * w) * rv[u];
                 if (cc.valid) *dst = (T)w;
+                dst -= fx;
+            }
+            slot = (slot + 1 == NS) ? 0 : slot + 1;
+        }
+    }
+    cp_async_wait<0>();
+    tmem_fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tmem_fence_after_sync();
+        tmem_free(*tslot, tcols);
+    }
+}
+
+// The same sweep at two CTAs per SM (k_thomas_th2; nx % 128 == 0 and a
+// right-hand side on a 16-byte boundary), row k's swept value at cell k of
+// the column's lane.  The recurrences run in FP64 in registers; the copy of
+// each swept value kept for the backward pass is rounded to FP32, one cell
+// per row, so a column takes nz cells of a lane and two CTAs share an SM's
+// 512 tensor-memory
+// columns: twice the chains in flight for the per-row instruction latency
+// that bounds the sweep.  The backward recurrence x_k = (s_k - c x_{k-+1})/d_k
+// is contractive, so the rounding of s_k enters x_k once, at the relative
+// size of the FP32 result's own rounding.
+//
+// The CTA's 128 columns of a round are one run of a plane row (nx % 128 ==
+// 0) and their eigenvalue classes one window of at most 128 consecutive
+// classes, so the ring is filled cooperatively with 16-byte copies: a row of
+// the right-hand side is 32 copies, a row of a table 65, for the whole CTA
+// (per-thread 4- and 8-byte copies, one per row and column, saturated the
+// memory-instruction queues at two CTAs per SM).  A barrier per 8-row group
+// publishes them.  A round takes 1.66-1.69 times as long as a round of
+// k_thomas_th (the barriers, and two CTAs' chains sharing the schedulers),
+// so the launcher takes this kernel only where it needs that many times
+// fewer rounds (0.162 against 0.176 ms at 512x384x256, 11 rounds against 6).
+constexpr int TTH2_CW = 130;       // class window of a round: 128 classes, from an even start
+constexpr int TTH2_CH = TTH2_CW / 2; // 16-byte copies per table row
+
+__host__ __device__ constexpr size_t tth2_slot_bytes()
+{
+    // right-hand side [2 halves][G][128] (float), table rows [2][G][CW] (double)
+    return (size_t)2 * TTW_G * TTM_THREADS * 4 + (size_t)2 * TTW_G * TTH2_CW * 8;
+}
+
+__host__ __device__ constexpr size_t tth2_smem_bytes()
+{
+    // ring of NS slots, (0,0)-mode ring [NS][2][G], c_k and a_k [256],
+    // junction values [2][2][128], TMEM address slot; at least 78 KB so that
+    // at most two CTAs (two times nz <= 256 tensor-memory columns) share an SM
+    const size_t b = (size_t)TTH_NS * tth2_slot_bytes() + TTH_NS * 2 * TTW_G * 8 + 2 * TTM_TM_ROWS * 8 +
+                     4 * TTM_THREADS * 8 + 16;
+    return b < 78 * 1024 ? 78 * 1024 : b;
+}
+
+__global__ void __launch_bounds__(2 * TTM_THREADS, 2)
+    k_thomas_th2(const float *xin, float *xout, const double *tm, const double *tr, const double *ak, const double *ck,
+                int nx, int ny, int nz, int ncx, int ncy, long long tcs, const double *mode0, int rounds,
+                uint32_t tcols)
+{
+    constexpr int G = TTW_G, NS = TTH_NS, NC = TTM_THREADS, NT = 2 * NC, CW = TTH2_CW, CH = TTH2_CH;
+    constexpr int SLOT = (int)tth2_slot_bytes();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    unsigned char *ring = smem_raw;                                            // [NS] slots
+    double *zring = reinterpret_cast<double *>(smem_raw + (size_t)NS * SLOT); // [NS][2][G] (0,0) mode
+    double *csh = zring + NS * 2 * G;                                         // c_k
+    double *ash = csh + TTM_TM_ROWS;                                          // a_k
+    double *jv = ash + TTM_TM_ROWS;                                           // [2 parities][2 halves][NC]
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(jv + 4 * NC);
+    const int tid = threadIdx.x, warp = tid >> 5, half = tid >= NC ? 1 : 0, lt = tid - half * NC;
+    const int p = nz / 2, ngh = p / G, per_round = 2 * ngh;
+    const long long stride = (long long)nx * ny;
+    const int ncol = nx * ny;
+    TridDev td{nx, ny, nz, ncx, ncy, nullptr, nullptr, nullptr};
+    const long long fx = half ? -stride : stride;
+
+    for (int k = tid; k < nz; k += NT) {
+        csh[k] = __ldg(ck + k);
+        ash[k] = __ldg(ak + k);
+    }
+    if (warp == 0) tmem_alloc(tslot, tcols);
+    tmem_fence_before_sync();
+    __syncthreads();
+    tmem_fence_after_sync();
+    const uint32_t tbase = *tslot + ((uint32_t)((warp & 3) * 32) << 16);
+
+    // the CTA's run of round r: its first column (plane offset; -1 past the
+    // last column) and the even start of its class window
+    struct Run {
+        long long col0, cbase;
+    };
+    auto run = [&](int r) {
+        Run u{-1, 0};
+        const int q0 = (r * (int)gridDim.x + (int)blockIdx.x) * NC;
+        if (q0 < ncol) {
+            const int b = q0 / nx, px0 = q0 - b * nx, py = trid_pair_row(b, ny);
+            const int ixmin = min(px0, nx - px0 - (NC - 1)), jy = min(py, ny - py);
+            u.col0 = (long long)px0 + (long long)nx * py;
+            u.cbase = ((long long)ixmin + (long long)ncx * jy) & ~1ll;
+        }
+        return u;
+    };
+    auto column = [&](int r) {
+        TtmColumn c{false, 0, 0};
+        const int q = (r * (int)gridDim.x + (int)blockIdx.x) * NC + lt;
+        if (q < ncol) {
+            const int b = q / nx, px = q - b * nx, py = trid_pair_row(b, ny);
+            c = TtmColumn{true, (size_t)px + (size_t)nx * py, trid_class(px, py, td)};
+        }
+        return c;
+    };
+    const bool zcta = (mode0 != nullptr) && blockIdx.x == 0;
+
+    // copy stream: step ig < ngh of a round brings the right-hand side and
+    // tm rows of forward group ig of both halves (lower: rows ig G + u,
+    // upper: nz-1 - ig G - u), step ngh + h the tr rows of backward group h
+    // (lower: p-1 - h G - u, upper: p + h G + u)
+    int ir = 0, ig = 0, islot = 0;
+    Run irun = run(0);
+    auto issue_next = [&]() {
+        if (ir < rounds) {
+            unsigned char *sl = ring + (size_t)islot * SLOT;
+            float *xr = reinterpret_cast<float *>(sl);
+            double *tb = reinterpret_cast<double *>(sl + (size_t)2 * G * NC * 4);
+            if (irun.col0 >= 0) {
+                const bool fwd = ig < ngh;
+                const int gg = fwd ? ig : ig - ngh;
+                auto row = [&](int h, int u) {
+                    return fwd ? (h ? nz - 1 - gg * G - u : gg * G + u) : (h ? p + gg * G + u : p - 1 - gg * G - u);
+                };
+                if (fwd) {
+#pragma unroll
+                    for (int e = tid; e < 2 * G * (NC / 4); e += NT) {
+                        const int h = e / (G * (NC / 4)), u = (e / (NC / 4)) % G, c = e % (NC / 4);
+                        cp_async_16(xr + (h * G + u) * NC + 4 * c, xin + irun.col0 + row(h, u) * stride + 4 * c);
+                    }
+                    if (zcta && ir == 0 && lt == 0) {
+#pragma unroll
+                        for (int u = 0; u < G; u++)
+                            cp_async_8(zring + (islot * 2 + half) * G + u, mode0 + row(half, u));
+                    }
+                }
+                const double *src = fwd ? tm : tr;
+#pragma unroll
+                for (int e = tid; e < 2 * G * CH; e += NT) {
+                    const int h = e / (G * CH), u = (e / CH) % G, c = e % CH;
+                    cp_async_16(tb + (h * G + u) * CW + 2 * c, src + irun.cbase + row(h, u) * tcs + 2 * c);
+                }
+            }
+            if (++ig == per_round) {
+                ig = 0;
+                if (++ir < rounds) irun = run(ir);
+            }
+        }
+        cp_async_commit(); // one group per step, empty or not
+        islot = (islot + 1 == NS) ? 0 : islot + 1;
+    };
+
+    for (int q = 0; q < NS - 1; q++) issue_next();
+    int slot = 0;
+    for (int r = 0; r < rounds; r++) {
+        const TtmColumn cc = column(r);
+        const int coff = (int)((long long)cc.cls - run(r).cbase); // this column's place in the class window
+        const bool zr = zcta && r == 0 && lt == 0;
+        // the junction's 2x2 coefficients, needed after the forward sweep
+        const double jE = __ldg(tm + cc.cls + nz * tcs), jC = __ldg(tm + cc.cls + (nz + 1) * tcs);
+        const double jD = __ldg(tr + cc.cls + nz * tcs), jA = __ldg(tr + cc.cls + (nz + 1) * tcs);
+        // forward: s_k = r_k - m_k s_{k -+ 1} from this half's wall
+        double s = 0.0;
+        for (int g = 0; g < ngh; g++) {
+            cp_async_wait<NS - 2>(); // this step's group has landed (every thread's share)
+            __syncthreads();
+            const unsigned char *sl = ring + (size_t)slot * SLOT;
+            const float *xs = reinterpret_cast<const float *>(sl) + half * G * NC + lt;
+            const double *cs = reinterpret_cast<const double *>(sl + (size_t)2 * G * NC * 4) + half * G * CW + coff;
+            double xv[G], mv[G];
+#pragma unroll
+            for (int u = 0; u < G; u++) {
+                xv[u] = (double)xs[u * NC];
+                mv[u] = cs[u * CW];
+            }
+            if (zr) {
+#pragma unroll
+                for (int u = 0; u < G; u++) xv[u] = zring[(slot * 2 + half) * G + u];
+            }
+            issue_next(); // refills the slot consumed one step ago
+            double sv[G];
+#pragma unroll
+            for (int u = 0; u < G; u++) sv[u] = s = xv[u] - mv[u] * s;
+            // cells of the 8-row block in ascending row order: the upper
+            // half walks its rows downwards (two branches, so that every
+            // index is a constant and the block stays in registers)
+            uint32_t v[G];
+            if (half) {
+#pragma unroll
+                for (int u = 0; u < G; u++) v[G - 1 - u] = __float_as_uint(__double2float_rn(sv[u]));
+            } else {
+#pragma unroll
+                for (int u = 0; u < G; u++) v[u] = __float_as_uint(__double2float_rn(sv[u]));
+            }
+            __syncwarp();
+            tmem_st8(tbase + (half ? nz - G - g * G : g * G), v);
+            slot = (slot + 1 == NS) ? 0 : slot + 1;
+        }
+        tmem_wait_st();
+        // rows p-1 and p from the 2x2 system that joins the halves
+        double *jr = jv + (r & 1) * 2 * NC;
+        jr[half * NC + lt] = s;
+        __syncthreads();
+        const double xs_ = jr[lt], ys_ = jr[NC + lt];
+        const double xj = half ? ys_ * jD - xs_ * jA : xs_ * jE - ys_ * jC;
+        // backward from the middle: x_k = (s_k - c_k x_{k+1}) / d_k below,
+        // x_k = (s_k - a_k x_{k-1}) / e_k above
+        double w = 0.0;
+        float *dst = xout + cc.col + (half ? p : p - 1) * stride;
+        for (int h = 0; h < ngh; h++) {
+            uint32_t v[G];
+            __syncwarp();
+            tmem_ld8_start(tbase + (half ? p + h * G : p - G - h * G), v);
+            cp_async_wait<NS - 2>();
+            __syncthreads();
+            const double *cs =
+                reinterpret_cast<const double *>(ring + (size_t)slot * SLOT + (size_t)2 * G * NC * 4) +
+                half * G * CW + coff;
+            double rv[G], cf[G];
+#pragma unroll
+            for (int u = 0; u < G; u++) {
+                rv[u] = cs[u * CW];
+                cf[u] = half ? ash[p + h * G + u] : csh[p - 1 - h * G - u];
+            }
+            issue_next();
+            tmem_wait_ld(v);
+            double sv[G];
+            if (half) {
+#pragma unroll
+                for (int u = 0; u < G; u++) sv[u] = (double)__uint_as_float(v[u]);
+            } else {
+#pragma unroll
+                for (int u = 0; u < G; u++) sv[u] = (double)__uint_as_float(v[G - 1 - u]);
+            }
+#pragma unroll
+            for (int u = 0; u < G; u++) {
+                w = (u == 0 && h == 0) ? xj : (sv[u] - cf[u] * w) * rv[u];
+                if (cc.valid) *dst = (float)w;
                 dst -= fx;
             }
             slot = (slot + 1 == NS) ? 0 : slot + 1;
@@ -1562,10 +1807,17 @@ int ppe_create(Ppe *s, int nx, int ny, int nz, double dx, double dy, const doubl
         PL_CUDA_TRY(cudaMemcpy(s->d_tmpv, tmpv.data(), sizeof(double) * ncls * P, cudaMemcpyHostToDevice));
     }
     if (twisted) {
-        PL_CUDA_TRY(cudaMalloc(&s->d_tmult, sizeof(double) * ncls * (nz + 2)));
-        PL_CUDA_TRY(cudaMalloc(&s->d_trb, sizeof(double) * ncls * (nz + 2)));
-        PL_CUDA_TRY(cudaMemcpy(s->d_tmult, tt.tmult.data(), sizeof(double) * ncls * (nz + 2), cudaMemcpyHostToDevice));
-        PL_CUDA_TRY(cudaMemcpy(s->d_trb, tt.trb.data(), sizeof(double) * ncls * (nz + 2), cudaMemcpyHostToDevice));
+        // rows of an even number of values: the sweep copies 16-byte pairs
+        s->tcs = (ncls + 1) / 2 * 2;
+        const size_t tb = sizeof(double) * s->tcs * (nz + 2);
+        PL_CUDA_TRY(cudaMalloc(&s->d_tmult, tb));
+        PL_CUDA_TRY(cudaMalloc(&s->d_trb, tb));
+        PL_CUDA_TRY(cudaMemset(s->d_tmult, 0, tb));
+        PL_CUDA_TRY(cudaMemset(s->d_trb, 0, tb));
+        PL_CUDA_TRY(cudaMemcpy2D(s->d_tmult, sizeof(double) * s->tcs, tt.tmult.data(), sizeof(double) * ncls,
+                                 sizeof(double) * ncls, nz + 2, cudaMemcpyHostToDevice));
+        PL_CUDA_TRY(cudaMemcpy2D(s->d_trb, sizeof(double) * s->tcs, tt.trb.data(), sizeof(double) * ncls,
+                                 sizeof(double) * ncls, nz + 2, cudaMemcpyHostToDevice));
     }
     if (prec == PREC_MIXED || nparts >= 1) {
         s->scratch_elems = (size_t)nx * ny * nz;
@@ -1853,17 +2105,36 @@ template <typename T> static int launch_trid(Ppe *s, T *x, cudaStream_t st, cons
     TridDev t{s->nx, s->ny, s->nz, s->ncx, s->ncy, s->d_mult, s->d_rb, s->d_c};
     dim3 grid((s->nx + 127) / 128, s->ny);
     if (sizeof(T) == 4 && s->nparts == 0 && s->d_tmult != nullptr) {
-        // the two-ended sweep (mixed path): two chains per column
-        // (one thread per half column: k_thomas_th)
+        // the two-ended sweep (mixed path): one thread per half column, one
+        // 256-thread CTA per SM (k_thomas_th), or two with FP32 copies of the
+        // swept values (k_thomas_th2) where its rounds, 1.68 times as long,
+        // are that many times fewer
+        const int ncol = s->nx * s->ny, cpr = TTM_THREADS;
+        const int ctas1 = std::max(1, std::min(sm_count(), (ncol + cpr - 1) / cpr));
+        const int rounds1 = (ncol + ctas1 * cpr - 1) / (ctas1 * cpr);
+        const int ctas2 = std::max(1, std::min(2 * sm_count(), (ncol + cpr - 1) / cpr));
+        const int rounds2 = (ncol + ctas2 * cpr - 1) / (ctas2 * cpr);
+        if constexpr (sizeof(T) == 4) {
+            if (s->nx % TTM_THREADS == 0 && (reinterpret_cast<uintptr_t>(x) & 15) == 0 &&
+                168 * rounds2 < 100 * rounds1) {
+                const size_t shm = tth2_smem_bytes();
+                uint32_t tcols = 32;
+                while (tcols < (uint32_t)s->nz) tcols *= 2;
+                PL_CUDA_TRY(cudaFuncSetAttribute(k_thomas_th2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+                k_thomas_th2<<<ctas2, 2 * TTM_THREADS, shm, st>>>(x, x, s->d_tmult, s->d_trb, s->d_a, s->d_c, s->nx,
+                                                                   s->ny, s->nz, s->ncx, s->ncy, (long long)s->tcs,
+                                                                   mode0, rounds2, tcols);
+                PL_CHECK_LAUNCH();
+                return 0;
+            }
+        }
         const size_t shm = tth_smem_bytes<T>();
-        const int ncol = s->nx * s->ny;
-        const int ctas = std::max(1, std::min(sm_count(), (ncol + TTM_THREADS - 1) / TTM_THREADS));
-        const int rounds = (ncol + ctas * TTM_THREADS - 1) / (ctas * TTM_THREADS);
         uint32_t tcols = 32;
         while (tcols < 2u * (uint32_t)s->nz) tcols *= 2;
         PL_CUDA_TRY(cudaFuncSetAttribute(k_thomas_th<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
-        k_thomas_th<T><<<ctas, 2 * TTM_THREADS, shm, st>>>(x, x, s->d_tmult, s->d_trb, s->d_a, s->d_c, s->nx, s->ny,
-                                                             s->nz, s->ncx, s->ncy, mode0, rounds, tcols);
+        k_thomas_th<T><<<ctas1, 2 * TTM_THREADS, shm, st>>>(x, x, s->d_tmult, s->d_trb, s->d_a, s->d_c, s->nx, s->ny,
+                                                              s->nz, s->ncx, s->ncy, (long long)s->tcs, mode0, rounds1,
+                                                              tcols);
         PL_CHECK_LAUNCH();
         return 0;
     }

@@ -38,9 +38,12 @@ struct Ppe {
     double *d_c = nullptr;   // c[k], nz (partition-local values)
     double *d_a = nullptr, *d_bt = nullptr; // a[k], b_tmp[k]: the z rows of the operator
     double *d_v = nullptr, *d_w = nullptr; // PDD spikes, class tables
-    // mixed-path Thomas, 16 <= nz <= 256, nz % 16 == 0: the two-ended sweep's
-    // tables (TridTables::tmult, trb; nz + 2 rows), else null
+    // mixed-path Thomas, 16 <= nz <= 256, nz % 16 == 0: the two-ended
+    // sweep's tables (TridTables::tmult, trb; nz + 2 rows of tcs values, tcs
+    // = the class count rounded up to even, so that every row starts on a
+    // 16-byte boundary), else null
     double *d_tmult = nullptr, *d_trb = nullptr;
+    size_t tcs = 0;
     double *d_tmpv = nullptr;              // PDD: v of partition m+1 at its k=0, [m][jy][ix]
     double *d_scratch = nullptr;           // mixed path: FP64 forward-sweep values
     size_t scratch_elems = 0;

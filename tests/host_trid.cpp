@@ -66,7 +66,11 @@ extern "C" int host_trid_solve(int nx, int ny, int nz, double dx, double dy, con
 // the two-ended sweep of k_thomas_th (mixed path): the LU elimination on rows
 // below p = nz/2, the elimination from the top wall on rows p .. nz-1, the
 // 2x2 system of rows p-1 and p, back substitution outwards (nz even)
-extern "C" int host_trid_solve_twisted(int nx, int ny, int nz, double dx, double dy, const double *dzf, double *x)
+// round_swept != 0: the swept values kept for the backward pass are rounded
+// to FP32, as k_thomas_th2 keeps them in tensor memory (the recurrences and
+// the junction stay FP64)
+extern "C" int host_trid_solve_twisted(int nx, int ny, int nz, double dx, double dy, const double *dzf, double *x,
+                                       int round_swept)
 {
     TridTables t;
     trid_build(t, nx, ny, nz, dx, dy, dzf, 0, true);
@@ -82,8 +86,9 @@ extern "C" int host_trid_solve_twisted(int nx, int ny, int nz, double dx, double
             auto M = [&](int k) { return t.tmult[cls + (size_t)k * cs]; };
             auto R = [&](int k) { return t.trb[cls + (size_t)k * cs]; };
             double sl = 0.0, su = 0.0;
-            for (int k = 0; k < p; k++) xs[k] = sl = x[col + (size_t)k * stride] - M(k) * sl;
-            for (int k = nz - 1; k >= p; k--) xs[k] = su = x[col + (size_t)k * stride] - M(k) * su;
+            auto keep = [&](double v) { return round_swept ? (double)(float)v : v; };
+            for (int k = 0; k < p; k++) xs[k] = keep(sl = x[col + (size_t)k * stride] - M(k) * sl);
+            for (int k = nz - 1; k >= p; k--) xs[k] = keep(su = x[col + (size_t)k * stride] - M(k) * su);
             double wl = sl * M(nz) - su * M(nz + 1), wu = su * R(nz) - sl * R(nz + 1);
             x[col + (size_t)(p - 1) * stride] = wl;
             x[col + (size_t)p * stride] = wu;

@@ -24,7 +24,12 @@ def rel_max(a, b):
     return float(np.abs(a - b).max() / np.abs(b).max())
 
 
-@pytest.mark.parametrize("nx,ny,nz,nsteps", [(64, 64, 64, 20), (96, 72, 48, 10), (32, 24, 320, 8)])
+# nz <= 256 takes the two-ended Thomas sweep: one CTA per SM (k_thomas_th)
+# at the first two sizes, two (k_thomas_th2, runs of 128 columns whose
+# eigenvalue classes ascend, descend and, at nx = 384, straddle the mirror
+# column nx/2) at the last two; nz = 320 the one-ended sweep
+@pytest.mark.parametrize("nx,ny,nz,nsteps", [(64, 64, 64, 20), (96, 72, 48, 10), (32, 24, 320, 8),
+                                             (256, 256, 16, 3), (384, 192, 16, 3)])
 def test_mixed_vs_fp64_oracle(gpu, oracle_mod, nx, ny, nz, nsteps):
     plb, O = gpu, oracle_mod
     cfg = plb.ChannelConfig(nx=nx, ny=ny, nz=nz, stretch_ratio=1.5, re_tau=180.0, precision=plb.PL_MIXED)
