@@ -85,11 +85,13 @@ int pl_ppe_destroy(pl_ppe *s);
  * its FP64 forward-swept values in device memory (pl_ppe_solve keeps them in
  * tensor memory where nz allows), and that memory is a fixed 16 MiB array
  * inside the library instead of the plan's buffer; it calls no cudaMalloc or
- * cudaFree.  The results equal pl_ppe_solve's (same arithmetic).
+ * cudaFree.  The results agree with pl_ppe_solve's to FP32 rounding, modulo
+ * the (0,0) mode's free constant where pl_ppe_solve runs the two-ended sweep
+ * (16 <= nz <= 256, nz % 16 == 0), which takes its own gauge.
  * Limit: nx*ny*nz <= 2,097,152 (e.g. 128^3); larger plans are rejected with an
  * error.  The array's device address is looked up on the first call on each
- * device (and again after the device's context is recreated): make that first
- * call before any stream capture.  Every call on a device shares the array:
+ * device (and again after the device's context is recreated).  Every call on a
+ * device shares the array:
  * calls that overlap on the GPU (other streams, other threads) race;
  * serialise them.  The plan's other tables are read-only and are shared
  * safely. */
