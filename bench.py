@@ -109,18 +109,49 @@ def traffic_from_profiles(kernel):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled during the timed
+    region: read through NVML every 5 ms between begin() and end(), which
+    _timed calls around the timed steps alone; without NVML, nvidia-smi
+    (`-lms 200`, the whole span from start() to stop()).  Reads only."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits (nvml.h nvmlClocksEventReason*)
+    REASON_BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+                   "hw_thermal_slowdown": 0x40}
 
     def __init__(self, index):
         self.index = index
         self.proc = None
+        self.nvml = None
         self.lines = []
+        self.samples = []
+        self.on = threading.Event()
+        self.done = threading.Event()
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        try:  # the NVML device of this CUDA device (CUDA_VISIBLE_DEVICES may renumber)
+            uuid = "GPU-" + str(torch.cuda.get_device_properties(self.index).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid.encode())
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
 
     def start(self):
+        try:
+            self.nvml, self.handle = self._nvml_handle()
+            self.smax = float(self.nvml.nvmlDeviceGetMaxClockInfo(self.handle, self.nvml.NVML_CLOCK_SM))
+            get = getattr(self.nvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                self.nvml.nvmlDeviceGetCurrentClocksThrottleReasons
+            self.reasons_of = lambda: int(get(self.handle))
+            self.th = threading.Thread(target=self._poll, daemon=True)
+            self.th.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
@@ -130,11 +161,39 @@ class ClockSampler:
         except Exception:
             self.proc = None
 
+    def begin(self):
+        self.on.set()
+
+    def end(self):
+        self.on.clear()
+
+    def _poll(self):
+        while not self.done.is_set():
+            if self.on.wait(timeout=0.05) and not self.done.is_set():
+                try:
+                    sm = float(self.nvml.nvmlDeviceGetClockInfo(self.handle, self.nvml.NVML_CLOCK_SM))
+                    self.samples.append((sm, self.reasons_of()))
+                except Exception:
+                    pass
+                time.sleep(0.005)
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def stop(self):
+        if self.nvml is not None:
+            self.done.set()
+            self.on.set()
+            self.th.join(timeout=5)
+            try:
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
+            sm = [x for x, _ in self.samples]
+            reasons = sorted(n for n, bit in self.REASON_BITS.items() if any(r & bit for _, r in self.samples))
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.smax,
+                    "reasons": reasons, "samples": len(sm), "source": "nvml, timed steps only"}
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         time.sleep(0.25)
@@ -158,7 +217,7 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi, warm-up and timed steps"}
 
 
 def cpu_threads():
@@ -246,10 +305,11 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def _timed(ch, K, W, body, world):
+def _timed(ch, K, W, body, world, clocks=None):
     """device time of K calls of body after W untimed ones: CUDA events on
     the channel's stream, barrier and synchronisation on both sides, the
-    slowest rank's"""
+    slowest rank's; `clocks` (a started ClockSampler) samples while the K
+    calls are enqueued and run"""
     import torch
     for _ in range(W):
         body()
@@ -259,12 +319,16 @@ def _timed(ch, K, W, body, world):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier(world)
     torch.cuda.synchronize()
+    if clocks is not None:
+        clocks.begin()
     e0.record(st)
     for _ in range(K):
         body()
     e1.record(st)
     ch.synchronize()
     torch.cuda.synchronize()
+    if clocks is not None:
+        clocks.end()
     barrier(world)
     return max_over_ranks(e0.elapsed_time(e1), world)
 
@@ -289,7 +353,7 @@ def run_slabs(args, world, rank, local):
         S.init_flow([sl], tr, nzs, SEED, NOISE)
         clocks = ClockSampler(local)
         clocks.start()
-        ms = _timed(sl, args.steps, args.warmup, lambda: S.step([sl], tr, nzs), world)
+        ms = _timed(sl, args.steps, args.warmup, lambda: S.step([sl], tr, nzs), world, clocks)
         clk = clocks.stop()
         # per-phase device times over 3 steps (events on the slab's stream)
         st = torch.cuda.ExternalStream(sl.stream_handle)
@@ -380,8 +444,8 @@ def run_b200(args):
         return
     import powerllel_channel_b200 as plb
 
-    def timed(ch, K, W, body):
-        return _timed(ch, K, W, body, world)
+    def timed(ch, K, W, body, clocks=None):
+        return _timed(ch, K, W, body, world, clocks)
 
     peak, peak_kind = peaks()
     npts = NX * NY * NZ
@@ -393,7 +457,7 @@ def run_b200(args):
         ch.init_flow(SEED, NOISE)
         clocks = ClockSampler(local)
         clocks.start()
-        ms = timed(ch, args.steps, args.warmup, lambda: ch.step(1))
+        ms = timed(ch, args.steps, args.warmup, lambda: ch.step(1), clocks)
         clk = clocks.stop()
         prof = ch.profile(3)
         alg = ALG_BYTES[prec_name]
