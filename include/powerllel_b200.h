@@ -70,8 +70,11 @@ typedef struct pl_ppe pl_ppe;
 int pl_ppe_create(pl_ppe **out, int nx, int ny, int nz, double dx, double dy, const double *dzf_global,
                   int nparts, int precision);
 /* In place on a device array of nx*ny*nz values (double for PL_FP64, float
- * for PL_MIXED), layout [k][j][i], i fastest, no ghosts.  Asynchronous on
- * `stream`.  Same operator as execute_poisson_solver (:468-605). */
+ * for PL_MIXED), layout [k][j][i], i fastest, no ghosts, starting on a
+ * boundary of two elements (16 bytes for PL_FP64, 8 for PL_MIXED; every
+ * cudaMalloc'd array does): other arrays are rejected with an error.
+ * Asynchronous on `stream`.  Same operator as execute_poisson_solver
+ * (:468-605). */
 int pl_ppe_solve(pl_ppe *s, void *d_var, void *stream);
 int pl_ppe_destroy(pl_ppe *s);
 
@@ -85,7 +88,8 @@ int pl_ppe_destroy(pl_ppe *s);
  * its FP64 forward-swept values in device memory (pl_ppe_solve keeps them in
  * tensor memory where nz allows), and that memory is a fixed 16 MiB array
  * inside the library instead of the plan's buffer; it calls no cudaMalloc or
- * cudaFree.  The results agree with pl_ppe_solve's to FP32 rounding, modulo
+ * cudaFree.  d_var as for pl_ppe_solve (8-byte boundary).  The results
+ * agree with pl_ppe_solve's to FP32 rounding, modulo
  * the (0,0) mode's free constant where pl_ppe_solve runs the two-ended sweep
  * (16 <= nz <= 256, nz % 16 == 0), which takes its own gauge.
  * Limit: nx*ny*nz <= 2,097,152 (e.g. 128^3); larger plans are rejected with an

@@ -6,6 +6,7 @@
 // write the fields (see stencil.cu).
 #include <cmath>
 #include <cstdlib>
+#include <cstdint>
 #include <cstring>
 #include <mutex>
 #include <utility>
@@ -153,6 +154,14 @@ extern "C" int pl_ppe_solve(pl_ppe *p, void *d_var, void *stream)
 {
     if (!p || !d_var) {
         set_error("pl_ppe_solve: null argument");
+        return -1;
+    }
+    // the y transform reads and writes adjacent column pairs as one complex
+    // value: the array must start on a boundary of two elements
+    const uintptr_t pair = p->s.prec == PREC_FP64 ? 16 : 8;
+    if (reinterpret_cast<uintptr_t>(d_var) % pair != 0) {
+        set_error(std::string("pl_ppe_solve: d_var must be aligned to ") + std::to_string(pair) +
+                  " bytes (two elements)");
         return -1;
     }
     cudaStream_t st = (cudaStream_t)stream;

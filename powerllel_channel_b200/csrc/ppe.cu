@@ -2493,5 +2493,9 @@ extern "C" int pl_ppe_solve_noalloc(pl_ppe *p, void *d_var, void *stream)
         pl::set_error("pl_ppe_solve_noalloc: null argument");
         return -1;
     }
+    if (reinterpret_cast<uintptr_t>(d_var) % 8 != 0) { // column pairs of the y transform, as pl_ppe_solve
+        pl::set_error("pl_ppe_solve_noalloc: d_var must be aligned to 8 bytes (two elements)");
+        return -1;
+    }
     return pl::ppe_solve_fp32_noalloc(&p->s, (float *)d_var, (cudaStream_t)stream);
 }

@@ -105,3 +105,43 @@ def test_mixed_phase_rk1_increment(gpu, oracle_mod):
         got = ch.get_field(which)
         inc = np.abs(ref - base).max()
         assert np.abs(got - ref).max() <= 2e-5 * inc + 1e-15, which
+
+
+def test_mixed_ppe_aligned_and_offset_arrays(gpu, oracle_mod):
+    """pl_ppe_solve with PL_MIXED at 384x192x16 against the oracle's FP64
+    solve, on an array that starts on a 16-byte boundary (staged transforms,
+    the two-ended Thomas sweep at two CTAs per SM) and on one 8 bytes past it
+    (the transforms' generic kernels, the sweep at one CTA per SM), compared
+    modulo the mean (the Neumann null mode): FP32 transforms, 1e-5 relative.
+    An array 4 bytes past a boundary is rejected before any launch (the y
+    transform reads column pairs as one 8-byte value)."""
+    import torch
+    plb, O = gpu, oracle_mod
+    nx, ny, nz = 384, 192, 16
+    g = O.Grid(nx, ny, nz, stretch=1.8)
+    rng = np.random.default_rng(7)
+    r = rng.standard_normal((nz, ny, nx))
+    wgt = g.dzf_global[1:-1]
+    r -= (r.mean(axis=(1, 2)) * wgt).sum() / wgt.sum()
+    var = np.zeros(g.shape)
+    var[1:-1, 1:-1, 1:-1] = r
+    O.PPE(nx, ny, nz, g.g.dx, g.g.dy, g.dzf_global).execute(var)
+    ref = var[1:-1, 1:-1, 1:-1]
+    ref = ref - ref.mean()
+    s = plb.DevicePoissonSolver(nx, ny, nz, g.g.dx, g.g.dy, g.dzf_global, precision=plb.PL_MIXED)
+    n = nx * ny * nz
+    src = torch.tensor(r.ravel(), dtype=torch.float32, device="cuda")
+    errs = []
+    for off in (0, 2):  # floats past the allocation's (256-byte aligned) start
+        buf = torch.zeros(n + 4, dtype=torch.float32, device="cuda")
+        x = buf[off:off + n]
+        x.copy_(src)
+        s.solve(x)
+        torch.cuda.synchronize()
+        got = x.cpu().numpy().reshape(nz, ny, nx).astype(np.float64)
+        errs.append(float(np.abs((got - got.mean()) - ref).max() / np.abs(ref).max()))
+    print("mixed PPE 384x192x16, rel. error (16-byte, 8-byte boundary):", errs)
+    assert max(errs) < 1e-5, errs
+    buf = torch.zeros(n + 4, dtype=torch.float32, device="cuda")
+    with pytest.raises(plb.PowerLLELError, match="aligned to 8 bytes"):
+        s.solve(buf[1:1 + n])
