@@ -157,11 +157,12 @@ extern "C" int pl_ppe_solve(pl_ppe *p, void *d_var, void *stream)
         return -1;
     }
     // the y transform reads and writes adjacent column pairs as one complex
-    // value: the array must start on a boundary of two elements
-    const uintptr_t pair = p->s.prec == PREC_FP64 ? 16 : 8;
-    if (reinterpret_cast<uintptr_t>(d_var) % pair != 0) {
-        set_error(std::string("pl_ppe_solve: d_var must be aligned to ") + std::to_string(pair) +
-                  " bytes (two elements)");
+    // value: the array must start on a boundary of two elements (checked
+    // before the plan is read)
+    const uintptr_t a = reinterpret_cast<uintptr_t>(d_var);
+    if (a % 8 != 0 || (a % 16 != 0 && p->s.prec == PREC_FP64)) {
+        set_error(std::string("pl_ppe_solve: d_var must be aligned to ") + (a % 8 != 0 ? "8" : "16") +
+                  " bytes (two elements: 8 for PL_MIXED, 16 for PL_FP64)");
         return -1;
     }
     cudaStream_t st = (cudaStream_t)stream;

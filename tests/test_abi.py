@@ -70,6 +70,23 @@ def test_host_layer_rejects_bad_arrays():
         plb._ptr(np.zeros((4, 4))[:, ::2])
 
 
+def test_ppe_solve_rejects_misaligned_array():
+    """pl_ppe_solve and pl_ppe_solve_noalloc reject a device array that does
+    not start on a boundary of two elements before they read the plan or
+    launch anything (neither address below is dereferenced), so the check
+    runs without a GPU."""
+    import powerllel_channel_b200 as plb
+    from powerllel_channel_b200 import build as B
+    B.build()
+    lib = C.CDLL(plb.LIB_PATH)
+    lib.pl_last_error.restype = C.c_char_p
+    for fn in (lib.pl_ppe_solve, lib.pl_ppe_solve_noalloc):
+        fn.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        fn.restype = C.c_int
+        assert fn(C.c_void_p(0x1000), C.c_void_p(0x2004), None) != 0
+        assert b"aligned to 8 bytes" in lib.pl_last_error()
+
+
 def test_package_has_no_oracle_dependency():
     """The product never imports, links or runs the oracle."""
     pkg = os.path.join(ROOT, "powerllel_channel_b200")
