@@ -122,3 +122,39 @@ def test_twisted_sweep_fp32_kept_values(path):
     ref = d["p"]
     err = np.abs((p - p.mean()) - (ref - ref.mean())).max() / np.abs(ref - ref.mean()).max()
     assert 0.0 < err < 1e-7, err
+
+
+def _pair_row(b, ny):
+    """trid_pair_row (ppe.cu): processing row b -> plane row py, mirror rows adjacent"""
+    if b == 0:
+        return 0
+    if b == ny - 1:
+        return ny // 2
+    jy = (b + 1) // 2
+    return jy if b & 1 else ny - jy
+
+
+@pytest.mark.parametrize("nx,ny", [(128, 24), (256, 256), (384, 192), (512, 384), (768, 32), (1024, 768)])
+def test_thomas_th2_class_windows(nx, ny):
+    """Index arithmetic of k_thomas_th2's cooperative copies (nx % 128 == 0):
+    the processing rows visit every plane row once; a round's 128 columns are
+    one run px0 .. px0+127 of plane row py, whose eigenvalue classes
+    min(px, nx-px) + ncx min(py, ny-py) all lie in the window of 130 table
+    values that starts at the even cbase; the window's 65 16-byte copies of
+    every swept row (rows < nz) stay inside the tables' nz + 2 rows of tcs
+    values."""
+    ncx, ncy = nx // 2 + 1, ny // 2 + 1
+    ncls = ncx * ncy
+    tcs = (ncls + 1) // 2 * 2
+    assert sorted(_pair_row(b, ny) for b in range(ny)) == list(range(ny))
+    for b in range(ny):
+        py = _pair_row(b, ny)
+        jy = min(py, ny - py)
+        for px0 in range(0, nx, 128):
+            ixmin = min(px0, nx - px0 - 127)
+            cbase = (ixmin + ncx * jy) & ~1
+            offs = [min(px, nx - px) + ncx * jy - cbase for px in range(px0, px0 + 128)]
+            assert cbase % 2 == 0 and min(offs) >= 0 and max(offs) < 130, (b, px0, min(offs), max(offs))
+            # last value read of a swept row k <= nz-1, against the table's end
+            for nz in (16, 256):
+                assert (nz - 1) * tcs + cbase + 129 < (nz + 2) * tcs
