@@ -179,6 +179,21 @@ class PoissonSolver:
         self.free()
 
 
+def _device_array_ptr(t, n: int, fp64: bool) -> int:
+    """The device address of a torch tensor handed to the solver, after the
+    checks the C ABI cannot make: a CUDA tensor of n contiguous values of the
+    plan's precision (float64 for PL_FP64, float32 for PL_MIXED).  A smaller
+    or wider array would be read past its end."""
+    want = "torch.float64" if fp64 else "torch.float32"
+    if not getattr(t, "is_cuda", False):
+        raise PowerLLELError("solve: the array must be a CUDA tensor")
+    if str(t.dtype) != want:
+        raise PowerLLELError(f"solve: the array is {t.dtype}, the plan needs {want}")
+    if not t.is_contiguous() or t.numel() != n:
+        raise PowerLLELError(f"solve: the array must be {n} contiguous values (nx*ny*nz)")
+    return t.data_ptr()
+
+
 class DevicePoissonSolver:
     """The PPE on a device array ([k][j][i], nx*ny*nz, float64 for PL_FP64,
     float32 for PL_MIXED).  ``solve`` takes a device pointer (int) or any
@@ -195,7 +210,10 @@ class DevicePoissonSolver:
         self.precision = precision
 
     def solve(self, d_var, stream=None) -> None:
-        ptr = d_var.data_ptr() if hasattr(d_var, "data_ptr") else int(d_var)
+        if hasattr(d_var, "data_ptr"):
+            ptr = _device_array_ptr(d_var, self.n[0] * self.n[1] * self.n[2], self.precision == PL_FP64)
+        else:
+            ptr = int(d_var)
         st = None
         if stream is not None:
             st = C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))

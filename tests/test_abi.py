@@ -95,3 +95,37 @@ def test_package_has_no_oracle_dependency():
             if f.endswith((".py", ".cu", ".cuh", ".h", ".cpp")):
                 txt = open(os.path.join(dirpath, f)).read()
                 assert "oracle" not in txt.lower().replace("no oracle", ""), f
+
+
+def test_host_layer_checks_solver_tensors():
+    """DevicePoissonSolver.solve checks a torch tensor before its address
+    crosses the C ABI: device, dtype of the plan's precision, contiguity and
+    size (nx*ny*nz values); the CUDA-only case is checked on CPU with a
+    stand-in that reports a CUDA tensor."""
+    import torch
+    import powerllel_channel_b200 as plb
+
+    class Fake:
+        def __init__(self, t):
+            self.t, self.is_cuda, self.dtype = t, True, t.dtype
+
+        def is_contiguous(self):
+            return self.t.is_contiguous()
+
+        def numel(self):
+            return self.t.numel()
+
+        def data_ptr(self):
+            return 0x1000
+
+    with pytest.raises(plb.PowerLLELError, match="CUDA tensor"):
+        plb._device_array_ptr(torch.zeros(8, dtype=torch.float64), 8, True)
+    with pytest.raises(plb.PowerLLELError, match="needs torch.float64"):
+        plb._device_array_ptr(Fake(torch.zeros(8, dtype=torch.float32)), 8, True)
+    with pytest.raises(plb.PowerLLELError, match="needs torch.float32"):
+        plb._device_array_ptr(Fake(torch.zeros(8, dtype=torch.float64)), 8, False)
+    with pytest.raises(plb.PowerLLELError, match="contiguous"):
+        plb._device_array_ptr(Fake(torch.zeros(4, 4)[:, ::2]), 8, False)
+    with pytest.raises(plb.PowerLLELError, match="contiguous"):
+        plb._device_array_ptr(Fake(torch.zeros(6)), 8, False)
+    assert plb._device_array_ptr(Fake(torch.zeros(8)), 8, False) == 0x1000
