@@ -335,15 +335,17 @@ class Channel:
         _check(lib().pl_channel_kinetic_energy(self._h, _ptr(ke)), "pl_channel_kinetic_energy")
         return float(ke[0])
 
-    def adjoint_ke_gradient(self, nsteps: int, every: int, d_gu: int, d_gv: int, d_gw: int):
+    def adjoint_ke_gradient(self, nsteps: int, every: int, d_gu, d_gv, d_gw):
         """Gradient of the kinetic energy after nsteps steps (hand-written
         adjoint, checkpoint every `every` steps) w.r.t. the current fields and
-        the body force. d_g*: device pointers of nx*ny*(nz+2) doubles.
-        Returns (J, dJ/df)."""
+        the body force. d_g*: nx*ny*(nz+2) doubles on the device, as CUDA
+        tensors (checked) or device addresses. Returns (J, dJ/df)."""
         ke = np.zeros(1)
         gf = np.zeros(3)
-        _check(lib().pl_adjoint_ke_gradient(self._h, int(nsteps), int(every), _ptr(ke), C.c_void_p(d_gu),
-                                            C.c_void_p(d_gv), C.c_void_p(d_gw), _ptr(gf)), "pl_adjoint_ke_gradient")
+        g = [_device_array_ptr(a, self.compact_elems, True) if hasattr(a, "data_ptr") else int(a)
+             for a in (d_gu, d_gv, d_gw)]
+        _check(lib().pl_adjoint_ke_gradient(self._h, int(nsteps), int(every), _ptr(ke), C.c_void_p(g[0]),
+                                            C.c_void_p(g[1]), C.c_void_p(g[2]), _ptr(gf)), "pl_adjoint_ke_gradient")
         return float(ke[0]), gf
 
     # statistics (mod_statistics.f90) -------------------------------------
